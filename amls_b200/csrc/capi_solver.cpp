@@ -1,0 +1,138 @@
+// C ABI: handle, solve and batched dense eigensolver entry points.
+#include <chrono>
+#include <cstring>
+
+#include "amls_b200.h"
+#include "host/engine.hpp"
+#include "host/status.hpp"
+
+using namespace amls_b200;
+
+struct amls_handle_s {
+    Engine* eng = nullptr;
+};
+
+namespace {
+int checkHandle(amls_handle h) {
+    if (!h || !h->eng) return fail(AMLS_ERR_INVALID_ARGUMENT, "null handle");
+    return AMLS_OK;
+}
+
+int checkOptions(const amls_options* opt) {
+    if (!opt) return fail(AMLS_ERR_INVALID_ARGUMENT, "null options");
+    if (opt->nev <= 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
+    if (opt->leafSize < 1) return fail(AMLS_ERR_INVALID_ARGUMENT, "leafSize must be >= 1");
+    if (opt->nLevels < 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "nLevels must be >= 0");
+    return AMLS_OK;
+}
+}  // namespace
+
+extern "C" int amls_create(int device, amls_handle* out) {
+    return guarded([&]() -> int {
+        if (!out) return fail(AMLS_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        auto* h = new amls_handle_s;
+        try {
+            h->eng = new Engine(device);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_destroy(amls_handle h) {
+    return guarded([&]() -> int {
+        if (!h) return AMLS_OK;
+        delete h->eng;
+        delete h;
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_analyze(amls_handle h, int64_t n, const int64_t* kp, const int32_t* kc,
+                            const int64_t* mp, const int32_t* mc, const amls_options* opt) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (int e = checkOptions(opt)) return e;
+        if (n <= 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "empty matrix");
+        if (!kp || !kc || !mp || !mc) return fail(AMLS_ERR_INVALID_ARGUMENT, "null CSR array");
+        h->eng->analyze(n, kp, kc, mp, mc, *opt);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_solve_values(amls_handle h, const double* kv, const double* mv,
+                                 int32_t values_on_device, double* theta, double* Z,
+                                 int32_t outputs_on_device, int64_t* p_out, double* timing) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!kv || !mv || !theta) return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        h->eng->solveValues(kv, mv, values_on_device != 0, theta, Z, outputs_on_device != 0, p_out,
+                            timing);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_solve(amls_handle h, int64_t n, const int64_t* kp, const int32_t* kc,
+                          const double* kv, const int64_t* mp, const int32_t* mc, const double* mv,
+                          const amls_options* opt, double* theta, double* Z, int64_t* p_out,
+                          double* timing) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (int e = checkOptions(opt)) return e;
+        if (n <= 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "empty matrix");
+        if (!kp || !kc || !kv || !mp || !mc || !mv || !theta)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        double t[AMLS_T_SLOTS] = {0};
+        const auto t0 = std::chrono::steady_clock::now();
+        h->eng->analyze(n, kp, kc, mp, mc, *opt);
+        const auto t1 = std::chrono::steady_clock::now();
+        h->eng->solveValues(kv, mv, false, theta, opt->recoverVectors ? Z : nullptr, false, p_out, t);
+        t[AMLS_T_PARTITION] = std::chrono::duration<double>(t1 - t0).count();
+        t[AMLS_T_TOTAL] += t[AMLS_T_PARTITION];
+        if (timing) std::memcpy(timing, t, sizeof(t));
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_info(amls_handle h, int64_t* info) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!info) return fail(AMLS_ERR_INVALID_ARGUMENT, "null info");
+        for (int i = 0; i < AMLS_INFO_SLOTS; ++i) info[i] = 0;
+        h->eng->info(info);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_work(amls_handle h, double* work) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!work) return fail(AMLS_ERR_INVALID_ARGUMENT, "null work");
+        h->eng->work(work);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n,
+                                  const int64_t* mat_off, const double* K, const double* M,
+                                  int32_t mode, int64_t il, int64_t iu, double lo, double hi,
+                                  const int64_t* cap, const int64_t* w_off, double* w,
+                                  const int64_t* v_off, double* V, int64_t* m) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (batch < 0 || (batch > 0 && (!n || !mat_off || !K || !M || !cap || !w_off || !w ||
+                                        !v_off || !V || !m)))
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        if (mode != 0 && mode != 1) return fail(AMLS_ERR_INVALID_ARGUMENT, "mode must be 0 or 1");
+        if (mode == 0 && il != 1)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "index mode supports il == 1 only");
+        if (mode == 1 && lo > -1e299)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "interval mode supports lo = -inf only");
+        h->eng->sygvxBatched(batch, n, mat_off, K, M, mode, il, iu, lo, hi, cap, w_off, w, v_off, V, m);
+        return AMLS_OK;
+    });
+}

@@ -1,0 +1,1241 @@
+// AMLS engine implementation (see engine.hpp for the algorithm map).
+#include "host/engine.hpp"
+
+#include <chrono>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+#include <stdexcept>
+
+namespace amls_b200 {
+
+namespace {
+
+constexpr int kSmallEig = 384;     // tridiagonalise n <= this with one CTA per matrix
+constexpr int kT = kGemmTile;      // 64
+
+int cdiv(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// tiles of a GEMM descriptor (M x N)
+void gemmTiles(std::vector<TileRef>& t, int desc, int64_t M, int64_t N) {
+    for (int j = 0; j < cdiv(N, kT); ++j)
+        for (int i = 0; i < cdiv(M, kT); ++i) t.push_back({desc, i * kT, j * kT, 0});
+}
+
+void trsmTiles(std::vector<TileRef>& t, int desc, int64_t rows) {
+    for (int i = 0; i < cdiv(rows, kTrsmRows); ++i) t.push_back({desc, i * kTrsmRows, 0, 0});
+}
+
+void copyTiles(std::vector<TileRef>& t, int desc, int64_t r, int64_t c) {
+    for (int j = 0; j < cdiv(c, 32); ++j)
+        for (int i = 0; i < cdiv(r, 32); ++i) t.push_back({desc, i * 32, j * 32, 0});
+}
+
+GemmDesc gemm(int64_t M, int64_t N, int64_t K, int flags, const double* A, int64_t lda,
+              const double* B, int64_t ldb, double* C, int64_t ldc, double alpha, double beta) {
+    GemmDesc d{};
+    d.M = static_cast<int32_t>(M);
+    d.N = static_cast<int32_t>(N);
+    d.K = static_cast<int32_t>(K);
+    d.flags = flags;
+    d.A = A;
+    d.lda = lda;
+    d.B = B;
+    d.ldb = ldb;
+    d.C = C;
+    d.ldc = ldc;
+    d.alpha = alpha;
+    d.beta = beta;
+    return d;
+}
+
+using Clock = std::chrono::steady_clock;
+double secs(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+}  // namespace
+
+// kernels launched only from here
+cudaError_t launchGemmBatched(const GemmDesc*, const TileRef*, int, cudaStream_t);
+
+#define LAUNCH(call)                                   \
+    do {                                               \
+        cudaCheck((call), #call);                      \
+        ++launches_;                                   \
+    } while (0)
+
+Engine::Engine(int device) : device_(device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        throw AmlsError(AMLS_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "bad device index");
+    cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+    cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device);
+    status_.ensure(4 * sizeof(int));
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+}
+
+double Engine::elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+}
+
+// ---------------------------------------------------------------------------
+// analysis
+// ---------------------------------------------------------------------------
+void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
+                     const int32_t* mc, const amls_options& opt) {
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    analyzed_ = false;
+    tridiagDone_ = false;
+    if (n <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty matrix");
+    for (int64_t r = 0; r < n; ++r) {
+        if (kp[r + 1] < kp[r] || mp[r + 1] < mp[r])
+            throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "CSR row pointers not monotone");
+    }
+    opt_ = opt;
+    n_ = n;
+    nnzK_ = kp[n];
+    nnzM_ = mp[n];
+
+    PartitionResult pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize);
+    perm_ = pr.perm;
+    inv_.assign(static_cast<size_t>(n), 0);
+    for (int64_t j = 0; j < n; ++j) inv_[static_cast<size_t>(perm_[static_cast<size_t>(j)])] = j;
+    const SeparatorTree& T = pr.tree;
+    const int N = static_cast<int>(T.nNodes());
+    nodes_.assign(static_cast<size_t>(N), Node());
+    order_.clear();
+    for (int64_t id : T.postOrder()) order_.push_back(static_cast<int>(id));
+    int64_t acc = 0;
+    for (int i : order_) {
+        Node& nd = nodes_[static_cast<size_t>(i)];
+        nd.off = acc;
+        nd.n = static_cast<int64_t>(T.node(i).indices.size());
+        nd.parent = static_cast<int>(T.node(i).parent);
+        for (int64_t a : T.ancestors(i)) nd.anc.push_back(static_cast<int>(a));
+        acc += nd.n;
+    }
+    maxLevel_ = 0;
+    for (int i : order_) {
+        int l = 0;
+        for (int64_t c : T.node(i).children) l = std::max(l, nodes_[static_cast<size_t>(c)].level + 1);
+        nodes_[static_cast<size_t>(i)].level = l;
+        maxLevel_ = std::max(maxLevel_, l);
+    }
+    byLevel_.assign(static_cast<size_t>(maxLevel_) + 1, {});
+    for (int i : order_) byLevel_[static_cast<size_t>(nodes_[static_cast<size_t>(i)].level)].push_back(i);
+    owner_.assign(static_cast<size_t>(n), -1);
+    for (int i = 0; i < N; ++i) {
+        Node& nd = nodes_[static_cast<size_t>(i)];
+        for (int64_t r = nd.off; r < nd.off + nd.n; ++r) owner_[static_cast<size_t>(r)] = i;
+        nd.pathPrefix = 0;
+        for (int a : nd.anc) nd.pathPrefix += nodes_[static_cast<size_t>(a)].n;
+    }
+    // subtree start offsets (post-order: a subtree is contiguous, ending at the node)
+    std::vector<int64_t> subStart(static_cast<size_t>(N));
+    for (int i : order_) {
+        int64_t s = nodes_[static_cast<size_t>(i)].off;
+        for (int64_t c : T.node(i).children) s = std::min(s, subStart[static_cast<size_t>(c)]);
+        subStart[static_cast<size_t>(i)] = s;
+    }
+
+    // symbolic fill: S_i = ancestor DOFs coupled to node i after elimination
+    std::vector<std::vector<int32_t>> push(static_cast<size_t>(N));
+    std::vector<char> isAnc(static_cast<size_t>(N), 0);
+    for (int i : order_) {
+        Node& nd = nodes_[static_cast<size_t>(i)];
+        for (int a : nd.anc) isAnc[static_cast<size_t>(a)] = 1;
+        std::vector<int32_t> S = std::move(push[static_cast<size_t>(i)]);
+        for (int64_t r = nd.off; r < nd.off + nd.n; ++r) {
+            const int64_t old = perm_[static_cast<size_t>(r)];
+            for (int pass = 0; pass < 2; ++pass) {
+                const int64_t* rp = pass ? mp : kp;
+                const int32_t* ci = pass ? mc : kc;
+                for (int64_t e = rp[old]; e < rp[old + 1]; ++e) {
+                    const int64_t c = inv_[static_cast<size_t>(ci[e])];
+                    const int o = owner_[static_cast<size_t>(c)];
+                    if (o == i) continue;
+                    if (c < nd.off) {
+                        if (c < subStart[static_cast<size_t>(i)])
+                            throw AmlsError(AMLS_ERR_PARTITION, "partition couples disjoint subtrees");
+                        continue;  // descendant: held in the descendant's front
+                    }
+                    if (!isAnc[static_cast<size_t>(o)])
+                        throw AmlsError(AMLS_ERR_PARTITION, "partition couples disjoint subtrees");
+                    S.push_back(static_cast<int32_t>(c));
+                }
+            }
+        }
+        std::sort(S.begin(), S.end());
+        S.erase(std::unique(S.begin(), S.end()), S.end());
+        if (!S.empty()) {
+            const int a0 = owner_[static_cast<size_t>(S[0])];
+            const Node& A0 = nodes_[static_cast<size_t>(a0)];
+            auto& dst = push[static_cast<size_t>(a0)];
+            for (int32_t c : S)
+                if (c >= A0.off + A0.n) dst.push_back(c);
+        }
+        nd.S = std::move(S);
+        for (int a : nd.anc) isAnc[static_cast<size_t>(a)] = 0;
+    }
+    // layout
+    frontTotal_ = eigTotal_ = vecTotal_ = 0;
+    for (int i : order_) {
+        Node& nd = nodes_[static_cast<size_t>(i)];
+        nd.ld = nd.n + static_cast<int64_t>(nd.S.size());
+        nd.frontOff = frontTotal_;
+        frontTotal_ += nd.ld * nd.n;
+        nd.eigOff = eigTotal_;
+        eigTotal_ += nd.n * nd.n;
+        nd.vecOff = vecTotal_;
+        vecTotal_ += nd.n;
+    }
+    // CSR destinations in the fronts
+    auto dstMap = [&](const int64_t* rp, const int32_t* ci, std::vector<int64_t>& out) {
+        out.assign(static_cast<size_t>(rp[n]), -1);
+        for (int64_t old = 0; old < n; ++old) {
+            const int64_t r = inv_[static_cast<size_t>(old)];
+            for (int64_t e = rp[old]; e < rp[old + 1]; ++e) {
+                const int64_t c = inv_[static_cast<size_t>(ci[e])];
+                const int a = owner_[static_cast<size_t>(c)];
+                const Node& A = nodes_[static_cast<size_t>(a)];
+                if (owner_[static_cast<size_t>(r)] == a) {
+                    out[static_cast<size_t>(e)] = A.frontOff + (r - A.off) + (c - A.off) * A.ld;
+                } else if (r > c) {
+                    auto it = std::lower_bound(A.S.begin(), A.S.end(), static_cast<int32_t>(r));
+                    if (it == A.S.end() || *it != r)
+                        throw AmlsError(AMLS_ERR_NUMERIC, "symbolic fill missed an entry");
+                    out[static_cast<size_t>(e)] =
+                        A.frontOff + A.n + (it - A.S.begin()) + (c - A.off) * A.ld;
+                }
+            }
+        }
+    };
+    dstMap(kp, kc, hostKDst_);
+    dstMap(mp, mc, hostMDst_);
+
+    // device: original M pattern (for the M-norms), maps
+    mRp_.ensure(sizeof(int64_t) * static_cast<size_t>(n + 1));
+    mCi_.ensure(sizeof(int32_t) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+    invDev_.ensure(sizeof(int64_t) * static_cast<size_t>(n));
+    permDev_.ensure(sizeof(int64_t) * static_cast<size_t>(n));
+    kDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzK_, 1)));
+    mDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+    cudaCheck(cudaMemcpyAsync(mRp_.as<int64_t>(), mp, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, stream_), "upload");
+    cudaCheck(cudaMemcpyAsync(mCi_.as<int32_t>(), mc, sizeof(int32_t) * nnzM_, cudaMemcpyHostToDevice, stream_), "upload");
+    cudaCheck(cudaMemcpyAsync(invDev_.as<int64_t>(), inv_.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, stream_), "upload");
+    cudaCheck(cudaMemcpyAsync(permDev_.as<int64_t>(), perm_.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, stream_), "upload");
+    cudaCheck(cudaMemcpyAsync(kDst_.as<int64_t>(), hostKDst_.data(), sizeof(int64_t) * nnzK_, cudaMemcpyHostToDevice, stream_), "upload");
+    cudaCheck(cudaMemcpyAsync(mDst_.as<int64_t>(), hostMDst_.data(), sizeof(int64_t) * nnzM_, cudaMemcpyHostToDevice, stream_), "upload");
+    kVal_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(nnzK_, 1)));
+    mVal_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+    kPool_.ensure(sizeof(double) * static_cast<size_t>(frontTotal_));
+    mPool_.ensure(sizeof(double) * static_cast<size_t>(frontTotal_));
+    eigPool_.ensure(sizeof(double) * static_cast<size_t>(eigTotal_));
+    dPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
+    ePool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
+    tauPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
+    buildStatic();
+    cudaCheck(cudaStreamSynchronize(stream_), "analyze");
+    analyzed_ = true;
+}
+
+void Engine::buildStatic() {
+    // ---- static int maps: extend-add (pmin, rowBase, rowIdx, colOff), panel rows, S ----
+    Blob ints;
+    std::vector<int32_t> pmin, rowBase, rowIdxAll, rowS, Sall;
+    std::vector<int64_t> colOff;
+    std::vector<int64_t> rowIdxStart(nodes_.size(), 0);
+    for (int i : order_) {
+        Node& nd = nodes_[static_cast<size_t>(i)];
+        const int64_t s = static_cast<int64_t>(nd.S.size());
+        nd.mapCol = static_cast<int64_t>(pmin.size());
+        nd.rowS = static_cast<int64_t>(rowS.size());
+        rowIdxStart[static_cast<size_t>(i)] = static_cast<int64_t>(rowIdxAll.size());
+        int64_t p = 0;
+        while (p < s) {
+            const int a = owner_[static_cast<size_t>(nd.S[static_cast<size_t>(p)])];
+            const Node& A = nodes_[static_cast<size_t>(a)];
+            int64_t p1 = p;
+            while (p1 < s && owner_[static_cast<size_t>(nd.S[static_cast<size_t>(p1)])] == a) ++p1;
+            const int64_t segOff = static_cast<int64_t>(rowIdxAll.size()) - rowIdxStart[static_cast<size_t>(i)];
+            for (int64_t pp = p; pp < s; ++pp) {
+                const int32_t d = nd.S[static_cast<size_t>(pp)];
+                if (pp < p1) {
+                    rowIdxAll.push_back(static_cast<int32_t>(d - A.off));
+                } else {
+                    auto it = std::lower_bound(A.S.begin(), A.S.end(), d);
+                    if (it == A.S.end() || *it != d)
+                        throw AmlsError(AMLS_ERR_NUMERIC, "symbolic fill is not closed");
+                    rowIdxAll.push_back(static_cast<int32_t>(A.n + (it - A.S.begin())));
+                }
+            }
+            for (int64_t q = p; q < p1; ++q) {
+                pmin.push_back(static_cast<int32_t>(p));
+                colOff.push_back(A.frontOff + (nd.S[static_cast<size_t>(q)] - A.off) * A.ld);
+                rowBase.push_back(static_cast<int32_t>(segOff - p));
+            }
+            p = p1;
+        }
+        for (int64_t q = 0; q < s; ++q) {
+            const int32_t d = nd.S[static_cast<size_t>(q)];
+            const Node& A = nodes_[static_cast<size_t>(owner_[static_cast<size_t>(d)])];
+            rowS.push_back(static_cast<int32_t>(A.pathPrefix + (d - A.off)));
+            Sall.push_back(d);
+        }
+    }
+    const size_t oPmin = ints.add(pmin), oRowBase = ints.add(rowBase), oRowIdx = ints.add(rowIdxAll),
+                 oRowS = ints.add(rowS), oS = ints.add(Sall), oColOff = ints.add(colOff);
+    ints.upload(staticInts_, stream_);
+    const int32_t* dPmin = ints.dev<int32_t>(oPmin);
+    const int32_t* dRowBase = ints.dev<int32_t>(oRowBase);
+    const int32_t* dRowIdx = ints.dev<int32_t>(oRowIdx);
+    const int64_t* dColOff = ints.dev<int64_t>(oColOff);
+    sIdxDev_ = ints.dev<int32_t>(oS);
+    rowSDev_ = ints.dev<int32_t>(oRowS);
+
+    // ---- level tables ----
+    sblob_.clear();
+    levelPlans_.assign(static_cast<size_t>(maxLevel_) + 1, LevelPlan());
+    double* kP = kPool_.as<double>();
+    double* mP = mPool_.as<double>();
+    double* eP = eigPool_.as<double>();
+    for (int l = 0; l <= maxLevel_; ++l) {
+        LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
+        std::vector<FrontDesc> fk, fm, fsym;
+        std::vector<TrsmDesc> td, cd;
+        std::vector<TileRef> tt, ct, copyT, rt, ut;
+        std::vector<CopyDesc> cp;
+        std::vector<GemmDesc> rg;
+        std::vector<FrontUpdDesc> ud;
+        int64_t maxN = 0, maxRows = 0;
+        for (int i : byLevel_[static_cast<size_t>(l)]) {
+            const Node& nd = nodes_[static_cast<size_t>(i)];
+            const int64_t s = static_cast<int64_t>(nd.S.size());
+            FrontDesc f{};
+            f.F = kP + nd.frontOff;
+            f.ld = nd.ld;
+            f.n = static_cast<int32_t>(nd.n);
+            f.rows = static_cast<int32_t>(nd.ld);
+            f.node = i;
+            fk.push_back(f);
+            f.F = mP + nd.frontOff;
+            fm.push_back(f);
+            FrontDesc fe{};
+            fe.F = eP + nd.eigOff;
+            fe.ld = nd.n;
+            fe.n = fe.rows = static_cast<int32_t>(nd.n);
+            fe.node = i;
+            fsym.push_back(fe);
+            maxN = std::max(maxN, nd.n);
+            maxRows = std::max(maxRows, nd.ld);
+            // G <- G L^-T (all n + s rows)
+            TrsmDesc t{};
+            t.L = kP + nd.frontOff;
+            t.ldl = nd.ld;
+            t.X = mP + nd.frontOff;
+            t.ldx = nd.ld;
+            t.n = static_cast<int32_t>(nd.n);
+            t.r = static_cast<int32_t>(nd.ld);
+            trsmTiles(tt, static_cast<int>(td.size()), nd.ld);
+            td.push_back(t);
+            // eig <- (G_ii L^-T)^T
+            CopyDesc c{};
+            c.in = mP + nd.frontOff;
+            c.ldin = nd.ld;
+            c.out = eP + nd.eigOff;
+            c.ldout = nd.n;
+            c.r = c.c = static_cast<int32_t>(nd.n);
+            copyTiles(copyT, static_cast<int>(cp.size()), nd.n, nd.n);
+            cp.push_back(c);
+            // eig <- eig L^-T  => C = L^-1 M^ L^-T
+            TrsmDesc t2{};
+            t2.L = kP + nd.frontOff;
+            t2.ldl = nd.ld;
+            t2.X = eP + nd.eigOff;
+            t2.ldx = nd.n;
+            t2.n = t2.r = static_cast<int32_t>(nd.n);
+            trsmTiles(ct, static_cast<int>(cd.size()), nd.n);
+            cd.push_back(t2);
+            if (s > 0) {
+                // R = Q - L_Si C / 2  (in place in the M front's lower block)
+                GemmDesc g = gemm(s, nd.n, nd.n, kAccumulate, kP + nd.frontOff + nd.n, nd.ld,
+                                  eP + nd.eigOff, nd.n, mP + nd.frontOff + nd.n, nd.ld, -0.5, 1.0);
+                gemmTiles(rt, static_cast<int>(rg.size()), s, nd.n);
+                rg.push_back(g);
+                FrontUpdDesc u{};
+                u.s = static_cast<int32_t>(s);
+                u.n = static_cast<int32_t>(nd.n);
+                u.A = kP + nd.frontOff + nd.n;
+                u.B = mP + nd.frontOff + nd.n;
+                u.ld = nd.ld;
+                u.pmin = dPmin + nd.mapCol;
+                u.colOff = dColOff + nd.mapCol;
+                u.rowIdx = dRowIdx + rowIdxStart[static_cast<size_t>(i)];
+                u.rowBase = dRowBase + nd.mapCol;
+                const int ud_i = static_cast<int>(ud.size());
+                for (int qt = 0; qt < cdiv(s, kT); ++qt) {
+                    int pm = static_cast<int>(s);
+                    for (int64_t q = qt * kT; q < std::min<int64_t>(s, (qt + 1) * kT); ++q)
+                        pm = std::min(pm, pmin[static_cast<size_t>(nd.mapCol + q)]);
+                    for (int pt = pm / kT; pt < cdiv(s, kT); ++pt) ut.push_back({ud_i, pt * kT, qt * kT, 0});
+                }
+                ud.push_back(u);
+            }
+        }
+        L.nFront = static_cast<int>(fk.size());
+        L.maxBlocks = cdiv(maxN, kCholBlock);
+        L.maxRowTiles = cdiv(maxRows, kTrsmRows);
+        L.frontK = sblob_.add(fk);
+        L.frontM = sblob_.add(fm);
+        L.symDesc = sblob_.add(fsym);
+        L.trsmDesc = sblob_.add(td);
+        L.trsmTiles = sblob_.add(tt);
+        L.nTrsmTiles = static_cast<int>(tt.size());
+        L.tDesc = sblob_.add(cp);
+        L.tTiles = sblob_.add(copyT);
+        L.nTTiles = static_cast<int>(copyT.size());
+        L.cDesc = sblob_.add(cd);
+        L.cTiles = sblob_.add(ct);
+        L.nCTiles = static_cast<int>(ct.size());
+        L.rDesc = sblob_.add(rg);
+        L.rTiles = sblob_.add(rt);
+        L.nRTiles = static_cast<int>(rt.size());
+        L.uDesc = sblob_.add(ud);
+        L.uTiles = sblob_.add(ut);
+        L.nUTiles = static_cast<int>(ut.size());
+    }
+    sblob_.upload(staticBlob_, stream_);
+
+    // ---- ledger: elimination flops/bytes ----
+    double fe = 0, be = 0;
+    for (const Node& nd : nodes_) {
+        const double nn = static_cast<double>(nd.n), s = static_cast<double>(nd.S.size());
+        fe += nn * nn * nn / 3.0 + s * nn * nn;          // partial Cholesky
+        fe += (nn + s) * nn * nn;                        // G <- G L^-T
+        fe += nn * nn * nn;                              // C = L^-1 (.)
+        fe += 2.0 * s * nn * nn;                         // R
+        fe += 3.0 * s * s * nn;                          // UK (s^2 n) + UM (2 s^2 n), lower half x2
+        be += 8.0 * (2.0 * (nn + s) * nn + nn * nn) * 2.0 + 8.0 * s * s;   // fronts r/w + updates
+    }
+    work_[0] = fe;
+    work_[1] = be;
+}
+
+// ---------------------------------------------------------------------------
+// elimination
+// ---------------------------------------------------------------------------
+void Engine::eliminate(cudaStream_t s) {
+    int* st = status_.as<int>();
+    for (int l = 0; l <= maxLevel_; ++l) {
+        const LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
+        const FrontDesc* fk = sblob_.dev<FrontDesc>(L.frontK);
+        for (int jb = 0; jb < L.maxBlocks; ++jb) {
+            LAUNCH(launchCholDiag(fk, L.nFront, jb, st, s));
+            LAUNCH(launchCholPanel(fk, L.nFront, jb, L.maxRowTiles, s));
+        }
+        LAUNCH(launchTrsmRows(sblob_.dev<TrsmDesc>(L.trsmDesc), sblob_.dev<TileRef>(L.trsmTiles),
+                              L.nTrsmTiles, s));
+        LAUNCH(launchTransposeBatched(sblob_.dev<CopyDesc>(L.tDesc), sblob_.dev<TileRef>(L.tTiles),
+                                      L.nTTiles, s));
+        LAUNCH(launchTrsmRows(sblob_.dev<TrsmDesc>(L.cDesc), sblob_.dev<TileRef>(L.cTiles),
+                              L.nCTiles, s));
+        LAUNCH(launchSymmetrize(sblob_.dev<FrontDesc>(L.symDesc), L.nFront, s));
+        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.rDesc), sblob_.dev<TileRef>(L.rTiles),
+                                 L.nRTiles, s));
+        LAUNCH(launchFrontUpdate(sblob_.dev<FrontUpdDesc>(L.uDesc), sblob_.dev<TileRef>(L.uTiles),
+                                 L.nUTiles, kPool_.as<double>(), mPool_.as<double>(), s));
+    }
+}
+
+void Engine::checkStatus(const char* phase) {
+    int h[2] = {0, 0};
+    cudaCheck(cudaMemcpyAsync(h, status_.as<int>(), sizeof(h), cudaMemcpyDeviceToHost, stream_), "status");
+    cudaCheck(cudaStreamSynchronize(stream_), phase);
+    if (h[0] == kDevNotSpd)
+        throw AmlsError(AMLS_ERR_NOT_SPD, std::string(phase) + ": non-positive pivot at tree node " +
+                                              std::to_string(h[1]) +
+                                              " (input outside the SPD range; shift K)");
+    if (h[0] == kDevIterCap)
+        throw AmlsError(AMLS_ERR_ITERATION, std::string(phase) + ": iteration cap at " + std::to_string(h[1]));
+}
+
+// ---------------------------------------------------------------------------
+// eigen driver
+// ---------------------------------------------------------------------------
+void Engine::tridiagonalizeAll(cudaStream_t s) {
+    std::vector<EigDesc> small, large;
+    int maxLargeN = 0;
+    for (int i : order_) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        if (nd.n == 0) continue;
+        EigDesc e{};
+        e.A = eigPool_.as<double>() + nd.eigOff;
+        e.lda = nd.n;
+        e.d = dPool_.as<double>() + nd.vecOff;
+        e.e = ePool_.as<double>() + nd.vecOff;
+        e.tau = tauPool_.as<double>() + nd.vecOff;
+        e.n = static_cast<int32_t>(nd.n);
+        e.id = i;
+        if (nd.n <= kSmallEig) small.push_back(e);
+        else {
+            large.push_back(e);
+            maxLargeN = std::max<int>(maxLargeN, static_cast<int>(nd.n));
+        }
+    }
+    Blob b;
+    const size_t oS = b.add(small), oL = b.add(large);
+    // group table for the cooperative launch
+    std::vector<int> groupOf, groupFirst, groupSize;
+    std::vector<int64_t> pOff;
+    int64_t pTot = 0;
+    if (!large.empty()) {
+        const int maxCta = tridiagLargeMaxCtas(maxLargeN);
+        double wsum = 0;
+        for (auto& e : large) wsum += static_cast<double>(e.n) * e.n;
+        int used = 0;
+        for (size_t g = 0; g < large.size(); ++g) {
+            int cnt = std::max(1, static_cast<int>(std::floor(maxCta * (static_cast<double>(large[g].n) * large[g].n) / wsum)));
+            cnt = std::min(cnt, maxCta - used - static_cast<int>(large.size() - g - 1));
+            cnt = std::max(cnt, 1);
+            groupFirst.push_back(used);
+            groupSize.push_back(cnt);
+            for (int c = 0; c < cnt; ++c) groupOf.push_back(static_cast<int>(g));
+            used += cnt;
+            pOff.push_back(pTot);
+            pTot += large[g].n;
+        }
+        if (used > maxCta) throw AmlsError(AMLS_ERR_CUDA, "too many large eigenproblems for one cooperative launch");
+    }
+    const size_t oGo = b.add(groupOf), oGf = b.add(groupFirst), oGs = b.add(groupSize), oPo = b.add(pOff);
+    b.upload(tlBlob_, s);
+    if (!small.empty()) LAUNCH(launchTridiagSmall(b.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
+    if (!large.empty()) {
+        redP_.ensure(sizeof(double) * static_cast<size_t>(pTot));
+        LAUNCH(launchTridiagLargeGroups(b.dev<EigDesc>(oL), b.dev<int>(oGo), b.dev<int>(oGf),
+                                        b.dev<int>(oGs), static_cast<int>(groupOf.size()),
+                                        redP_.as<double>(), b.dev<int64_t>(oPo), maxLargeN, s));
+    }
+    // keep the blob alive until the work is done
+    cudaCheck(cudaStreamSynchronize(s), "tridiagonalise");
+    tridiagDone_ = true;
+}
+
+// modes: 0 = index (the `want` largest nu), 1 = interval (nu >= thr)
+void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
+    const int N = static_cast<int>(nodes_.size());
+    if (!tridiagDone_) tridiagonalizeAll(s);
+    // ---- counts ----
+    P.k.assign(static_cast<size_t>(N), 0);
+    kOutDev_.ensure(sizeof(int32_t) * static_cast<size_t>(N));
+    std::vector<EigDesc> descs(static_cast<size_t>(N));
+    for (int i = 0; i < N; ++i) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        EigDesc e{};
+        e.A = eigPool_.as<double>() + nd.eigOff;
+        e.lda = std::max<int64_t>(nd.n, 1);
+        e.d = dPool_.as<double>() + nd.vecOff;
+        e.e = ePool_.as<double>() + nd.vecOff;
+        e.tau = tauPool_.as<double>() + nd.vecOff;
+        e.n = static_cast<int32_t>(nd.n);
+        e.id = i;
+        e.kOut = kOutDev_.as<int32_t>() + i;
+        e.kcap = (mode == 0) ? static_cast<int32_t>(std::min<int64_t>(want, nd.n)) : static_cast<int32_t>(nd.n);
+        descs[static_cast<size_t>(i)] = e;
+    }
+    {
+        Blob b;
+        const size_t o = b.add(descs);
+        b.upload(passBlob_, s);
+        LAUNCH(launchBisect(b.dev<EigDesc>(o), N, mode == 0 ? 0 : 1, want, thr, 0, nullptr, s));
+        std::vector<int32_t> kh(static_cast<size_t>(N));
+        cudaCheck(cudaMemcpyAsync(kh.data(), kOutDev_.as<int32_t>(), sizeof(int32_t) * N, cudaMemcpyDeviceToHost, s), "k");
+        cudaCheck(cudaStreamSynchronize(s), "counts");
+        for (int i = 0; i < N; ++i) P.k[static_cast<size_t>(i)] = kh[static_cast<size_t>(i)];
+    }
+    // ---- offsets, buffers ----
+    P.projOff.assign(static_cast<size_t>(N), 0);
+    int64_t p = 0, ysz = 0, wsz = 0;
+    yOff_.assign(static_cast<size_t>(N), 0);
+    int maxK = 0;
+    for (int i = 0; i < N; ++i) {
+        P.projOff[static_cast<size_t>(i)] = p;     // by node id, as the reference's finalize
+        p += P.k[static_cast<size_t>(i)];
+        yOff_[static_cast<size_t>(i)] = ysz;
+        ysz += nodes_[static_cast<size_t>(i)].n * P.k[static_cast<size_t>(i)];
+        wsz += 6 * nodes_[static_cast<size_t>(i)].n * P.k[static_cast<size_t>(i)];
+        maxK = std::max(maxK, P.k[static_cast<size_t>(i)]);
+    }
+    P.p = p;
+    if (p <= 0) throw AmlsError(AMLS_ERR_NUMERIC, "reduced problem is empty (all nodes truncated)");
+    yPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(ysz, 1)));
+    wPool_.ensure(sizeof(double) * static_cast<size_t>(p));
+    iiWork_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(wsz, 1)));
+    int64_t workOff = 0;
+    for (int i = 0; i < N; ++i) {
+        EigDesc& e = descs[static_cast<size_t>(i)];
+        e.kcap = P.k[static_cast<size_t>(i)];
+        e.w = wPool_.as<double>() + P.projOff[static_cast<size_t>(i)];
+        e.Y = yPool_.as<double>() + yOff_[static_cast<size_t>(i)];
+        e.ldy = std::max<int64_t>(nodes_[static_cast<size_t>(i)].n, 1);
+        e.work = iiWork_.as<double>() + workOff;
+        workOff += 6 * nodes_[static_cast<size_t>(i)].n * P.k[static_cast<size_t>(i)];
+    }
+
+    // ---- projection tables (all levels) ----
+    const double* F = kPool_.as<double>();
+    const double* G = mPool_.as<double>();
+    // panels
+    panelOff_.assign(static_cast<size_t>(N), -1);
+    int64_t panelTot = 0;
+    for (int i = 0; i < N; ++i) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        if (!nd.anc.empty() && P.k[static_cast<size_t>(i)] > 0) {
+            panelOff_[static_cast<size_t>(i)] = panelTot;
+            panelTot += nd.pathPrefix * P.k[static_cast<size_t>(i)];
+        }
+    }
+    panelPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(panelTot, 1)));
+    credPool_.ensure(sizeof(double) * static_cast<size_t>(p * p));
+    double* panel = panelPool_.as<double>();
+    double* cred = credPool_.as<double>();
+    // descendants with k > 0, in post-order, per node; Wt sizes
+    std::vector<int> pos(static_cast<size_t>(N));
+    for (size_t t = 0; t < order_.size(); ++t) pos[static_cast<size_t>(order_[t])] = static_cast<int>(t);
+    std::vector<std::vector<int>> descK(static_cast<size_t>(N));
+    for (int kk = 0; kk < N; ++kk) {
+        if (P.k[static_cast<size_t>(kk)] <= 0) continue;
+        for (int a : nodes_[static_cast<size_t>(kk)].anc) descK[static_cast<size_t>(a)].push_back(kk);
+    }
+    std::vector<int64_t> wtOff(static_cast<size_t>(N), 0), Ksum(static_cast<size_t>(N), 0);
+    int64_t wtTot = 0;
+    for (int i = 0; i < N; ++i) {
+        auto& D = descK[static_cast<size_t>(i)];
+        std::sort(D.begin(), D.end(), [&](int x, int y) { return pos[static_cast<size_t>(x)] < pos[static_cast<size_t>(y)]; });
+        for (int kk : D) Ksum[static_cast<size_t>(i)] += P.k[static_cast<size_t>(kk)];
+        wtOff[static_cast<size_t>(i)] = wtTot;
+        wtTot += Ksum[static_cast<size_t>(i)] * nodes_[static_cast<size_t>(i)].n;
+    }
+    wtPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(wtTot, 1)));
+    double* wt = wtPool_.as<double>();
+    const double* Y = yPool_.as<double>();
+
+    Blob b;
+    const size_t oDescs = b.add(descs);
+    // per-node index arrays for the scatters (own blob, uploaded first so the
+    // GEMM descriptors can point into it)
+    std::vector<int32_t> descRowIdx, nodeRowIdx;
+    std::vector<int64_t> descColOff, nodeColOff, panelColOff, initColOff;
+    std::vector<int64_t> oDescRow(static_cast<size_t>(N)), oDescCol(static_cast<size_t>(N)),
+        oNodeRow(static_cast<size_t>(N)), oNodeCol(static_cast<size_t>(N)),
+        oPanelCol(static_cast<size_t>(N)), oInitCol(static_cast<size_t>(N));
+    for (int i = 0; i < N; ++i) {
+        oDescRow[static_cast<size_t>(i)] = static_cast<int64_t>(descRowIdx.size());
+        oDescCol[static_cast<size_t>(i)] = static_cast<int64_t>(descColOff.size());
+        oPanelCol[static_cast<size_t>(i)] = static_cast<int64_t>(panelColOff.size());
+        for (int kk : descK[static_cast<size_t>(i)]) {
+            const int64_t pk = P.projOff[static_cast<size_t>(kk)];
+            for (int bcol = 0; bcol < P.k[static_cast<size_t>(kk)]; ++bcol) {
+                descRowIdx.push_back(static_cast<int32_t>(pk + bcol));
+                descColOff.push_back((pk + bcol) * p);
+                panelColOff.push_back(panelOff_[static_cast<size_t>(kk)] + bcol * nodes_[static_cast<size_t>(kk)].pathPrefix);
+            }
+        }
+        oNodeRow[static_cast<size_t>(i)] = static_cast<int64_t>(nodeRowIdx.size());
+        oNodeCol[static_cast<size_t>(i)] = static_cast<int64_t>(nodeColOff.size());
+        oInitCol[static_cast<size_t>(i)] = static_cast<int64_t>(initColOff.size());
+        const int64_t pi = P.projOff[static_cast<size_t>(i)];
+        for (int a = 0; a < P.k[static_cast<size_t>(i)]; ++a) {
+            nodeRowIdx.push_back(static_cast<int32_t>(pi + a));
+            nodeColOff.push_back((pi + a) * p);
+            initColOff.push_back(panelOff_[static_cast<size_t>(i)] + a * nodes_[static_cast<size_t>(i)].pathPrefix);
+        }
+    }
+    struct LevelTabs {
+        size_t cpD, cpT, trD, trT, g1D, g1T, g2D, g2T, midD, midT, i1D, i1T, i2D, i2T;
+        int ncpT, ntrT, ng1T, ng2T, nmidT, ni1T, ni2T;
+    };
+    std::vector<LevelTabs> tabs(static_cast<size_t>(maxLevel_) + 1);
+    Blob idx;
+    const size_t xDR = idx.add(descRowIdx), xDC = idx.add(descColOff), xNR = idx.add(nodeRowIdx),
+                 xNC = idx.add(nodeColOff), xPC = idx.add(panelColOff), xIC = idx.add(initColOff);
+    idx.upload(idxBlob_, s);
+    const int32_t* dDR = idx.dev<int32_t>(xDR);
+    const int64_t* dDC = idx.dev<int64_t>(xDC);
+    const int32_t* dNR = idx.dev<int32_t>(xNR);
+    const int64_t* dNC = idx.dev<int64_t>(xNC);
+    const int64_t* dPC = idx.dev<int64_t>(xPC);
+    const int64_t* dIC = idx.dev<int64_t>(xIC);
+    const double* wDev = wPool_.as<double>();
+
+    double fc = 0, bc = 0;
+    for (int l = 0; l <= maxLevel_; ++l) {
+        std::vector<CopyDesc> cp;
+        std::vector<TrsmDesc> tr;
+        std::vector<GemmDesc> g1, g2, mid, i1, i2;
+        std::vector<TileRef> cpT, trT, g1T, g2T, midT, i1T, i2T;
+        for (int i : byLevel_[static_cast<size_t>(l)]) {
+            const Node& nd = nodes_[static_cast<size_t>(i)];
+            const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
+            const int64_t Ki = Ksum[static_cast<size_t>(i)];
+            const int ki = P.k[static_cast<size_t>(i)];
+            double* wti = wt + wtOff[static_cast<size_t>(i)];
+            const double* Yi = Y + yOff_[static_cast<size_t>(i)];
+            if (Ki > 0 && ni > 0) {
+                int64_t colPos = 0;
+                for (int kk : descK[static_cast<size_t>(i)]) {
+                    const Node& nk = nodes_[static_cast<size_t>(kk)];
+                    CopyDesc c{};
+                    c.in = panel + panelOff_[static_cast<size_t>(kk)] + nd.pathPrefix;
+                    c.ldin = nk.pathPrefix;
+                    c.out = wti + colPos;
+                    c.ldout = Ki;
+                    c.r = static_cast<int32_t>(ni);
+                    c.c = P.k[static_cast<size_t>(kk)];
+                    copyTiles(cpT, static_cast<int>(cp.size()), ni, c.c);
+                    cp.push_back(c);
+                    colPos += c.c;
+                }
+                TrsmDesc t{};
+                t.L = F + nd.frontOff;
+                t.ldl = nd.ld;
+                t.X = wti;
+                t.ldx = Ki;
+                t.n = static_cast<int32_t>(ni);
+                t.r = static_cast<int32_t>(Ki);
+                trsmTiles(trT, static_cast<int>(tr.size()), Ki);
+                tr.push_back(t);
+                fc += static_cast<double>(Ki) * ni * ni;
+                if (ki > 0) {
+                    GemmDesc a = gemm(ki, Ki, ni, kTransA | kTransB | kScatter, Yi, ni, wti, Ki, cred, p, 1.0, 0.0);
+                    a.rowIdx = dNR + oNodeRow[static_cast<size_t>(i)];
+                    a.colOff = dDC + oDescCol[static_cast<size_t>(i)];
+                    gemmTiles(g1T, static_cast<int>(g1.size()), ki, Ki);
+                    g1.push_back(a);
+                    GemmDesc a2 = gemm(Ki, ki, ni, kScatter, wti, Ki, Yi, ni, cred, p, 1.0, 0.0);
+                    a2.rowIdx = dDR + oDescRow[static_cast<size_t>(i)];
+                    a2.colOff = dNC + oNodeCol[static_cast<size_t>(i)];
+                    gemmTiles(g2T, static_cast<int>(g2.size()), Ki, ki);
+                    g2.push_back(a2);
+                    fc += 4.0 * ki * Ki * ni;
+                }
+                if (si > 0) {
+                    GemmDesc m = gemm(si, Ki, ni, kTransB | kScatter | kAccumulate, F + nd.frontOff + ni, nd.ld,
+                                      wti, Ki, panel, 0, -1.0, 0.0);
+                    m.rowIdx = rowSDev_ + nd.rowS;
+                    m.colOff = dPC + oPanelCol[static_cast<size_t>(i)];
+                    gemmTiles(midT, static_cast<int>(mid.size()), si, Ki);
+                    mid.push_back(m);
+                    fc += 2.0 * si * Ki * ni;
+                }
+            }
+            if (ki > 0 && si > 0 && panelOff_[static_cast<size_t>(i)] >= 0) {
+                GemmDesc a = gemm(si, ki, ni, kScatter, G + nd.frontOff + ni, nd.ld, Yi, ni, panel, 0, 1.0, 0.0);
+                a.rowIdx = rowSDev_ + nd.rowS;
+                a.colOff = dIC + oInitCol[static_cast<size_t>(i)];
+                gemmTiles(i1T, static_cast<int>(i1.size()), si, ki);
+                i1.push_back(a);
+                GemmDesc a2 = gemm(si, ki, ni, kScatter | kAccumulate | kColScale, F + nd.frontOff + ni, nd.ld, Yi,
+                                   ni, panel, 0, -0.5, 0.0);
+                a2.rowIdx = rowSDev_ + nd.rowS;
+                a2.colOff = dIC + oInitCol[static_cast<size_t>(i)];
+                a2.colScale = wDev + P.projOff[static_cast<size_t>(i)];
+                gemmTiles(i2T, static_cast<int>(i2.size()), si, ki);
+                i2.push_back(a2);
+                fc += 4.0 * si * ki * ni;
+            }
+            bc += 8.0 * (static_cast<double>(Ki) * ni * 3 + si * (Ki + ki) * 2);
+        }
+        LevelTabs& T = tabs[static_cast<size_t>(l)];
+        T.cpD = b.add(cp); T.cpT = b.add(cpT); T.ncpT = static_cast<int>(cpT.size());
+        T.trD = b.add(tr); T.trT = b.add(trT); T.ntrT = static_cast<int>(trT.size());
+        T.g1D = b.add(g1); T.g1T = b.add(g1T); T.ng1T = static_cast<int>(g1T.size());
+        T.g2D = b.add(g2); T.g2T = b.add(g2T); T.ng2T = static_cast<int>(g2T.size());
+        T.midD = b.add(mid); T.midT = b.add(midT); T.nmidT = static_cast<int>(midT.size());
+        T.i1D = b.add(i1); T.i1T = b.add(i1T); T.ni1T = static_cast<int>(i1T.size());
+        T.i2D = b.add(i2); T.i2T = b.add(i2T); T.ni2T = static_cast<int>(i2T.size());
+    }
+    b.upload(passBlob_, s);
+
+    // ---- local eigenpairs (largest nu of C_i) ----
+    const EigDesc* dd = b.dev<EigDesc>(oDescs);
+    LAUNCH(launchBisect(dd, N, mode == 0 ? 0 : 1, want, thr, maxK, nullptr, s));
+    LAUNCH(launchInverseIter(dd, N, maxK, nullptr, s));
+    LAUNCH(launchBackTransform(dd, N, maxK, s));
+
+    // ---- projection ----
+    LAUNCH(launchZero(panel, panelTot, s));
+    LAUNCH(launchZero(cred, p * p, s));
+    LAUNCH(launchSetDiagonal(cred, wDev, p, s));
+    for (int l = 0; l <= maxLevel_; ++l) {
+        const LevelTabs& T = tabs[static_cast<size_t>(l)];
+        LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(T.cpD), b.dev<TileRef>(T.cpT), T.ncpT, s));
+        LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.trD), b.dev<TileRef>(T.trT), T.ntrT, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.ng1T, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.ng2T, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.midD), b.dev<TileRef>(T.midT), T.nmidT, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i1D), b.dev<TileRef>(T.i1T), T.ni1T, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i2D), b.dev<TileRef>(T.i2T), T.ni2T, s));
+    }
+    // ledger (local eig: bisection + inverse iteration + back-transform)
+    for (int i = 0; i < N; ++i) {
+        const double nn = static_cast<double>(nodes_[static_cast<size_t>(i)].n), kk = P.k[static_cast<size_t>(i)];
+        fc += 4.0 * nn * nn * kk;
+    }
+    work_[2] += fc;
+    work_[3] += bc;
+    cudaCheck(cudaStreamSynchronize(s), "condense");
+}
+
+// largest `want` eigenpairs of the reduced matrix; fills P.theta ascending
+int Engine::reducedSolve(Pass& P, int want, cudaStream_t s) {
+    const int64_t p = P.p;
+    want = static_cast<int>(std::min<int64_t>(want, p));
+    redD_.ensure(sizeof(double) * static_cast<size_t>(p));
+    redE_.ensure(sizeof(double) * static_cast<size_t>(p));
+    redTau_.ensure(sizeof(double) * static_cast<size_t>(p));
+    redW_.ensure(sizeof(double) * static_cast<size_t>(want));
+    redY_.ensure(sizeof(double) * static_cast<size_t>(p * want));
+    redWork_.ensure(sizeof(double) * static_cast<size_t>(6 * p * want));
+    redK_.ensure(sizeof(int32_t) * 4);
+    EigDesc e{};
+    e.A = credPool_.as<double>();
+    e.lda = p;
+    e.d = redD_.as<double>();
+    e.e = redE_.as<double>();
+    e.tau = redTau_.as<double>();
+    e.n = static_cast<int32_t>(p);
+    e.id = -1;
+    e.w = redW_.as<double>();
+    e.Y = redY_.as<double>();
+    e.ldy = p;
+    e.kcap = want;
+    e.kOut = redK_.as<int32_t>();
+    e.work = redWork_.as<double>();
+    Blob b;
+    const size_t o = b.add(&e, 1);
+    std::vector<int> gOf, gFirst{0}, gSize;
+    std::vector<int64_t> pOff{0};
+    int nCta = 0;
+    if (p > kSmallEig) {
+        nCta = tridiagLargeMaxCtas(static_cast<int>(p));
+        gOf.assign(static_cast<size_t>(nCta), 0);
+        gSize.push_back(nCta);
+    }
+    const size_t oGo = b.add(gOf), oGf = b.add(gFirst), oGs = b.add(gSize), oPo = b.add(pOff);
+    b.upload(redBlob_, s);
+    const EigDesc* dd = b.dev<EigDesc>(o);
+    if (p <= kSmallEig) LAUNCH(launchTridiagSmall(dd, 1, s));
+    else {
+        redP_.ensure(sizeof(double) * static_cast<size_t>(p));
+        LAUNCH(launchTridiagLargeGroups(dd, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
+                                        redP_.as<double>(), b.dev<int64_t>(oPo), static_cast<int>(p), s));
+    }
+    LAUNCH(launchBisect(dd, 1, 0, want, 0.0, want, nullptr, s));
+    LAUNCH(launchInverseIter(dd, 1, want, nullptr, s));
+    LAUNCH(launchBackTransform(dd, 1, want, s));
+    std::vector<double> nu(static_cast<size_t>(want));
+    cudaCheck(cudaMemcpyAsync(nu.data(), redW_.as<double>(), sizeof(double) * want, cudaMemcpyDeviceToHost, s), "theta");
+    cudaCheck(cudaStreamSynchronize(s), "reduced");
+    P.theta.resize(static_cast<size_t>(want));
+    for (int j = 0; j < want; ++j) P.theta[static_cast<size_t>(j)] = 1.0 / nu[static_cast<size_t>(j)];
+    const double pp = static_cast<double>(p);
+    work_[4] += 4.0 / 3.0 * pp * pp * pp + 4.0 * pp * pp * want;
+    work_[5] += 8.0 * pp * pp * pp / 3.0;
+    return want;
+}
+
+void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
+    const int N = static_cast<int>(nodes_.size());
+    ztPool_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
+    sqrtTheta_.ensure(sizeof(double) * static_cast<size_t>(m));
+    std::vector<double> st(static_cast<size_t>(m));
+    for (int j = 0; j < m; ++j) st[static_cast<size_t>(j)] = std::sqrt(P.theta[static_cast<size_t>(j)]);
+    cudaCheck(cudaMemcpyAsync(sqrtTheta_.as<double>(), st.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s), "sqrt theta");
+    double* zt = ztPool_.as<double>();
+    const double* F = kPool_.as<double>();
+    const double* Y = yPool_.as<double>();
+    const double* V = redY_.as<double>();
+    Blob b;
+    struct Tabs { size_t g1D, g1T, g2D, g2T, tD, tT; int n1, n2, nt; };
+    std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
+    double fb = 0;
+    for (int l = maxLevel_; l >= 0; --l) {
+        std::vector<GemmDesc> g1, g2;
+        std::vector<TrsmDesc> tr;
+        std::vector<TileRef> g1T, g2T, tT;
+        for (int i : byLevel_[static_cast<size_t>(l)]) {
+            const Node& nd = nodes_[static_cast<size_t>(i)];
+            const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
+            const int ki = P.k[static_cast<size_t>(i)];
+            if (ni == 0) continue;
+            double* zi = zt + nd.off * m;
+            GemmDesc a = gemm(m, ni, ki, kTransA | kTransB | kRowScale, V + P.projOff[static_cast<size_t>(i)], P.p,
+                              Y + yOff_[static_cast<size_t>(i)], std::max<int64_t>(ni, 1), zi, m, 1.0, 0.0);
+            a.rowScale = sqrtTheta_.as<double>();
+            gemmTiles(g1T, static_cast<int>(g1.size()), m, ni);
+            g1.push_back(a);
+            if (si > 0) {
+                GemmDesc c = gemm(m, ni, si, kGatherA | kAccumulate, zt, m, F + nd.frontOff + ni, nd.ld, zi, m, -1.0, 1.0);
+                c.aMap = sIdxDev_ + nd.mapCol;
+                gemmTiles(g2T, static_cast<int>(g2.size()), m, ni);
+                g2.push_back(c);
+            }
+            TrsmDesc t{};
+            t.L = F + nd.frontOff;
+            t.ldl = nd.ld;
+            t.X = zi;
+            t.ldx = m;
+            t.n = static_cast<int32_t>(ni);
+            t.r = m;
+            t.backward = 1;
+            trsmTiles(tT, static_cast<int>(tr.size()), m);
+            tr.push_back(t);
+            fb += 2.0 * m * ni * (ki + si) + static_cast<double>(m) * ni * ni;
+        }
+        Tabs& T = tabs[static_cast<size_t>(l)];
+        T.g1D = b.add(g1); T.g1T = b.add(g1T); T.n1 = static_cast<int>(g1T.size());
+        T.g2D = b.add(g2); T.g2T = b.add(g2T); T.n2 = static_cast<int>(g2T.size());
+        T.tD = b.add(tr); T.tT = b.add(tT); T.nt = static_cast<int>(tT.size());
+    }
+    (void)N;
+    b.upload(passBlob_, s);
+    for (int l = maxLevel_; l >= 0; --l) {
+        const Tabs& T = tabs[static_cast<size_t>(l)];
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.n1, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
+        LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
+    }
+    // M-normalise and un-permute
+    norms_.ensure(sizeof(double) * static_cast<size_t>(m));
+    zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
+    LAUNCH(launchMNorm(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n_, invDev_.as<int64_t>(), zt, m,
+                       norms_.as<double>(), s));
+    LAUNCH(launchUnpermute(zt, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
+    work_[6] += fb + 4.0 * static_cast<double>(nnzM_) * m;
+    work_[7] += 8.0 * (2.0 * m * n_ * 3 + 12.0 * nnzM_);
+    cudaCheck(cudaStreamSynchronize(s), "backtransform");
+}
+
+// ---------------------------------------------------------------------------
+// numeric solve
+// ---------------------------------------------------------------------------
+void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
+                         double* Z, bool outputsOnDevice, int64_t* pOut, double* timing) {
+    if (!analyzed_) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_solve_values before amls_analyze");
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    if (opt_.nev <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
+    const int64_t nev = std::min<int64_t>(opt_.nev, n_);
+    cudaStream_t s = stream_;
+    launches_ = 0;
+    for (int t = 2; t < AMLS_WORK_SLOTS; ++t) work_[t] = 0;
+    tridiagDone_ = false;
+    const auto t0 = Clock::now();
+    cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
+    if (valuesOnDevice) {
+        cudaCheck(cudaMemcpyAsync(kVal_.as<double>(), kv, sizeof(double) * nnzK_, cudaMemcpyDeviceToDevice, s), "values");
+        cudaCheck(cudaMemcpyAsync(mVal_.as<double>(), mv, sizeof(double) * nnzM_, cudaMemcpyDeviceToDevice, s), "values");
+    } else {
+        cudaCheck(cudaMemcpyAsync(kVal_.as<double>(), kv, sizeof(double) * nnzK_, cudaMemcpyHostToDevice, s), "values");
+        cudaCheck(cudaMemcpyAsync(mVal_.as<double>(), mv, sizeof(double) * nnzM_, cudaMemcpyHostToDevice, s), "values");
+    }
+    cudaCheck(cudaStreamSynchronize(s), "upload");
+    const auto t1 = Clock::now();
+    // assemble fronts
+    LAUNCH(launchZero(kPool_.as<double>(), frontTotal_, s));
+    LAUNCH(launchZero(mPool_.as<double>(), frontTotal_, s));
+    LAUNCH(launchScatterAdd(kVal_.as<double>(), kDst_.as<int64_t>(), nnzK_, 1.0, kPool_.as<double>(), s));
+    if (opt_.shift != 0.0)
+        LAUNCH(launchScatterAdd(mVal_.as<double>(), mDst_.as<int64_t>(), nnzM_, opt_.shift, kPool_.as<double>(), s));
+    LAUNCH(launchScatterAdd(mVal_.as<double>(), mDst_.as<int64_t>(), nnzM_, 1.0, mPool_.as<double>(), s));
+    eliminate(s);
+    checkStatus("elimination");
+    const auto t2 = Clock::now();
+    double tRed = 0;
+    Pass P;
+    const int N = static_cast<int>(nodes_.size());
+    if (opt_.fixedKeep > 0) {
+        condense(0, static_cast<int>(opt_.fixedKeep), 0.0, P, s);
+        pA_ = P.p;
+    } else {
+        if (!opt_.twoPass)
+            throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "twoPass=false with fixedKeep=0 cannot set the cut");
+        const int64_t k0 = std::max<int64_t>(4, (3 * nev + N - 1) / N);
+        Pass A;
+        condense(0, static_cast<int>(k0), 0.0, A, s);
+        pA_ = A.p;
+        const auto ta = Clock::now();
+        const int got = reducedSolve(A, static_cast<int>(std::min<int64_t>(nev, A.p)), s);
+        tRed += secs(ta, Clock::now());
+        if (got < nev)
+            throw AmlsError(AMLS_ERR_NUMERIC, "pass A reduced problem too small (p < nev); reduce nLevels or grow leafSize");
+        const double lambdaHat = A.theta[static_cast<size_t>(nev - 1)];
+        const double lambdaCut = opt_.thresholdFactor * lambdaHat;
+        if (opt_.verbosity > 0)
+            std::fprintf(stderr, "[amls_b200] pass A: p0=%lld lambda_hat=%.10g lambda_cut=%.10g\n",
+                         static_cast<long long>(A.p), lambdaHat, lambdaCut);
+        // keep mu <= lambda_cut  <=>  nu >= 1 / lambda_cut (all local mu > 0)
+        const double thr = lambdaCut > 0 ? 1.0 / lambdaCut : 1e300;
+        condense(1, 0, thr, P, s);
+    }
+    const auto t3 = Clock::now();
+    pFinal_ = P.p;
+    if (P.p > opt_.denseProjectedMax && opt_.verbosity > 0)
+        std::fprintf(stderr, "[amls_b200] warning: p=%lld exceeds denseProjectedMax=%lld (dense solve used)\n",
+                     static_cast<long long>(P.p), static_cast<long long>(opt_.denseProjectedMax));
+    const int want = reducedSolve(P, static_cast<int>(std::min<int64_t>(nev, P.p)), s);
+    const auto t4 = Clock::now();
+    tRed += secs(t3, t4);
+    const bool recover = opt_.recoverVectors && Z != nullptr;
+    if (recover) backtransform(P, want, s);
+    const auto t5 = Clock::now();
+    // outputs
+    if (outputsOnDevice) {
+        cudaCheck(cudaMemcpyAsync(theta, P.theta.data(), sizeof(double) * want, cudaMemcpyHostToDevice, s), "theta");
+        if (recover)
+            cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * want * n_, cudaMemcpyDeviceToDevice, s), "Z");
+    } else {
+        std::copy(P.theta.begin(), P.theta.end(), theta);
+        if (recover)
+            cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * want * n_, cudaMemcpyDeviceToHost, s), "Z");
+    }
+    cudaCheck(cudaStreamSynchronize(s), "outputs");
+    const auto t6 = Clock::now();
+    if (pOut) *pOut = P.p;
+    if (timing) {
+        timing[AMLS_T_UPLOAD] = secs(t0, t1);
+        timing[AMLS_T_ELIMINATION] = secs(t1, t2);
+        timing[AMLS_T_CONDENSE] = secs(t2, t3) - (tRed - secs(t3, t4));
+        timing[AMLS_T_REDUCED] = tRed;
+        timing[AMLS_T_BACKTRANSFORM] = secs(t4, t5) + secs(t5, t6);
+        timing[AMLS_T_TOTAL] = secs(t0, t6);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// batched dense generalized eigensolver: M_b = L L^T, C = L^-1 K_b L^-T,
+// smallest eigenpairs of C, x = L^-T y (dsygvx itype 1 semantics)
+// ---------------------------------------------------------------------------
+void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, const double* K,
+                          const double* M, int mode, int64_t il, int64_t iu, double lo, double hi,
+                          const int64_t* cap, const int64_t* wOff, double* w, const int64_t* vOff,
+                          double* V, int64_t* m) {
+    (void)il;
+    (void)lo;
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    if (batch <= 0) return;
+    cudaStream_t s = stream_;
+    int64_t matTot = 0, vecTot = 0, yTot = 0, wTot = 0, workTot = 0, maxN = 0;
+    std::vector<int64_t> mo(static_cast<size_t>(batch)), vo(static_cast<size_t>(batch)),
+        yo(static_cast<size_t>(batch)), wo(static_cast<size_t>(batch)), ko(static_cast<size_t>(batch)),
+        kc(static_cast<size_t>(batch));
+    for (int b = 0; b < batch; ++b) {
+        const int64_t nb = n[b];
+        if (nb < 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "negative matrix order");
+        const int64_t want = mode == 0 ? std::min<int64_t>(iu, nb) : nb;
+        kc[static_cast<size_t>(b)] = std::max<int64_t>(0, std::min<int64_t>(want, cap[b]));
+        mo[static_cast<size_t>(b)] = matTot;
+        matTot += nb * nb;
+        vo[static_cast<size_t>(b)] = vecTot;
+        vecTot += nb;
+        yo[static_cast<size_t>(b)] = yTot;
+        yTot += nb * kc[static_cast<size_t>(b)];
+        wo[static_cast<size_t>(b)] = wTot;
+        wTot += kc[static_cast<size_t>(b)];
+        ko[static_cast<size_t>(b)] = workTot;
+        workTot += 6 * nb * kc[static_cast<size_t>(b)];
+        maxN = std::max(maxN, nb);
+    }
+    DevBuf dF, dG, dE, dd, de, dtau, dY, dYt, dw, dk, dwork, blob, tl, pbuf;
+    double* F = static_cast<double*>(dF.ensure(sizeof(double) * (matTot + 1)));
+    double* G = static_cast<double*>(dG.ensure(sizeof(double) * (matTot + 1)));
+    double* E = static_cast<double*>(dE.ensure(sizeof(double) * (matTot + 1)));
+    double* Yd = static_cast<double*>(dY.ensure(sizeof(double) * (yTot + 1)));
+    double* Ytd = static_cast<double*>(dYt.ensure(sizeof(double) * (yTot + 1)));
+    for (int b = 0; b < batch; ++b) {
+        const size_t bytes = sizeof(double) * static_cast<size_t>(n[b] * n[b]);
+        cudaCheck(cudaMemcpyAsync(F + mo[static_cast<size_t>(b)], M + matOff[b], bytes, cudaMemcpyHostToDevice, s), "upload M");
+        cudaCheck(cudaMemcpyAsync(G + mo[static_cast<size_t>(b)], K + matOff[b], bytes, cudaMemcpyHostToDevice, s), "upload K");
+    }
+    dd.ensure(sizeof(double) * (vecTot + 1));
+    de.ensure(sizeof(double) * (vecTot + 1));
+    dtau.ensure(sizeof(double) * (vecTot + 1));
+    dw.ensure(sizeof(double) * (wTot + 1));
+    dk.ensure(sizeof(int32_t) * batch);
+    dwork.ensure(sizeof(double) * (workTot + 1));
+    cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
+    std::vector<FrontDesc> fF, fE;
+    std::vector<TrsmDesc> t1, t2, t3;
+    std::vector<TileRef> t1T, t2T, t3T, cpT, cp2T;
+    std::vector<CopyDesc> cp, cp2;
+    std::vector<EigDesc> small, large, all;
+    int maxLargeN = 0;
+    for (int b = 0; b < batch; ++b) {
+        const int64_t nb = n[b];
+        if (nb == 0) continue;
+        double* Fb = F + mo[static_cast<size_t>(b)];
+        double* Gb = G + mo[static_cast<size_t>(b)];
+        double* Eb = E + mo[static_cast<size_t>(b)];
+        FrontDesc f{Fb, nb, static_cast<int32_t>(nb), static_cast<int32_t>(nb), b, 0};
+        fF.push_back(f);
+        fE.push_back(FrontDesc{Eb, nb, static_cast<int32_t>(nb), static_cast<int32_t>(nb), b, 0});
+        TrsmDesc a{Fb, nb, Gb, nb, static_cast<int32_t>(nb), static_cast<int32_t>(nb), 0, 0};
+        trsmTiles(t1T, static_cast<int>(t1.size()), nb);
+        t1.push_back(a);
+        CopyDesc c{Gb, nb, Eb, nb, static_cast<int32_t>(nb), static_cast<int32_t>(nb)};
+        copyTiles(cpT, static_cast<int>(cp.size()), nb, nb);
+        cp.push_back(c);
+        TrsmDesc a2{Fb, nb, Eb, nb, static_cast<int32_t>(nb), static_cast<int32_t>(nb), 0, 0};
+        trsmTiles(t2T, static_cast<int>(t2.size()), nb);
+        t2.push_back(a2);
+        const int64_t kb = kc[static_cast<size_t>(b)];
+        EigDesc e{};
+        e.A = Eb;
+        e.lda = nb;
+        e.d = dd.as<double>() + vo[static_cast<size_t>(b)];
+        e.e = de.as<double>() + vo[static_cast<size_t>(b)];
+        e.tau = dtau.as<double>() + vo[static_cast<size_t>(b)];
+        e.n = static_cast<int32_t>(nb);
+        e.id = b;
+        e.w = dw.as<double>() + wo[static_cast<size_t>(b)];
+        e.Y = Yd + yo[static_cast<size_t>(b)];
+        e.ldy = nb;
+        e.kcap = static_cast<int32_t>(kb);
+        e.kOut = dk.as<int32_t>() + b;
+        e.work = dwork.as<double>() + ko[static_cast<size_t>(b)];
+        all.push_back(e);
+        if (nb <= kSmallEig) small.push_back(e);
+        else {
+            large.push_back(e);
+            maxLargeN = std::max<int>(maxLargeN, static_cast<int>(nb));
+        }
+        if (kb > 0) {
+            // Y (nb x kb) -> Yt (kb x nb), Yt <- Yt L^-1, Yt -> Y
+            CopyDesc y1{Yd + yo[static_cast<size_t>(b)], nb, Ytd + yo[static_cast<size_t>(b)], kb,
+                        static_cast<int32_t>(nb), static_cast<int32_t>(kb)};
+            copyTiles(cp2T, static_cast<int>(cp2.size()), nb, kb);
+            cp2.push_back(y1);
+            TrsmDesc a3{Fb, nb, Ytd + yo[static_cast<size_t>(b)], kb, static_cast<int32_t>(nb),
+                        static_cast<int32_t>(kb), 0, 1};
+            trsmTiles(t3T, static_cast<int>(t3.size()), kb);
+            t3.push_back(a3);
+        }
+    }
+    // back-copy descriptors (Yt -> Y)
+    std::vector<CopyDesc> cp3;
+    std::vector<TileRef> cp3T;
+    for (const CopyDesc& c : cp2) {
+        CopyDesc r{c.out, c.ldout, const_cast<double*>(c.in), c.ldin, c.c, c.r};
+        copyTiles(cp3T, static_cast<int>(cp3.size()), c.c, c.r);
+        cp3.push_back(r);
+    }
+    std::vector<int> gOf, gFirst, gSize;
+    std::vector<int64_t> pOff;
+    int64_t pTot = 0;
+    if (!large.empty()) {
+        const int maxCta = tridiagLargeMaxCtas(maxLargeN);
+        if (static_cast<int>(large.size()) > maxCta)
+            throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "too many large matrices in one batch");
+        double wsum = 0;
+        for (auto& e : large) wsum += static_cast<double>(e.n) * e.n;
+        int used = 0;
+        for (size_t g = 0; g < large.size(); ++g) {
+            int cnt = std::max(1, static_cast<int>(std::floor(maxCta * (static_cast<double>(large[g].n) * large[g].n) / wsum)));
+            cnt = std::max(1, std::min(cnt, maxCta - used - static_cast<int>(large.size() - g - 1)));
+            gFirst.push_back(used);
+            gSize.push_back(cnt);
+            for (int c = 0; c < cnt; ++c) gOf.push_back(static_cast<int>(g));
+            used += cnt;
+            pOff.push_back(pTot);
+            pTot += large[g].n;
+        }
+    }
+    Blob B;
+    const size_t ofF = B.add(fF), ofE = B.add(fE), ot1 = B.add(t1), ot1T = B.add(t1T), ocp = B.add(cp),
+                 ocpT = B.add(cpT), ot2 = B.add(t2), ot2T = B.add(t2T), oS = B.add(small), oL = B.add(large),
+                 oA = B.add(all), ocp2 = B.add(cp2), ocp2T = B.add(cp2T), ot3 = B.add(t3), ot3T = B.add(t3T),
+                 ocp3 = B.add(cp3), ocp3T = B.add(cp3T), oGo = B.add(gOf), oGf = B.add(gFirst),
+                 oGs = B.add(gSize), oPo = B.add(pOff);
+    B.upload(blob, s);
+    const int nb = static_cast<int>(fF.size());
+    const int maxBlocks = cdiv(maxN, kCholBlock), maxRowTiles = cdiv(maxN, kTrsmRows);
+    for (int jb = 0; jb < maxBlocks; ++jb) {
+        LAUNCH(launchCholDiag(B.dev<FrontDesc>(ofF), nb, jb, status_.as<int>(), s));
+        LAUNCH(launchCholPanel(B.dev<FrontDesc>(ofF), nb, jb, maxRowTiles, s));
+    }
+    LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot1), B.dev<TileRef>(ot1T), static_cast<int>(t1T.size()), s));
+    LAUNCH(launchTransposeBatched(B.dev<CopyDesc>(ocp), B.dev<TileRef>(ocpT), static_cast<int>(cpT.size()), s));
+    LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot2), B.dev<TileRef>(ot2T), static_cast<int>(t2T.size()), s));
+    LAUNCH(launchSymmetrize(B.dev<FrontDesc>(ofE), nb, s));
+    if (!small.empty()) LAUNCH(launchTridiagSmall(B.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
+    if (!large.empty()) {
+        pbuf.ensure(sizeof(double) * (pTot + 1));
+        LAUNCH(launchTridiagLargeGroups(B.dev<EigDesc>(oL), B.dev<int>(oGo), B.dev<int>(oGf), B.dev<int>(oGs),
+                                        static_cast<int>(gOf.size()), pbuf.as<double>(), B.dev<int64_t>(oPo),
+                                        maxLargeN, s));
+    }
+    int maxK = 0;
+    for (auto x : kc) maxK = std::max<int>(maxK, static_cast<int>(x));
+    const int bmode = mode == 0 ? 2 : 3;
+    LAUNCH(launchBisect(B.dev<EigDesc>(oA), static_cast<int>(all.size()), bmode, static_cast<int>(iu), hi, maxK,
+                        nullptr, s));
+    LAUNCH(launchInverseIter(B.dev<EigDesc>(oA), static_cast<int>(all.size()), maxK, nullptr, s));
+    LAUNCH(launchBackTransform(B.dev<EigDesc>(oA), static_cast<int>(all.size()), maxK, s));
+    LAUNCH(launchTransposeBatched(B.dev<CopyDesc>(ocp2), B.dev<TileRef>(ocp2T), static_cast<int>(cp2T.size()), s));
+    LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot3), B.dev<TileRef>(ot3T), static_cast<int>(t3T.size()), s));
+    LAUNCH(launchTransposeBatched(B.dev<CopyDesc>(ocp3), B.dev<TileRef>(ocp3T), static_cast<int>(cp3T.size()), s));
+    checkStatus("sygvx");
+    std::vector<int32_t> kh(static_cast<size_t>(batch), 0);
+    cudaCheck(cudaMemcpy(kh.data(), dk.as<int32_t>(), sizeof(int32_t) * batch, cudaMemcpyDeviceToHost), "k");
+    int idx = 0;
+    for (int b = 0; b < batch; ++b) {
+        if (n[b] == 0) {
+            m[b] = 0;
+            continue;
+        }
+        const int64_t kb = std::min<int64_t>(kh[static_cast<size_t>(idx++)], kc[static_cast<size_t>(b)]);
+        m[b] = kb;
+        if (kb <= 0) continue;
+        cudaCheck(cudaMemcpy(w + wOff[b], dw.as<double>() + wo[static_cast<size_t>(b)], sizeof(double) * kb,
+                             cudaMemcpyDeviceToHost), "w");
+        cudaCheck(cudaMemcpy(V + vOff[b], Yd + yo[static_cast<size_t>(b)], sizeof(double) * kb * n[b],
+                             cudaMemcpyDeviceToHost), "V");
+    }
+    (void)ko;
+}
+
+void Engine::info(int64_t* out) const {
+    int64_t ft = frontTotal_;
+    out[0] = static_cast<int64_t>(nodes_.size());
+    out[1] = maxLevel_ + 1;
+    out[2] = pA_;
+    out[3] = pFinal_;
+    out[4] = ft;
+    size_t freeB = 0, totB = 0;
+    cudaMemGetInfo(&freeB, &totB);
+    out[5] = static_cast<int64_t>(totB - freeB);
+    out[6] = launches_;
+}
+
+void Engine::work(double* out) const {
+    for (int i = 0; i < AMLS_WORK_SLOTS; ++i) out[i] = work_[i];
+}
+
+}  // namespace amls_b200

@@ -1,0 +1,156 @@
+// AMLS engine: host analysis + device numeric pipeline for one handle.
+//
+// Algorithm (the reference's AmlsSolver::solve, src/amls/solver.cpp:154-373,
+// re-designed for one B200):
+//   analysis (host):  shift pattern, METIS nested dissection, post-order
+//     offsets, symbolic fill of every node's coupling set S_i (the rows of
+//     ancestors coupled to node i after elimination; the reference's
+//     symbolicFill_ column masks, gaussian_elimination.cpp:221-270), front
+//     layout and extend-add maps, per-level launch tables.
+//   elimination (device, once per solve; the reference runs it per pass):
+//     per tree level, partial Cholesky of the K fronts (L_ii, L_Si), G_i <- G_i
+//     L_ii^-T on the M fronts, C_i = L_ii^-1 M^_ii L_ii^-T, R_i = Q_i - C_i
+//     L_Si^T / 2, and the extend-add of UK = L_Si L_Si^T and UM = L_Si R_i^T +
+//     R_i L_Si^T into the ancestors' fronts.  This is the reference's Schur
+//     and congruence update (K^_aa -= K_ai X_a, M^_ab -= K_ai Y_b + (K_bi
+//     Y_a)^T - K_ai WX_b, gaussian_elimination.cpp:678-826) in factored form.
+//   condensation (per pass): local eigenpairs of (K^_ii, M^_ii) as the largest
+//     eigenvalues nu = 1/mu of C_i (tridiagonalised once), truncation (index
+//     [1, k0] in pass A, mu <= lambda_cut in pass B), and the projection of
+//     subspace_condensation.cpp:129-261 on per-node panels.
+//   reduced eigensolve: the largest eigenvalues of Kp^-1/2 Mp Kp^-1/2.
+//   back-transform z = L^-T S q (subspace_condensation.cpp:263-319),
+//     un-permutation and M-normalisation (solver.cpp:350-365).
+#pragma once
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "amls_b200.h"
+#include "host/devmem.hpp"
+#include "host/tree.hpp"
+#include "kernels/launch.hpp"
+
+namespace amls_b200 {
+
+class Engine {
+public:
+    explicit Engine(int device);
+    ~Engine();
+
+    void analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
+                 const int32_t* mc, const amls_options& opt);
+    void solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
+                     double* Z, bool outputsOnDevice, int64_t* pOut, double* timing);
+    // dense batched generalized eigensolver (amls_sygvx_batched)
+    void sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, const double* K,
+                      const double* M, int mode, int64_t il, int64_t iu, double lo, double hi,
+                      const int64_t* cap, const int64_t* wOff, double* w, const int64_t* vOff,
+                      double* V, int64_t* m);
+
+    void info(int64_t* out) const;
+    void work(double* out) const;
+    bool analyzed() const { return analyzed_; }
+
+private:
+    struct Node {
+        int64_t off = 0, n = 0;      // permuted offset and size
+        int level = 0;
+        int parent = -1;
+        std::vector<int> anc;        // parent .. root
+        std::vector<int32_t> S;      // coupling set (permuted indices, sorted)
+        int64_t ld = 0;              // n + |S|
+        int64_t frontOff = 0;        // doubles into the front pools
+        int64_t eigOff = 0;          // doubles into the eig matrix pool (n*n)
+        int64_t vecOff = 0;          // doubles into d/e/tau pools (n)
+        int64_t pathPrefix = 0;      // sum of ancestor sizes (panel rows)
+        // extend-add maps (offsets into the static int arrays)
+        int64_t mapCol = 0;          // pmin/colOff/rowBase start (|S| entries)
+        int64_t rowS = 0;            // panel row index of each S entry (|S| entries)
+    };
+
+    // pass-dependent state
+    struct Pass {
+        std::vector<int32_t> k;      // kept modes per node
+        std::vector<int64_t> projOff;
+        int64_t p = 0;
+        std::vector<double> theta;   // host copy of reduced eigenvalues (ascending)
+    };
+
+    void buildStatic();
+    void eliminate(cudaStream_t s);
+    void tridiagonalizeAll(cudaStream_t s);
+    void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
+    int reducedSolve(Pass& P, int want, cudaStream_t s);
+    void backtransform(const Pass& P, int m, cudaStream_t s);
+    void checkStatus(const char* phase);
+    // generic selected-eigenpair driver over prepared EigDesc tables
+    void selectEigen(std::vector<EigDesc>& descs, int mode, int want, double thr, bool tridiag,
+                     cudaStream_t s);
+    double elapsed(cudaEvent_t a, cudaEvent_t b);
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    int sms_ = 148;
+    bool analyzed_ = false;
+    amls_options opt_{};
+
+    // problem
+    int64_t n_ = 0, nnzK_ = 0, nnzM_ = 0;
+    std::vector<int64_t> perm_, inv_;
+    std::vector<Node> nodes_;
+    std::vector<int> order_;                       // post-order
+    std::vector<std::vector<int>> byLevel_;
+    int maxLevel_ = 0;
+    std::vector<int32_t> owner_;                   // permuted index -> node
+    int64_t frontTotal_ = 0, eigTotal_ = 0, vecTotal_ = 0;
+
+    // static device data
+    DevBuf kPool_, mPool_, eigPool_, dPool_, ePool_, tauPool_;
+    DevBuf kVal_, mVal_, kDst_, mDst_;             // CSR values and their front destinations
+    DevBuf mRp_, mCi_, invDev_, permDev_;          // original M CSR pattern, maps
+    DevBuf staticInts_;                            // extend-add and panel maps
+    DevBuf staticBlob_;                            // level launch tables
+    DevBuf status_;
+    Blob sblob_;
+    // offsets into sblob_ for level tables
+    struct LevelPlan {
+        size_t frontK = 0, frontM = 0;             // FrontDesc tables
+        int nFront = 0, maxBlocks = 0, maxRowTiles = 0;
+        size_t trsmDesc = 0, trsmTiles = 0;
+        int nTrsmTiles = 0;
+        size_t tDesc = 0, tTiles = 0;              // transpose G_ii -> eig matrix
+        int nTTiles = 0;
+        size_t cDesc = 0, cTiles = 0;              // TRSM on eig matrix
+        int nCTiles = 0;
+        size_t symDesc = 0;                        // symmetrize eig matrices
+        size_t rDesc = 0, rTiles = 0;              // R = Q - L C / 2
+        int nRTiles = 0;
+        size_t uDesc = 0, uTiles = 0;              // extend-add
+        int nUTiles = 0;
+    };
+    std::vector<LevelPlan> levelPlans_;
+    std::vector<int64_t> hostKDst_, hostMDst_;
+
+    // eigen
+    std::vector<EigDesc> eigDescs_;                // one per node (static part)
+    bool tridiagDone_ = false;
+
+    // per-pass device buffers
+    DevBuf yPool_, wPool_, kOutDev_, iiWork_, panelPool_, wtPool_, credPool_;
+    DevBuf redY_, redW_, redWork_, redD_, redE_, redTau_, redK_, redP_;
+    DevBuf ztPool_, zOut_, norms_, sqrtTheta_, passBlob_, tlBlob_, redBlob_, idxBlob_;
+    const int32_t* sIdxDev_ = nullptr;              // S_i lists (device, static)
+    const int32_t* rowSDev_ = nullptr;             // panel rows of S_i (device, static)
+    std::vector<int64_t> panelOff_;                // per node (doubles), -1 none
+    std::vector<int64_t> yOff_;                    // per node (doubles into yPool_)
+
+    // diagnostics / ledger
+    int64_t pA_ = 0, pFinal_ = 0, launches_ = 0;
+    double work_[AMLS_WORK_SLOTS] = {0};
+};
+
+}  // namespace amls_b200

@@ -1,0 +1,225 @@
+// Nested-dissection partition on the host through METIS.
+//
+// The METIS library is the one shipped with the CUDA toolkit
+// (libmetis_static.a, METIS 5 API, 64-bit idx_t established at run time by
+// METIS_SetDefaultOptions filling 40 x 8 bytes).  The graph construction and
+// the recursion restate src/partition/metis_partitioner.cpp:
+//   * extractGraph (:20-45): adjacency of |K|+|M| without self loops, built by
+//     inserting into one std::unordered_set per vertex while walking columns
+//     in ascending order, and emitted in the set's iteration order - the same
+//     container and insertion sequence, hence the same order with libstdc++;
+//   * inducedSubgraph (:48-73): neighbour lists sorted;
+//   * bisect (:80-106): PartGraphRecursive (result unused) then
+//     ComputeVertexSeparator, both with options seed 42;
+//   * recursion (:110-160) and perm = post-order concatenation (:168-175).
+#include "tree.hpp"
+
+#include <algorithm>
+#include <functional>
+#include <numeric>
+#include <stdexcept>
+#include <unordered_set>
+
+extern "C" {
+// METIS 5 public prototypes (idx_t = int64_t in the linked library).
+int METIS_SetDefaultOptions(int64_t* options);
+int METIS_PartGraphRecursive(int64_t* nvtxs, int64_t* ncon, int64_t* xadj, int64_t* adjncy,
+                             int64_t* vwgt, int64_t* vsize, int64_t* adjwgt, int64_t* nparts,
+                             void* tpwgts, void* ubvec, int64_t* options, int64_t* edgecut,
+                             int64_t* part);
+int METIS_ComputeVertexSeparator(int64_t* nvtxs, int64_t* xadj, int64_t* adjncy, int64_t* vwgt,
+                                 int64_t* options, int64_t* sepsize, int64_t* part);
+}
+
+namespace amls_b200 {
+
+namespace {
+constexpr int kMetisOk = 1;
+constexpr int kMetisNOptions = 40;
+constexpr int kMetisOptionSeed = 8;
+
+struct Csr {
+    std::vector<int64_t> xadj, adjncy;
+};
+
+// Pattern of K + M column by column (the matrices are symmetric, so CSR row c
+// is CSC column c).  Row indices of the union are visited in ascending order.
+Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
+                 const int32_t* mc) {
+    std::vector<std::unordered_set<int64_t>> nbr(static_cast<size_t>(n));
+    std::vector<int64_t> col;
+    for (int64_t c = 0; c < n; ++c) {
+        col.clear();
+        int64_t a = kp[c], ae = kp[c + 1], b = mp[c], be = mp[c + 1];
+        while (a < ae || b < be) {  // sorted merge = union pattern of column c
+            int64_t r;
+            if (b >= be || (a < ae && kc[a] < mc[b])) r = kc[a++];
+            else if (a >= ae || mc[b] < kc[a]) r = mc[b++];
+            else { r = kc[a]; ++a; ++b; }
+            col.push_back(r);
+        }
+        for (int64_t r : col) {
+            if (r == c) continue;
+            nbr[static_cast<size_t>(r)].insert(c);
+            nbr[static_cast<size_t>(c)].insert(r);
+        }
+    }
+    Csr g;
+    g.xadj.assign(static_cast<size_t>(n) + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+        g.xadj[static_cast<size_t>(i) + 1] =
+            g.xadj[static_cast<size_t>(i)] + static_cast<int64_t>(nbr[static_cast<size_t>(i)].size());
+    g.adjncy.resize(static_cast<size_t>(g.xadj.back()));
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t p = g.xadj[static_cast<size_t>(i)];
+        for (int64_t j : nbr[static_cast<size_t>(i)]) g.adjncy[static_cast<size_t>(p++)] = j;
+    }
+    return g;
+}
+
+Csr inducedSubgraph(const Csr& g, const std::vector<int64_t>& verts, std::vector<int64_t>& localOf) {
+    const int64_t m = static_cast<int64_t>(verts.size());
+    localOf.assign(g.xadj.size() - 1, -1);
+    for (int64_t i = 0; i < m; ++i) localOf[static_cast<size_t>(verts[static_cast<size_t>(i)])] = i;
+    Csr sub;
+    sub.xadj.assign(static_cast<size_t>(m) + 1, 0);
+    std::vector<int64_t> tmp;
+    for (int64_t i = 0; i < m; ++i) {
+        const int64_t v = verts[static_cast<size_t>(i)];
+        tmp.clear();
+        for (int64_t p = g.xadj[static_cast<size_t>(v)]; p < g.xadj[static_cast<size_t>(v) + 1]; ++p) {
+            const int64_t u = g.adjncy[static_cast<size_t>(p)];
+            if (localOf[static_cast<size_t>(u)] >= 0) tmp.push_back(localOf[static_cast<size_t>(u)]);
+        }
+        std::sort(tmp.begin(), tmp.end());
+        sub.xadj[static_cast<size_t>(i) + 1] = sub.xadj[static_cast<size_t>(i)] + static_cast<int64_t>(tmp.size());
+        sub.adjncy.insert(sub.adjncy.end(), tmp.begin(), tmp.end());
+    }
+    return sub;
+}
+
+// part[v] in {0, 1, 2}; 2 = vertex separator.
+std::vector<int64_t> bisect(Csr g) {
+    const int64_t n = static_cast<int64_t>(g.xadj.size()) - 1;
+    std::vector<int64_t> part(static_cast<size_t>(n), 0);
+    if (n == 0) return part;
+    int64_t nvtxs = n, ncon = 1, nparts = 2, edgecut = 0;
+    std::vector<int64_t> where(static_cast<size_t>(n), 0);
+    int64_t opts[kMetisNOptions];
+    METIS_SetDefaultOptions(opts);
+    opts[kMetisOptionSeed] = 42;
+    if (METIS_PartGraphRecursive(&nvtxs, &ncon, g.xadj.data(), g.adjncy.data(), nullptr, nullptr,
+                                 nullptr, &nparts, nullptr, nullptr, opts, &edgecut,
+                                 where.data()) != kMetisOk)
+        throw std::runtime_error("METIS_PartGraphRecursive failed");
+    int64_t sepsize = 0;
+    if (METIS_ComputeVertexSeparator(&nvtxs, g.xadj.data(), g.adjncy.data(), nullptr, opts,
+                                     &sepsize, part.data()) != kMetisOk)
+        throw std::runtime_error("METIS_ComputeVertexSeparator failed");
+    return part;
+}
+}  // namespace
+
+int64_t SeparatorTree::addNode(NodeRole role, std::vector<int64_t> idx) {
+    TreeNode nd;
+    nd.id = static_cast<int64_t>(nodes_.size());
+    nd.role = role;
+    nd.indices = std::move(idx);
+    nodes_.push_back(std::move(nd));
+    return nodes_.back().id;
+}
+
+void SeparatorTree::postOrderRec(int64_t id, std::vector<int64_t>& out) const {
+    for (int64_t c : node(id).children) postOrderRec(c, out);
+    out.push_back(id);
+}
+
+std::vector<int64_t> SeparatorTree::postOrder() const {
+    std::vector<int64_t> out;
+    out.reserve(nodes_.size());
+    if (!nodes_.empty()) postOrderRec(root(), out);
+    return out;
+}
+
+std::vector<int64_t> SeparatorTree::ancestors(int64_t id) const {
+    std::vector<int64_t> out;
+    for (int64_t p = node(id).parent; p != -1; p = node(p).parent) out.push_back(p);
+    return out;
+}
+
+int64_t SeparatorTree::root() const {
+    for (const auto& nd : nodes_)
+        if (nd.parent == -1) return nd.id;
+    return -1;
+}
+
+void SeparatorTree::relabelRoot() {
+    const int64_t r = root();
+    if (r >= 0 && nodes_[static_cast<size_t>(r)].role == NodeRole::Separator)
+        nodes_[static_cast<size_t>(r)].role = NodeRole::Root;
+}
+
+bool SeparatorTree::validate(int64_t nTotal) const {
+    if (nodes_.empty()) return false;
+    int roots = 0;
+    for (const auto& nd : nodes_) roots += nd.parent == -1;
+    if (roots != 1) return false;
+    for (const auto& nd : nodes_) {
+        if (nd.role == NodeRole::Leaf && !nd.children.empty()) return false;
+        if (nd.role != NodeRole::Leaf && nd.children.size() != 2) return false;
+        for (int64_t c : nd.children)
+            if (node(c).parent != nd.id) return false;
+    }
+    std::vector<int64_t> all;
+    for (const auto& nd : nodes_) all.insert(all.end(), nd.indices.begin(), nd.indices.end());
+    if (static_cast<int64_t>(all.size()) != nTotal) return false;
+    std::sort(all.begin(), all.end());
+    for (int64_t i = 0; i < nTotal; ++i)
+        if (all[static_cast<size_t>(i)] != i) return false;
+    return true;
+}
+
+PartitionResult recursiveBisection(int64_t n, const int64_t* kRowPtr, const int32_t* kCol,
+                                   const int64_t* mRowPtr, const int32_t* mCol, int nLevels,
+                                   int64_t leafSize) {
+    PartitionResult res;
+    if (n == 0) return res;
+    const Csr g = extractGraph(n, kRowPtr, kCol, mRowPtr, mCol);
+
+    std::function<int64_t(const std::vector<int64_t>&, int)> recurse =
+        [&](const std::vector<int64_t>& verts, int depth) -> int64_t {
+        const int64_t m = static_cast<int64_t>(verts.size());
+        if (m <= leafSize || depth >= nLevels || m < 4)
+            return res.tree.addNode(NodeRole::Leaf, verts);
+        std::vector<int64_t> localOf;
+        Csr sub = inducedSubgraph(g, verts, localOf);
+        const std::vector<int64_t> part = bisect(std::move(sub));
+        std::vector<int64_t> side[2], sep;
+        for (int64_t i = 0; i < m; ++i) {
+            const int64_t p = part[static_cast<size_t>(i)];
+            if (p == 2) sep.push_back(verts[static_cast<size_t>(i)]);
+            else side[p].push_back(verts[static_cast<size_t>(i)]);
+        }
+        const int64_t minSide = static_cast<int64_t>(std::min(side[0].size(), side[1].size()));
+        if (sep.empty() || minSide < 2) return res.tree.addNode(NodeRole::Leaf, verts);
+        const int64_t sepId = res.tree.addNode(NodeRole::Separator, sep);
+        const int64_t l = recurse(side[0], depth + 1);
+        const int64_t r = recurse(side[1], depth + 1);
+        res.tree.setChildren(sepId, l, r);
+        res.tree.setParent(l, sepId);
+        res.tree.setParent(r, sepId);
+        return sepId;
+    };
+    std::vector<int64_t> all(static_cast<size_t>(n));
+    std::iota(all.begin(), all.end(), 0);
+    recurse(all, 0);
+    res.tree.relabelRoot();
+    for (int64_t id : res.tree.postOrder()) {
+        const auto& idx = res.tree.node(id).indices;
+        res.perm.insert(res.perm.end(), idx.begin(), idx.end());
+    }
+    if (!res.tree.validate(n)) throw std::runtime_error("partition: tree validation failed");
+    return res;
+}
+
+}  // namespace amls_b200

@@ -1,0 +1,246 @@
+// Batched FP64 GEMM with gather/scatter epilogues, and the front extend-add
+// update (SYRK + SYR2K of the eliminated front, scattered into ancestors).
+//
+// B200 has no FP64 tcgen05 kind; FP64 runs on the DFMA pipe, so these are
+// register-tiled CUDA-core kernels: 64x64 output tile per CTA, 256 threads,
+// 4x4 accumulators per thread, K staged through shared memory in slices of
+// 16 with register prefetch of the next slice (one barrier per slice).
+// Thread (tx, ty) owns rows tx + 16*i and columns ty + 16*j so that the
+// epilogue stores of a warp are contiguous in a column.
+#include "common.cuh"
+#include "launch.hpp"
+
+namespace amls_b200 {
+
+namespace {
+constexpr int TM = 64, TN = 64, TK = 16, NT = 256;
+
+struct RegTile {
+    double a[4], b[4];
+};
+
+__device__ __forceinline__ void loadA(const GemmDesc& D, int m0, int k0, double (&r)[4]) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + NT * u;
+        int i, k;
+        if (D.flags & kTransA) { k = idx % TK; i = idx / TK; }
+        else { i = idx % TM; k = idx / TM; }
+        const int gi = m0 + i, gk = k0 + k;
+        double v = 0.0;
+        if (gi < D.M && gk < D.K) {
+            if (D.flags & kTransA) v = D.A[gk + (int64_t)gi * D.lda];
+            else if (D.flags & kGatherA) v = D.A[gi + (int64_t)D.aMap[gk] * D.lda];
+            else v = D.A[gi + (int64_t)gk * D.lda];
+        }
+        r[u] = v;
+    }
+}
+
+__device__ __forceinline__ void storeA(const GemmDesc& D, const double (&r)[4], double (*As)[TM + 2]) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + NT * u;
+        int i, k;
+        if (D.flags & kTransA) { k = idx % TK; i = idx / TK; }
+        else { i = idx % TM; k = idx / TM; }
+        As[k][i] = r[u];
+    }
+}
+
+__device__ __forceinline__ void loadB(const GemmDesc& D, int n0, int k0, double (&r)[4]) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + NT * u;
+        int j, k;
+        if (D.flags & kTransB) { j = idx % TN; k = idx / TN; }
+        else { k = idx % TK; j = idx / TK; }
+        const int gj = n0 + j, gk = k0 + k;
+        double v = 0.0;
+        if (gj < D.N && gk < D.K) {
+            if (D.flags & kTransB) v = D.B[gj + (int64_t)gk * D.ldb];
+            else v = D.B[gk + (int64_t)gj * D.ldb];
+        }
+        r[u] = v;
+    }
+}
+
+__device__ __forceinline__ void storeB(const GemmDesc& D, const double (&r)[4], double (*Bs)[TN + 2]) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int idx = tid + NT * u;
+        int j, k;
+        if (D.flags & kTransB) { j = idx % TN; k = idx / TN; }
+        else { k = idx % TK; j = idx / TK; }
+        Bs[k][j] = r[u];
+    }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restrict__ descs,
+                                                        const TileRef* __restrict__ tiles) {
+    __shared__ double As[2][TK][TM + 2];
+    __shared__ double Bs[2][TK][TN + 2];
+    const TileRef t = tiles[blockIdx.x];
+    const GemmDesc D = descs[t.desc];
+    const int m0 = t.m0, n0 = t.n0;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+    double ra[4], rb[4];
+    int cur = 0;
+    if (D.K > 0) {
+        loadA(D, m0, 0, ra);
+        loadB(D, n0, 0, rb);
+        storeA(D, ra, As[0]);
+        storeB(D, rb, Bs[0]);
+    }
+    __syncthreads();
+    for (int k0 = 0; k0 < D.K; k0 += TK) {
+        const bool more = k0 + TK < D.K;
+        if (more) {
+            loadA(D, m0, k0 + TK, ra);
+            loadB(D, n0, k0 + TK, rb);
+        }
+#pragma unroll
+        for (int kk = 0; kk < TK; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[cur][kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[cur][kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        if (more) {
+            storeA(D, ra, As[cur ^ 1]);
+            storeB(D, rb, Bs[cur ^ 1]);
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    // epilogue
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int col = n0 + ty + 16 * j;
+        if (col >= D.N) continue;
+        const double cs = (D.flags & kColScale) ? D.colScale[col] : 1.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = m0 + tx + 16 * i;
+            if (row >= D.M) continue;
+            double v = D.alpha * acc[i][j] * cs;
+            if (D.flags & kRowScale) v *= D.rowScale[row];
+            if (D.flags & kScatter) {
+                double* dst = D.C + D.colOff[col] + D.rowIdx[row];
+                if (D.flags & kAtomic) atomicAdd(dst, v);
+                else if (D.flags & kAccumulate) *dst += v;
+                else *dst = v;
+            } else {
+                double* dst = D.C + row + (int64_t)col * D.ldc;
+                if (D.flags & kAccumulate) *dst = v + D.beta * (*dst);
+                else *dst = v;
+            }
+        }
+    }
+}
+
+cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
+                              cudaStream_t s) {
+    if (nTiles <= 0) return cudaSuccess;
+    gemmBatchedKernel<<<nTiles, NT, 0, s>>>(dDescs, dTiles);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// front extend-add: UK = A A^T, UM = A B^T + B A^T, scattered (subtracted)
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) frontUpdateKernel(const FrontUpdDesc* __restrict__ descs,
+                                                        const TileRef* __restrict__ tiles,
+                                                        double* __restrict__ kPool,
+                                                        double* __restrict__ mPool) {
+    __shared__ double Ap[TK][TM + 2], Bp[TK][TM + 2], Aq[TK][TN + 2], Bq[TK][TN + 2];
+    const TileRef t = tiles[blockIdx.x];
+    const FrontUpdDesc D = descs[t.desc];
+    const int p0 = t.m0, q0 = t.n0;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double aK[4][4], aM[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) aK[i][j] = aM[i][j] = 0.0;
+
+    for (int k0 = 0; k0 < D.n; k0 += TK) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int idx = threadIdx.x + NT * u;
+            const int r = idx % TM, k = idx / TM;
+            const int gk = k0 + k;
+            const bool kin = gk < D.n;
+            const int gp = p0 + r, gq = q0 + r;
+            const int64_t cofs = (int64_t)gk * D.ld;
+            Ap[k][r] = (kin && gp < D.s) ? D.A[gp + cofs] : 0.0;
+            Bp[k][r] = (kin && gp < D.s) ? D.B[gp + cofs] : 0.0;
+            Aq[k][r] = (kin && gq < D.s) ? D.A[gq + cofs] : 0.0;
+            Bq[k][r] = (kin && gq < D.s) ? D.B[gq + cofs] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; ++kk) {
+            double ap[4], bp[4], aq[4], bq[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ap[i] = Ap[kk][tx + 16 * i];
+                bp[i] = Bp[kk][tx + 16 * i];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                aq[j] = Aq[kk][ty + 16 * j];
+                bq[j] = Bq[kk][ty + 16 * j];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    aK[i][j] = fma(ap[i], aq[j], aK[i][j]);
+                    aM[i][j] = fma(ap[i], bq[j], fma(bp[i], aq[j], aM[i][j]));
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int q = q0 + ty + 16 * j;
+        if (q >= D.s) continue;
+        const int pm = D.pmin[q];
+        const int64_t co = D.colOff[q];
+        const int rb = D.rowBase[q];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int p = p0 + tx + 16 * i;
+            if (p >= D.s || p < pm) continue;
+            const int64_t o = co + D.rowIdx[rb + p];
+            atomicAdd(kPool + o, -aK[i][j]);
+            atomicAdd(mPool + o, -aM[i][j]);
+        }
+    }
+}
+
+cudaError_t launchFrontUpdate(const FrontUpdDesc* dDescs, const TileRef* dTiles, int nTiles,
+                              double* kPool, double* mPool, cudaStream_t s) {
+    if (nTiles <= 0) return cudaSuccess;
+    frontUpdateKernel<<<nTiles, NT, 0, s>>>(dDescs, dTiles, kPool, mPool);
+    return cudaGetLastError();
+}
+
+}  // namespace amls_b200

@@ -1,0 +1,181 @@
+// Host-side launch interface of the AMLS kernels.  Plain structs shared with
+// the device code; every launcher enqueues on the given stream and returns
+// the cudaError_t of the launch.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace amls_b200 {
+
+// Device status word codes written by kernels (read back by the host):
+// status[0] = code of the first failure, status[1] = where (node / matrix).
+enum DevStatus : int {
+    kDevOk = 0,
+    kDevNotSpd = 1,      // non-positive or NaN pivot
+    kDevIterCap = 2,     // iteration cap reached
+};
+
+// ---------------------------------------------------------------- GEMM --
+// C(MxN) = alpha * op(A)(MxK) * op(B)(KxN) [+ beta*C], column-major, FP64.
+enum GemmFlags : int32_t {
+    kTransA = 1,        // op(A)[i,k] = A[k + i*lda]
+    kTransB = 2,        // op(B)[k,j] = B[j + k*ldb]
+    kScatter = 4,       // output address = C + colOff[j] + rowIdx[i]
+    kAtomic = 8,        // accumulate with atomicAdd (scatter only)
+    kGatherA = 16,      // op(A)[i,k] = A[i + aMap[k]*lda]   (no transA)
+    kRowScale = 32,     // multiply result row i by rowScale[i]
+    kColScale = 64,     // multiply result column j by colScale[j]
+    kAccumulate = 128,  // dense: C = alpha*AB + beta*C ; scatter: *dst += alpha*AB
+};
+
+struct GemmDesc {
+    int32_t M, N, K, flags;
+    const double* A;
+    int64_t lda;
+    const double* B;
+    int64_t ldb;
+    double* C;
+    int64_t ldc;
+    double alpha, beta;
+    const int32_t* rowIdx;
+    const int64_t* colOff;
+    const int32_t* aMap;
+    const double* rowScale;
+    const double* colScale;
+};
+
+struct TileRef {
+    int32_t desc, m0, n0, pad;
+};
+
+// Tile size of the batched GEMM (host builds TileRef tables with it).
+constexpr int kGemmTile = 64;
+
+cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
+                              cudaStream_t s);
+
+// Extend-add update of one eliminated front (multifrontal form of the
+// reference's Schur + congruence updates):
+//   UK = A A^T, UM = A B^T + B A^T  (s x s), A = L_Si, B = R_i^T (s x n each)
+// entry (p, q) with p >= pmin[q] is subtracted (atomically) from
+//   kPool[colOff[q] + rowIdx[rowBase[q] + p]]  and  mPool[same offset].
+struct FrontUpdDesc {
+    int32_t s, n;          // update order s, inner dimension n
+    int32_t tilesM, pad;   // number of 64-row tiles
+    const double* A;       // s x n, ld
+    const double* B;
+    int64_t ld;
+    const int32_t* pmin;   // per column q
+    const int64_t* colOff; // per column q (element offset in pools)
+    const int32_t* rowIdx; // row target offsets
+    const int32_t* rowBase;// per column q, index base into rowIdx
+};
+cudaError_t launchFrontUpdate(const FrontUpdDesc* dDescs, const TileRef* dTiles, int nTiles,
+                              double* kPool, double* mPool, cudaStream_t s);
+
+// -------------------------------------------------------- factorisation --
+// Batched blocked partial Cholesky of fronts F_i ((n+s) x n, ld = n+s):
+// L_ii = chol(F_ii), L_Si = F_Si L_ii^-T, in place.  One call per column
+// block jb; descs list the fronts of one tree level.
+struct FrontDesc {
+    double* F;             // front (column-major)
+    int64_t ld;            // n + s
+    int32_t n, rows;       // n pivots, rows = n + s
+    int32_t node, pad;
+};
+constexpr int kCholBlock = 32;
+cudaError_t launchCholDiag(const FrontDesc* d, int nDesc, int jb, int* status, cudaStream_t s);
+cudaError_t launchCholPanel(const FrontDesc* d, int nDesc, int jb, int maxRowTiles,
+                            cudaStream_t s);
+
+// Batched row-panel triangular solve with a factored front's L (n x n):
+//   forward  (backward=0):  X <- X L^-T   (X: r x n, ld ldx)
+//   backward (backward=1):  X <- X L^-1
+struct TrsmDesc {
+    const double* L;
+    int64_t ldl;
+    double* X;
+    int64_t ldx;
+    int32_t n, r;
+    int32_t rowTiles, backward;
+};
+constexpr int kTrsmRows = 32;
+cudaError_t launchTrsmRows(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
+
+// ------------------------------------------------------- eigensolver ----
+// Symmetric tridiagonalisation (Householder), in place.  A (n x n, full
+// symmetric, ld) is overwritten: v_k stored in A[k+1:n, k] (v_k[0] = 1);
+// d[n], e[n-1], tau[n-1].
+struct EigDesc {
+    double* A;
+    int64_t lda;
+    double* d;
+    double* e;
+    double* tau;
+    int32_t n, id;
+    // selection and outputs
+    double* w;          // selected eigenvalues (of the tridiagonal/symmetric matrix)
+    double* Y;          // n x kcap eigenvectors, ld = ldy
+    int64_t ldy;
+    int32_t kcap;       // capacity (columns of Y)
+    int32_t* kOut;      // number selected (device)
+    double* work;       // per-matrix scratch (>= 8n doubles)
+};
+cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s);
+// Cooperative multi-CTA tridiagonalisation of a batch of large matrices: the
+// grid is split into CTA groups, group g (CTAs groupFirst[g] ..
+// + groupSize[g]) works on descs[g]; p vectors at dP + dPOff[g].
+cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
+                                     const int* dGroupFirst, const int* dGroupSize, int nCta,
+                                     double* dP, const int64_t* dPOff, int maxN, cudaStream_t s);
+// Co-resident CTA count for the cooperative kernel at a given maxN.
+int tridiagLargeMaxCtas(int maxN);
+// Select eigenvalues of T: mode 0 = the k largest (k = want), mode 1 = all
+// >= thr; mode 2 = the k smallest, mode 3 = all <= thr.  Bisection.
+// Selected values are written in "wanted" order (largest first for modes
+// 0/1, smallest first for modes 2/3).
+cudaError_t launchBisect(const EigDesc* d, int nDesc, int mode, int want, double thr,
+                         int maxN, int* status, cudaStream_t s);
+// Inverse iteration for the selected eigenvalues (clusters reorthogonalised).
+cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int* status,
+                              cudaStream_t s);
+// Y <- Q Y with Q = H_0 ... H_{n-3} (back-transform of tridiagonal vectors).
+cudaError_t launchBackTransform(const EigDesc* d, int nDesc, int maxK, cudaStream_t s);
+
+// --------------------------------------------------------------- misc ---
+// Zero a list of (pointer, count) ranges.
+cudaError_t launchZero(double* p, int64_t count, cudaStream_t s);
+// Scatter permuted CSR entries into the fronts: entry e -> pool[dst[e]]
+// (dst < 0: skipped).
+cudaError_t launchScatterAdd(const double* vals, const int64_t* dst, int64_t nnz, double scale,
+                             double* pool, cudaStream_t s);
+// C[j + j*p] = w[j], j < p.
+cudaError_t launchSetDiagonal(double* C, const double* w, int64_t p, cudaStream_t s);
+// Symmetrise a batch of square blocks: A = (A + A^T)/2.
+cudaError_t launchSymmetrize(const FrontDesc* d, int nDesc, cudaStream_t s);
+// Transpose-copy: out(c x r) = in(r x c)^T  for a batch.
+struct CopyDesc {
+    const double* in;
+    int64_t ldin;
+    double* out;
+    int64_t ldout;
+    int32_t r, c;
+};
+cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int nTiles,
+                                   cudaStream_t s);
+// Segment copies: out[dstOff[g] + t] = in[srcOff[g] + t] for t < len[g].
+cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* out,
+                             const int64_t* dstOff, const int32_t* len, int nSeg,
+                             cudaStream_t s);
+// M-norms of the columns of X under the original M (CSR rp/ci/v), with X
+// held transposed in permuted order: x[o, j] = zt[j + inv[o]*m].
+cudaError_t launchMNorm(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
+                        const int64_t* inv, const double* zt, int m, double* norms,
+                        cudaStream_t s);
+// Z[perm[d] + j*n] = zt[j + d*m] / sqrt(norms[j]).
+cudaError_t launchUnpermute(const double* zt, int m, int64_t n, const int64_t* perm,
+                            const double* norms, double* Z, cudaStream_t s);
+// out[i] = 1 / in[i]   (reciprocals, for eigenvalue maps)
+cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s);
+
+}  // namespace amls_b200

@@ -1,0 +1,523 @@
+// FP64 symmetric eigensolver for selected eigenpairs, batched.
+//
+// This is the device replacement of LAPACK's dsygvx path used by the
+// reference for every local and reduced eigenproblem
+// (src/linalg/dense_eigensolver.cpp:44-133): after the pencil has been
+// reduced to a standard symmetric matrix (see engine), the steps are the
+// classical ones - Householder tridiagonalisation (dsytrd), bisection on
+// Sturm counts for the selected eigenvalues (dstebz), inverse iteration with
+// reorthogonalisation inside clusters (dstein) and back-transformation by
+// the reflectors (dormtr) - each written for the GPU:
+//   * tridiagSmall:  one CTA per matrix (batched), trailing matrix in L2;
+//   * tridiagLarge:  cooperative launch, the grid split into CTA groups, one
+//                    group per matrix, two grid barriers per column step;
+//   * bisect:        one thread per wanted eigenvalue;
+//   * inverseIter:   one CTA per cluster, members solved in sequence, the
+//                    tridiagonal LU/solve on one thread, the
+//                    reorthogonalisation and norms block-parallel;
+//   * backTransform: one warp per eigenvector column.
+#include <cooperative_groups.h>
+
+#include <cfloat>
+
+#include "common.cuh"
+#include "launch.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace amls_b200 {
+
+namespace {
+constexpr int kSmallThreads = 512;
+}
+
+// ------------------------------------------------------------------------
+// Householder step helpers
+// ------------------------------------------------------------------------
+struct HouseholderScalars {
+    double beta, tau, scale;  // v = [1, x[1:] * scale]
+};
+
+// dlarfg on x = A[k+1:n, k] (alpha = x[0], xnorm2 = |x[1:]|^2).
+__device__ __forceinline__ HouseholderScalars makeReflector(double alpha, double xnorm2) {
+    HouseholderScalars h;
+    if (xnorm2 == 0.0) {
+        h.beta = alpha;
+        h.tau = 0.0;
+        h.scale = 0.0;
+    } else {
+        const double nrm = sqrt(alpha * alpha + xnorm2);
+        h.beta = alpha >= 0.0 ? -nrm : nrm;
+        h.tau = (h.beta - alpha) / h.beta;
+        h.scale = 1.0 / (alpha - h.beta);
+    }
+    return h;
+}
+
+// ------------------------------------------------------------------------
+// tridiagonalisation, one CTA per matrix
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDesc* __restrict__ descs) {
+    extern __shared__ double sm[];
+    __shared__ double red[32];
+    const EigDesc D = descs[blockIdx.x];
+    const int n = D.n;
+    double* A = D.A;
+    const int64_t lda = D.lda;
+    double* v = sm;        // n
+    double* p = sm + n;    // n
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        double* col = A + (k + 1) + (int64_t)k * lda;
+        double part = 0.0;
+        for (int i = 1 + tid; i < m; i += blockDim.x) part += col[i] * col[i];
+        const double xnorm2 = blockSum(part, red);
+        const double alpha = col[0];
+        const HouseholderScalars h = makeReflector(alpha, xnorm2);
+        for (int i = tid; i < m; i += blockDim.x) v[i] = (i == 0) ? 1.0 : col[i] * h.scale;
+        __syncthreads();
+        if (tid == 0) {
+            D.d[k] = A[k + (int64_t)k * lda];
+            D.e[k] = h.beta;
+            D.tau[k] = h.tau;
+        }
+        for (int i = tid; i < m; i += blockDim.x) col[i] = v[i];
+        if (h.tau != 0.0) {
+            double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
+            // p = tau * A22 v  (warp per column)
+            for (int j = wid; j < m; j += nw) {
+                const double* cj = A22 + (int64_t)j * lda;
+                double s = 0.0;
+                for (int i = lane; i < m; i += 32) s += cj[i] * v[i];
+                s = warpSum<32>(s);
+                if (lane == 0) p[j] = h.tau * s;
+            }
+            __syncthreads();
+            double pv = 0.0;
+            for (int i = tid; i < m; i += blockDim.x) pv += p[i] * v[i];
+            pv = blockSum(pv, red);
+            const double a2 = -0.5 * h.tau * pv;
+            for (int i = tid; i < m; i += blockDim.x) p[i] += a2 * v[i];   // p := w
+            __syncthreads();
+            for (int j = wid; j < m; j += nw) {
+                double* cj = A22 + (int64_t)j * lda;
+                const double vj = v[j], wj = p[j];
+                for (int i = lane; i < m; i += 32) cj[i] -= v[i] * wj + p[i] * vj;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (n >= 2) {
+            D.d[n - 2] = A[(n - 2) + (int64_t)(n - 2) * lda];
+            D.e[n - 2] = A[(n - 1) + (int64_t)(n - 2) * lda];
+            D.tau[n - 2] = 0.0;
+        }
+        if (n >= 1) D.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda];
+    }
+}
+
+cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s) {
+    // callers guarantee n <= 2048 for this path (2 * 2048 doubles of smem)
+    if (nDesc <= 0) return cudaSuccess;
+    tridiagSmallKernel<<<nDesc, kSmallThreads, 2 * 2048 * sizeof(double), s>>>(d);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// tridiagonalisation, cooperative, grid split into groups (one per matrix)
+// ------------------------------------------------------------------------
+struct LargeArgs {
+    const EigDesc* descs;     // device
+    const int* groupOf;       // CTA -> group (matrix)
+    const int* groupFirst;    // first CTA of each group
+    const int* groupSize;     // CTAs in each group
+    double* pbuf;             // per matrix p vectors (offsets = pOff)
+    const int64_t* pOff;
+    int maxN;
+};
+
+__global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
+    extern __shared__ double sv[];   // v (maxN)
+    __shared__ double red[32];
+    cg::grid_group grid = cg::this_grid();
+    const int g = a.groupOf[blockIdx.x];
+    const int rank = blockIdx.x - a.groupFirst[g];
+    const int gsize = a.groupSize[g];
+    const EigDesc D = a.descs[g];
+    const int n = D.n;
+    double* A = D.A;
+    const int64_t lda = D.lda;
+    double* p = a.pbuf + a.pOff[g];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int gw = rank * nw + wid, GW = gsize * nw;
+    for (int k = 0; k + 2 < a.maxN; ++k) {
+        const bool active = k + 2 < n;
+        const int m = n - k - 1;
+        double* col = A + (k + 1) + (int64_t)k * lda;
+        HouseholderScalars h{0.0, 0.0, 0.0};
+        if (active) {
+            double part = 0.0;
+            for (int i = 1 + tid; i < m; i += blockDim.x) part += col[i] * col[i];
+            const double xnorm2 = blockSum(part, red);
+            h = makeReflector(col[0], xnorm2);
+            for (int i = tid; i < m; i += blockDim.x) sv[i] = (i == 0) ? 1.0 : col[i] * h.scale;
+            __syncthreads();
+            if (h.tau != 0.0) {
+                const double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
+                for (int j = gw; j < m; j += GW) {
+                    const double* cj = A22 + (int64_t)j * lda;
+                    double s = 0.0;
+                    for (int i = lane; i < m; i += 32) s += cj[i] * sv[i];
+                    s = warpSum<32>(s);
+                    if (lane == 0) p[j] = h.tau * s;
+                }
+            }
+        }
+        grid.sync();
+        if (active) {
+            if (h.tau != 0.0) {
+                double pv = 0.0;
+                for (int i = tid; i < m; i += blockDim.x) pv += p[i] * sv[i];
+                pv = blockSum(pv, red);
+                const double a2 = -0.5 * h.tau * pv;
+                double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
+                for (int j = gw; j < m; j += GW) {
+                    double* cj = A22 + (int64_t)j * lda;
+                    const double vj = sv[j], wj = p[j] + a2 * vj;
+                    for (int i = lane; i < m; i += 32) {
+                        const double wi = p[i] + a2 * sv[i];
+                        cj[i] -= sv[i] * wj + wi * vj;
+                    }
+                }
+            }
+            if (rank == 0) {
+                for (int i = tid; i < m; i += blockDim.x) col[i] = sv[i];
+                if (tid == 0) {
+                    D.d[k] = A[k + (int64_t)k * lda];
+                    D.e[k] = h.beta;
+                    D.tau[k] = h.tau;
+                }
+            }
+        }
+        grid.sync();
+    }
+    if (rank == 0 && tid == 0) {
+        if (n >= 2) {
+            D.d[n - 2] = A[(n - 2) + (int64_t)(n - 2) * lda];
+            D.e[n - 2] = A[(n - 1) + (int64_t)(n - 2) * lda];
+            D.tau[n - 2] = 0.0;
+        }
+        if (n >= 1) D.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda];
+    }
+}
+
+cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
+                                     const int* dGroupFirst, const int* dGroupSize, int nCta,
+                                     double* dP, const int64_t* dPOff, int maxN, cudaStream_t s) {
+    LargeArgs a{dDescs, dGroupOf, dGroupFirst, dGroupSize, dP, dPOff, maxN};
+    void* args[] = {&a};
+    const size_t smem = (size_t)maxN * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(tridiagLargeKernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaLaunchCooperativeKernel((void*)tridiagLargeKernel, dim3(nCta), dim3(256), args, smem, s);
+}
+
+int tridiagLargeMaxCtas(int maxN) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = (size_t)maxN * sizeof(double);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(tridiagLargeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiagLargeKernel, 256, smem);
+    if (per > 4) per = 4;
+    return per * sms;
+}
+
+// ------------------------------------------------------------------------
+// bisection (Sturm counts)
+// ------------------------------------------------------------------------
+__device__ __forceinline__ int sturmLess(const double* d, const double* e, int n, double x,
+                                         double pivmin) {
+    int cnt = 0;
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+    for (int i = 1; i < n; ++i) {
+        q = d[i] - x - e[i - 1] * e[i - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        cnt += q < 0.0;
+    }
+    return cnt;
+}
+
+__device__ void gershgorin(const double* d, const double* e, int n, double& lo, double& hi,
+                           double& pivmin, double& tnorm) {
+    lo = DBL_MAX;
+    hi = -DBL_MAX;
+    double emax2 = 0.0;
+    tnorm = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+        lo = fmin(lo, d[i] - r);
+        hi = fmax(hi, d[i] + r);
+        tnorm = fmax(tnorm, fabs(d[i]) + r);
+        if (i + 1 < n) emax2 = fmax(emax2, e[i] * e[i]);
+    }
+    pivmin = DBL_MIN * fmax(1.0, emax2);
+    const double pad = 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + 2.0 * pivmin;
+    lo -= pad;
+    hi += pad;
+}
+
+// count kernel: kOut[b] for modes 0/2 (min(want, n, kcap)) and 1/3 (threshold)
+__global__ void bisectCountKernel(const EigDesc* __restrict__ descs, int nDesc, int mode, int want,
+                                  double thr) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nDesc) return;
+    const EigDesc D = descs[b];
+    const int n = D.n;
+    int k;
+    if (n <= 0) k = 0;
+    else if (mode == 0 || mode == 2) k = min(want, n);
+    else {
+        double lo, hi, pivmin, tn;
+        gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
+        const int less = sturmLess(D.d, D.e, n, thr, pivmin);
+        k = (mode == 1) ? (n - less) : less;
+    }
+    *D.kOut = min(k, D.kcap);
+}
+
+__global__ void bisectKernel(const EigDesc* __restrict__ descs, int mode, int maxK) {
+    const int b = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const EigDesc D = descs[b];
+    const int k = *D.kOut;
+    if (j >= k) return;
+    const int n = D.n;
+    // 1-based ascending index of the wanted eigenvalue
+    const int t = (mode <= 1) ? (n - j) : (j + 1);
+    double lo, hi, pivmin, tn;
+    gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin || mid <= lo ||
+            mid >= hi)
+            break;
+        // count(< mid) >= t  <=>  lambda_t < mid
+        if (sturmLess(D.d, D.e, n, mid, pivmin) >= t) hi = mid;
+        else lo = mid;
+    }
+    D.w[j] = 0.5 * (lo + hi);
+}
+
+cudaError_t launchBisect(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
+                         int*, cudaStream_t s) {
+    if (nDesc <= 0) return cudaSuccess;
+    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || maxK <= 0) return e;
+    dim3 grid((maxK + 63) / 64, nDesc);
+    bisectKernel<<<grid, 64, 0, s>>>(d, mode, maxK);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// inverse iteration (dlagtf / dlagts / dstein), one CTA per cluster
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restrict__ descs,
+                                                          int maxK) {
+    __shared__ double red[32];
+    __shared__ double sh[4];
+    const int b = blockIdx.y;
+    const int j = blockIdx.x;
+    const EigDesc D = descs[b];
+    const int k = *D.kOut;
+    const int n = D.n;
+    if (j >= k || n <= 0) return;
+    const int tid = threadIdx.x;
+    // T norm and cluster tolerance (dstein: ortol = 1e-3 * onenrm)
+    double lo, hi, pivmin, tnorm;
+    gershgorin(D.d, D.e, n, lo, hi, pivmin, tnorm);
+    const double ortol = 1e-3 * tnorm;
+    // cluster start: j is a start if j == 0 or |w[j] - w[j-1]| > ortol
+    if (j > 0 && fabs(D.w[j] - D.w[j - 1]) <= ortol) return;
+    int jend = j + 1;
+    while (jend < k && fabs(D.w[jend] - D.w[jend - 1]) <= ortol) ++jend;
+    if (n == 1) {
+        if (tid == 0) D.Y[0 + (int64_t)j * D.ldy] = 1.0;
+        return;
+    }
+    // scratch: a, b(super), c(sub), dd(2nd super), y, piv  (6n doubles)
+    double* W = D.work + (int64_t)j * 6 * n;
+    double* a = W;
+    double* bs = W + n;
+    double* c = W + 2 * n;
+    double* dd = W + 3 * n;
+    double* piv = W + 5 * n;
+    const double eps = DBL_EPSILON;
+    double prevLam = 0.0;
+    for (int jj = j; jj < jend; ++jj) {
+        double lam = D.w[jj];
+        if (jj > j) {
+            // perturb away from the previous member (dstein pertol = 10 |eps * x|)
+            const double pertol = 10.0 * fabs(eps * lam);
+            const double dir = (D.w[jend - 1] >= D.w[j]) ? 1.0 : -1.0;  // ordering direction
+            if (dir * (lam - prevLam) < pertol) lam = prevLam + dir * pertol;
+        }
+        prevLam = lam;
+        double* x = D.Y + (int64_t)jj * D.ldy;
+        // LU with partial pivoting of T - lam I (dlagtf), on one thread
+        if (tid == 0) {
+            for (int i = 0; i < n; ++i) a[i] = D.d[i] - lam;
+            for (int i = 0; i + 1 < n; ++i) {
+                bs[i] = D.e[i];
+                c[i] = D.e[i];
+            }
+            for (int kk = 0; kk + 1 < n; ++kk) {
+                const double scale1 = fabs(a[kk]) + fabs(bs[kk]);
+                const double piv1 = scale1 == 0.0 ? 0.0 : fabs(a[kk]) / scale1;
+                double scale2 = fabs(c[kk]) + fabs(a[kk + 1]);
+                if (kk + 2 < n) scale2 += fabs(bs[kk + 1]);
+                const double piv2 = (c[kk] == 0.0 || scale2 == 0.0) ? 0.0 : fabs(c[kk]) / scale2;
+                if (c[kk] == 0.0 || piv2 <= piv1) {
+                    piv[kk] = 0.0;
+                    const double mult = (c[kk] == 0.0 || a[kk] == 0.0) ? 0.0 : c[kk] / a[kk];
+                    c[kk] = mult;
+                    a[kk + 1] -= mult * bs[kk];
+                    if (kk + 2 < n) dd[kk] = 0.0;
+                } else {
+                    piv[kk] = 1.0;
+                    const double mult = a[kk] / c[kk];
+                    a[kk] = c[kk];
+                    const double temp = a[kk + 1];
+                    a[kk + 1] = bs[kk] - mult * temp;
+                    if (kk + 2 < n) {
+                        dd[kk] = bs[kk + 1];
+                        bs[kk + 1] = -mult * dd[kk];
+                    }
+                    bs[kk] = temp;
+                    c[kk] = mult;
+                }
+            }
+        }
+        // deterministic start vector
+        for (int i = tid; i < n; i += blockDim.x) {
+            unsigned h = (unsigned)(i * 2654435761u) ^ (unsigned)(jj * 40503u + 12345u);
+            h ^= h >> 13;
+            h *= 0x5bd1e995u;
+            h ^= h >> 15;
+            x[i] = ((h & 0xffffff) / double(0x1000000)) - 0.5 + 1e-3;
+        }
+        __syncthreads();
+        const double tol = fmax(eps * tnorm, DBL_MIN);
+        for (int it = 0; it < 4; ++it) {
+            if (tid == 0) {
+                // apply L^-1 with interchanges, then U^-1 (dlagts, job -1)
+                for (int kk = 0; kk + 1 < n; ++kk) {
+                    if (piv[kk] == 0.0) x[kk + 1] -= c[kk] * x[kk];
+                    else {
+                        const double temp = x[kk];
+                        x[kk] = x[kk + 1];
+                        x[kk + 1] = temp - c[kk] * x[kk];
+                    }
+                }
+                for (int kk = n - 1; kk >= 0; --kk) {
+                    double temp = x[kk];
+                    if (kk + 1 < n) temp -= bs[kk] * x[kk + 1];
+                    if (kk + 2 < n) temp -= dd[kk] * x[kk + 2];
+                    double ak = a[kk];
+                    if (fabs(ak) < tol) ak = (ak >= 0.0) ? tol : -tol;
+                    x[kk] = temp / ak;
+                }
+            }
+            __syncthreads();
+            // reorthogonalise against earlier members of the cluster (MGS)
+            for (int q = j; q < jj; ++q) {
+                const double* xq = D.Y + (int64_t)q * D.ldy;
+                double part = 0.0;
+                for (int i = tid; i < n; i += blockDim.x) part += xq[i] * x[i];
+                const double dot = blockSum(part, red);
+                for (int i = tid; i < n; i += blockDim.x) x[i] -= dot * xq[i];
+                __syncthreads();
+            }
+            // normalise (2-norm), guard against overflow by max-scaling first
+            double mx = 0.0;
+            for (int i = tid; i < n; i += blockDim.x) mx = fmax(mx, fabs(x[i]));
+            mx = blockMax(mx, red);
+            const double inv = mx > 0.0 ? 1.0 / mx : 1.0;
+            double ss = 0.0;
+            for (int i = tid; i < n; i += blockDim.x) {
+                const double t = x[i] * inv;
+                ss += t * t;
+            }
+            ss = blockSum(ss, red);
+            const double sc = inv / sqrt(fmax(ss, DBL_MIN));
+            for (int i = tid; i < n; i += blockDim.x) x[i] *= sc;
+            __syncthreads();
+        }
+        // sign convention: largest-magnitude component positive (dstein)
+        double mx = 0.0;
+        int imx = 0;
+        if (tid == 0) {
+            for (int i = 0; i < n; ++i)
+                if (fabs(x[i]) > mx) {
+                    mx = fabs(x[i]);
+                    imx = i;
+                }
+            sh[0] = x[imx] < 0.0 ? -1.0 : 1.0;
+        }
+        __syncthreads();
+        const double sg = sh[0];
+        for (int i = tid; i < n; i += blockDim.x) x[i] *= sg;
+        __syncthreads();
+    }
+}
+
+cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int*, cudaStream_t s) {
+    if (nDesc <= 0 || maxK <= 0) return cudaSuccess;
+    dim3 grid(maxK, nDesc);
+    inverseIterKernel<<<grid, 256, 0, s>>>(d, maxK);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// back-transform Y <- H_0 ... H_{n-3} Y, one warp per column
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) backTransformKernel(const EigDesc* __restrict__ descs,
+                                                            int maxK) {
+    const int b = blockIdx.y;
+    const int col = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const EigDesc D = descs[b];
+    const int k = *D.kOut;
+    if (col >= k) return;
+    const int n = D.n;
+    double* y = D.Y + (int64_t)col * D.ldy;
+    for (int kk = n - 3; kk >= 0; --kk) {
+        const double tau = D.tau[kk];
+        if (tau == 0.0) continue;
+        const double* v = D.A + (kk + 1) + (int64_t)kk * D.lda;   // v[0] = 1
+        const int m = n - kk - 1;
+        double s = 0.0;
+        for (int i = lane; i < m; i += 32) s += v[i] * y[kk + 1 + i];
+        s = warpSum<32>(s) * tau;
+        for (int i = lane; i < m; i += 32) y[kk + 1 + i] -= s * v[i];
+        __syncwarp();
+    }
+}
+
+cudaError_t launchBackTransform(const EigDesc* d, int nDesc, int maxK, cudaStream_t s) {
+    if (nDesc <= 0 || maxK <= 0) return cudaSuccess;
+    dim3 grid((maxK + 7) / 8, nDesc);
+    backTransformKernel<<<grid, 256, 0, s>>>(d, maxK);
+    return cudaGetLastError();
+}
+
+}  // namespace amls_b200

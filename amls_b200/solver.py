@@ -1,0 +1,169 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+``AmlsSolver.solve(K, M, opt)`` corresponds to ``AmlsSolver::solve``
+(src/amls/solver.cpp:154-373): same options and defaults, same exceptions
+(``ValueError`` for std::invalid_argument, ``RuntimeError`` subclasses for
+std::runtime_error), ``Solution`` with theta ascending, Z M-normalised in the
+original ordering, the reduced size p and the phase timings.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+
+
+@dataclasses.dataclass
+class AmlsOptions:
+    """AmlsOptions (src/amls/solver.hpp:18-30)."""
+    nLevels: int = 6
+    leafSize: int = 500
+    thresholdFactor: float = 2.0
+    fixedKeep: int = 0
+    nev: int = 100
+    denseProjectedMax: int = 5000
+    shift: float = 0.0
+    twoPass: bool = True
+    numThreads: int = 0
+    recoverVectors: bool = True
+    verbosity: int = 0
+
+    def to_c(self) -> _lib.Options:
+        o = _lib.Options()
+        _lib.check(_lib.lib().amls_options_default(C.byref(o)))
+        o.nLevels = int(self.nLevels)
+        o.leafSize = int(self.leafSize)
+        o.thresholdFactor = float(self.thresholdFactor)
+        o.fixedKeep = int(self.fixedKeep)
+        o.nev = int(self.nev)
+        o.denseProjectedMax = int(self.denseProjectedMax)
+        o.shift = float(self.shift)
+        o.twoPass = 1 if self.twoPass else 0
+        o.numThreads = int(self.numThreads)
+        o.recoverVectors = 1 if self.recoverVectors else 0
+        o.verbosity = int(self.verbosity)
+        return o
+
+
+@dataclasses.dataclass
+class Solution:
+    theta: np.ndarray
+    Z: np.ndarray | None
+    p: int
+    timing: dict
+    info: dict
+
+
+def _csr_arrays(A):
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    ci = np.ascontiguousarray(A.indices, dtype=np.int32)
+    v = np.ascontiguousarray(A.data, dtype=np.float64)
+    return rp, ci, v
+
+
+def recursive_bisection(K, M, nLevels: int, leafSize: int):
+    """Partition of |K| + |M|: returns (perm, tree arrays dict)."""
+    kp, kc, _ = _csr_arrays(K)
+    mp, mc, _ = _csr_arrays(M)
+    n = K.shape[0]
+    perm = np.zeros(n, np.int64)
+    nn = C.c_int64(0)
+    parent = np.zeros(n, np.int64)
+    role = np.zeros(n, np.int32)
+    left = np.zeros(n, np.int64)
+    right = np.zeros(n, np.int64)
+    idx_ptr = np.zeros(n + 1, np.int64)
+    idx = np.zeros(n, np.int64)
+    _lib.check(_lib.lib().amls_partition(n, kp, kc, mp, mc, int(nLevels), int(leafSize), perm,
+                                         C.byref(nn), parent, role, left, right, idx_ptr, idx))
+    N = nn.value
+    return perm, dict(parent=parent[:N].copy(), role=role[:N].copy(), left=left[:N].copy(),
+                      right=right[:N].copy(), idx_ptr=idx_ptr[:N + 1].copy(), idx=idx.copy())
+
+
+class AmlsSolver:
+    """One GPU handle; ``solve`` is the drop-in for AmlsSolver::solve."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _lib.check(_lib.lib().amls_create(int(device), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            _lib.lib().amls_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, K, M, opt: AmlsOptions) -> Solution:
+        kp, kc, kv = _csr_arrays(K)
+        mp, mc, mv = _csr_arrays(M)
+        n = K.shape[0]
+        nev = max(0, min(int(opt.nev), n))
+        theta = np.zeros(max(nev, 1), np.float64)
+        Z = np.zeros((nev, n), np.float64) if opt.recoverVectors and nev > 0 else None
+        p = C.c_int64(0)
+        timing = np.zeros(_lib.T_SLOTS, np.float64)
+        o = opt.to_c()
+        _lib.check(_lib.lib().amls_solve(self._h, n, _lib.ptr(kp), _lib.ptr(kc), _lib.ptr(kv),
+                                         _lib.ptr(mp), _lib.ptr(mc), _lib.ptr(mv), C.byref(o),
+                                         _lib.ptr(theta), _lib.ptr(Z), C.byref(p),
+                                         _lib.ptr(timing)))
+        return Solution(theta[:nev].copy(), None if Z is None else Z.T.copy(), int(p.value),
+                        dict(zip(_lib.TIMING_KEYS, timing.tolist())), self.info())
+
+    def info(self) -> dict:
+        buf = np.zeros(_lib.INFO_SLOTS, np.int64)
+        _lib.check(_lib.lib().amls_info(self._h, _lib.ptr(buf)))
+        keys = ["tree_nodes", "levels", "p_passA", "p", "front_doubles", "device_bytes",
+                "launches"]
+        return {k: int(v) for k, v in zip(keys, buf)}
+
+    def work(self) -> dict:
+        buf = np.zeros(_lib.WORK_SLOTS, np.float64)
+        _lib.check(_lib.lib().amls_work(self._h, _lib.ptr(buf)))
+        keys = ["flops_elim", "bytes_elim", "flops_cond", "bytes_cond", "flops_reduced",
+                "bytes_reduced", "flops_back", "bytes_back"]
+        return dict(zip(keys, buf.tolist()))
+
+
+def sygvx_batched(solver: AmlsSolver, Ks, Ms, mode: str = "index", il: int = 1, iu: int = 1,
+                  lo: float = -1e300, hi: float = 0.0):
+    """Lowest eigenpairs of each dense pencil (K_b, M_b) on the GPU
+    (dsygvx semantics, dense_eigensolver.cpp:44-133).  Returns lists (w_b, V_b)."""
+    B = len(Ks)
+    n = np.array([k.shape[0] for k in Ks], np.int64)
+    mat_off = np.zeros(B, np.int64)
+    mat_off[1:] = np.cumsum(n * n)[:-1]
+    Kf = np.concatenate([np.asfortranarray(k).ravel(order="F") for k in Ks]).astype(np.float64)
+    Mf = np.concatenate([np.asfortranarray(m).ravel(order="F") for m in Ms]).astype(np.float64)
+    cap = n.copy() if mode != "index" else np.minimum(n, iu - il + 1)
+    w_off = np.zeros(B, np.int64)
+    w_off[1:] = np.cumsum(cap)[:-1]
+    v_off = np.zeros(B, np.int64)
+    v_off[1:] = np.cumsum(n * cap)[:-1]
+    w = np.zeros(max(int(cap.sum()), 1))
+    V = np.zeros(max(int((n * cap).sum()), 1))
+    m = np.zeros(B, np.int64)
+    _lib.check(_lib.lib().amls_sygvx_batched(
+        solver._h, B, _lib.ptr(n), _lib.ptr(mat_off), _lib.ptr(Kf), _lib.ptr(Mf),
+        0 if mode == "index" else 1, int(il), int(iu), float(lo), float(hi), _lib.ptr(cap),
+        _lib.ptr(w_off), _lib.ptr(w), _lib.ptr(v_off), _lib.ptr(V), _lib.ptr(m)))
+    out = []
+    for b in range(B):
+        mb, nb = int(m[b]), int(n[b])
+        wb = w[w_off[b]:w_off[b] + mb].copy()
+        Vb = V[v_off[b]:v_off[b] + nb * mb].reshape(mb, nb).T.copy()
+        out.append((wb, Vb))
+    return out

@@ -1,0 +1,161 @@
+/* amls_b200.h - C ABI of the B200 AMLS eigensolver (libamls_b200.so).
+ *
+ * Solves K x = lambda M x for the lowest eigenpairs of a sparse symmetric
+ * positive-definite pencil by automated multilevel substructuring (AMLS),
+ * with nested dissection on the host (METIS) and every numeric phase
+ * (block elimination, congruence updates, local eigensolves, projection,
+ * reduced eigensolve, back-transform) in hand-written sm_100a kernels.
+ *
+ * Conventions (same as the reference, src/core/types.hpp:11-28):
+ *   - sparse input is CSR with int64 row pointers, int32 column indices
+ *     sorted within each row, float64 values; K and M symmetric (both
+ *     triangles stored);
+ *   - dense output is column-major;
+ *   - perm[new] = old.
+ * Every entry point returns an int status (AMLS_OK = 0).  No C++ exception
+ * crosses this boundary; amls_last_error() gives the message of the last
+ * failure on the calling thread.  A handle owns one CUDA stream and its
+ * device memory; calls on one handle must not overlap.
+ */
+#ifndef AMLS_B200_H
+#define AMLS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define AMLS_OK 0
+#define AMLS_ERR_INVALID_ARGUMENT 1 /* reference: std::invalid_argument           */
+#define AMLS_ERR_NOT_SPD 2          /* non-positive or NaN pivot (sparse_direct.cpp:17-22, 48-53) */
+#define AMLS_ERR_ITERATION 3        /* an iterative kernel hit its iteration cap  */
+#define AMLS_ERR_TIMEOUT 4          /* a bounded device-side wait expired         */
+#define AMLS_ERR_OOM 5              /* device allocation failed                   */
+#define AMLS_ERR_CUDA 6             /* other CUDA runtime error                   */
+#define AMLS_ERR_NUMERIC 7          /* reference: std::runtime_error (solver.cpp:202-203, 308-310) */
+#define AMLS_ERR_PARTITION 8        /* METIS failure (metis_partitioner.cpp:128-137) */
+#define AMLS_ERR_NO_DEVICE 9        /* no usable CUDA device                      */
+
+/* Options: the fields and defaults of AmlsOptions (src/amls/solver.hpp:18-30). */
+typedef struct amls_options {
+    int32_t nLevels;            /* 6    */
+    int32_t twoPass;            /* 1    */
+    int64_t leafSize;           /* 500  */
+    double thresholdFactor;     /* 2.0  (eta) */
+    int64_t fixedKeep;          /* 0    */
+    int64_t nev;                /* 100  */
+    int64_t denseProjectedMax;  /* 5000 (warning only, as in solver.cpp:339-342) */
+    double shift;               /* 0.0  K <- K + shift*M */
+    int32_t numThreads;         /* 0    host threads (partition/analysis)  */
+    int32_t recoverVectors;     /* 1    */
+    int32_t verbosity;          /* 1    */
+    int32_t reserved0;
+} amls_options;
+
+/* slots of the timing array filled by amls_solve (seconds) */
+#define AMLS_T_PARTITION 0     /* METIS + permutation + symbolic analysis (host) */
+#define AMLS_T_UPLOAD 1        /* host -> device copies of the pencil            */
+#define AMLS_T_ELIMINATION 2   /* front assembly, factorisation, Schur/congruence */
+#define AMLS_T_CONDENSE 3      /* local eigensolves + projection (both passes)   */
+#define AMLS_T_REDUCED 4       /* reduced eigensolve(s)                          */
+#define AMLS_T_BACKTRANSFORM 5 /* back-transform, un-permute, M-normalise        */
+#define AMLS_T_TOTAL 6
+#define AMLS_T_SLOTS 8
+
+typedef struct amls_handle_s* amls_handle;
+
+/* Fill *opt with the reference defaults. */
+int amls_options_default(amls_options* opt);
+
+/* Create a solver handle on CUDA device `device` (one stream, lazily grown
+ * device arena).  Replaces constructing AmlsSolver (src/amls/solver.hpp:32). */
+int amls_create(int device, amls_handle* out);
+int amls_destroy(amls_handle h);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* amls_last_error(void);
+
+/* Nested dissection of the graph of |K|+|M| (host only, no GPU needed).
+ * Replaces MetisPartitioner::recursiveBisection
+ * (src/partition/metis_partitioner.cpp:143-212).  All output arrays are
+ * caller-owned with capacity n (idx_ptr: n+1):
+ *   perm[n]            perm[new] = old
+ *   *n_nodes           number of tree nodes N
+ *   parent[N]          parent id, -1 for the root
+ *   role[N]            0 leaf, 1 separator, 2 root
+ *   left[N], right[N]  children ids, -1 for leaves
+ *   idx_ptr[N+1], idx[n]  node index lists (original indices) by node id */
+int amls_partition(int64_t n, const int64_t* k_rowptr, const int32_t* k_col,
+                   const int64_t* m_rowptr, const int32_t* m_col, int32_t nLevels,
+                   int64_t leafSize, int64_t* perm, int64_t* n_nodes, int64_t* parent,
+                   int32_t* role, int64_t* left, int64_t* right, int64_t* idx_ptr,
+                   int64_t* idx);
+
+/* Whole AMLS solve from host CSR arrays.  Replaces AmlsSolver::solve
+ * (src/amls/solver.cpp:154-373): optional shift, partition + permutation,
+ * two-pass truncation (k0 = max(4, ceil(3 nev / N)), lambda_cut = eta *
+ * lambda_hat) or fixedKeep, reduced eigensolve, back-transform, un-permute
+ * and M-normalisation.  Outputs (host, caller-owned):
+ *   theta[nev]      ascending Ritz values (nev clamped to n)
+ *   Z[n * nev]      M-normalised vectors, column-major, original ordering;
+ *                   may be NULL (or recoverVectors = 0) to skip recovery
+ *   *p_out          size of the final reduced problem
+ *   timing[AMLS_T_SLOTS] phase seconds, may be NULL */
+int amls_solve(amls_handle h, int64_t n, const int64_t* k_rowptr, const int32_t* k_col,
+               const double* k_val, const int64_t* m_rowptr, const int32_t* m_col,
+               const double* m_val, const amls_options* opt, double* theta, double* Z,
+               int64_t* p_out, double* timing);
+
+/* Split form of amls_solve for callers that reuse one sparsity pattern:
+ * amls_analyze runs the host phase (partition, permutation, symbolic fill,
+ * device plan) for a pattern; amls_solve_values then runs the numeric solve
+ * for values given either as host arrays (values_on_device = 0) or as device
+ * arrays of nnz(K), nnz(M) float64 already resident in HBM
+ * (values_on_device = 1).  Outputs as for amls_solve; with
+ * outputs_on_device = 1, theta and Z are device pointers. */
+int amls_analyze(amls_handle h, int64_t n, const int64_t* k_rowptr, const int32_t* k_col,
+                 const int64_t* m_rowptr, const int32_t* m_col, const amls_options* opt);
+int amls_solve_values(amls_handle h, const double* k_val, const double* m_val,
+                      int32_t values_on_device, double* theta, double* Z,
+                      int32_t outputs_on_device, int64_t* p_out, double* timing);
+
+/* Diagnostics of the last analysis/solve on the handle:
+ *   info[0] tree nodes, [1] levels, [2] p of pass A, [3] p of the final pass,
+ *   [4] sum of front sizes (doubles), [5] device bytes in use,
+ *   [6] kernel launches in the last numeric solve */
+#define AMLS_INFO_SLOTS 16
+int amls_info(amls_handle h, int64_t* info);
+
+/* Algorithmic work of the last numeric solve, from the host ledger built
+ * from the tree and the symbolic fronts (independent of the kernels):
+ *   work[0] fp64 flops, elimination      [1] bytes, elimination
+ *   work[2] fp64 flops, condensation     [3] bytes, condensation
+ *   work[4] fp64 flops, reduced          [5] bytes, reduced
+ *   work[6] fp64 flops, back-transform   [7] bytes, back-transform */
+#define AMLS_WORK_SLOTS 8
+int amls_work(amls_handle h, double* work);
+
+/* Batched dense generalized symmetric-definite eigensolver on the GPU,
+ * lowest eigenpairs of (K_b, M_b) for b = 0..batch-1.  Replaces
+ * LapackDenseEigensolver::solveIndex / solveInterval
+ * (src/linalg/dense_eigensolver.cpp:44-133: dsygvx, itype 1, uplo 'L',
+ * abstol 0): mode 0 = index range [il, iu] (1-based, il must be 1),
+ * mode 1 = value interval (lo, hi].  Host arrays, column-major, K_b and M_b
+ * of order n[b] at offsets mat_off[b] (doubles); on return
+ * w[w_off[b] ...] holds m[b] ascending eigenvalues and
+ * V[v_off[b] ...] the n[b] x m[b] M-orthonormal eigenvectors (capacity
+ * n[b] * cap[b] doubles, cap[b] = max vectors accepted).  K and M are not
+ * modified. */
+int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n, const int64_t* mat_off,
+                       const double* K, const double* M, int32_t mode, int64_t il, int64_t iu,
+                       double lo, double hi, const int64_t* cap, const int64_t* w_off,
+                       double* w, const int64_t* v_off, double* V, int64_t* m);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMLS_B200_H */

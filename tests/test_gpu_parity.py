@@ -1,0 +1,144 @@
+"""GPU parity tests through the C ABI: the CUDA path against the oracle
+(the CPU restatement of the reference) and against known answers.
+
+Tolerances: eigenvalues of the plain FP64 path within 1e-10 relative of the
+oracle's theta on the same input (same partition, same truncation); the
+keep-all case within 1e-10 of the closed-form spectrum
+(tests/unit/test_amls.cpp:110-151 of the reference); dense eigensolver
+within 1e-12 relative of LAPACK dsygvx (tests/unit/test_linalg.cpp:16-55).
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from amls_b200 import AmlsOptions, NotSPDError, cases, sygvx_batched
+from oracle import amls_ref as R
+
+from .helpers import oracle_solve, rel_err, residuals
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_pencil(n, rng):
+    A = rng.standard_normal((n, n))
+    K = A @ A.T + n * np.eye(n)
+    B = rng.standard_normal((n, n))
+    M = B @ B.T / n + np.eye(n)
+    return K, M
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 40, 200, 383, 390, 700])
+def test_sygvx_index_matches_lapack(solver, n):
+    rng = np.random.default_rng(n)
+    K, M = _rand_pencil(n, rng)
+    k = min(n, 12)
+    (w, V), = sygvx_batched(solver, [K], [M], mode="index", il=1, iu=k)
+    wr, Vr = R.LapackDense.solve_index(K, M, 1, k)
+    assert w.shape == wr.shape
+    assert rel_err(w, wr) < 1e-12
+    # M-orthonormal, residual small
+    assert np.allclose(V.T @ M @ V, np.eye(k), atol=1e-10)
+    res = np.linalg.norm(K @ V - M @ V * w[None, :], axis=0) / np.linalg.norm(K, 1)
+    assert res.max() < 1e-12
+
+
+def test_sygvx_interval_batched_uneven(solver):
+    rng = np.random.default_rng(5)
+    sizes = [3, 17, 64, 150, 420]
+    Ks, Ms = zip(*[_rand_pencil(n, rng) for n in sizes])
+    hi = 1.5 * np.median([sla.eigh(K, M, eigvals_only=True)[2] for K, M in zip(Ks, Ms)])
+    out = sygvx_batched(solver, list(Ks), list(Ms), mode="interval", lo=-1e300, hi=hi)
+    for (w, V), K, M in zip(out, Ks, Ms):
+        wr, _ = R.LapackDense.solve_interval(K, M, -1e300, hi)
+        assert w.shape == wr.shape            # same count in (lo, hi]
+        if w.size:
+            assert rel_err(w, wr) < 1e-12
+
+
+def test_keep_all_is_exact_grid(solver):
+    """Keep-all AMLS reproduces the closed-form 10x10 grid spectrum
+    (reference tests/unit/test_amls.cpp:110-151)."""
+    p = cases.grid_graph_2d(10, 10)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=10, nLevels=2, leafSize=20, fixedKeep=10 ** 6))
+    ref = cases.grid_graph_2d_spectrum(10, 10)[:10]
+    assert sol.p == 100
+    assert rel_err(sol.theta, ref) < 1e-10
+    assert residuals(p.K, p.M, sol.theta, sol.Z)[:3].max() < 1e-10
+
+
+def test_keep_all_is_exact_hex(solver):
+    p = cases.hex_pencil(4, 4, 4, 1, seed=3)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=15, nLevels=3, leafSize=60, fixedKeep=10 ** 6))
+    wr, _ = R.smallest_eigenpairs(p.K, p.M, 15)
+    assert rel_err(sol.theta, wr) < 1e-10
+
+
+@pytest.mark.parametrize("case", ["hex8_5", "grid_40", "path_600"])
+def test_two_pass_matches_oracle(solver, case):
+    if case == "hex8_5":
+        p = cases.hex_pencil(5, 5, 5, 1, seed=1)
+        o = dict(nev=20, nLevels=3, leafSize=100)
+    elif case == "grid_40":
+        p = cases.grid_graph_2d(40, 40)
+        o = dict(nev=30, nLevels=4, leafSize=150)
+    else:
+        p = cases.path_graph(600, True)
+        o = dict(nev=25, nLevels=4, leafSize=60)
+    ref = oracle_solve(p, R.OptionsRef(silMode=-1, **o))
+    sol = solver.solve(p.K, p.M, AmlsOptions(**o))
+    assert sol.p == ref.p
+    assert rel_err(sol.theta, ref.theta) < 1e-10
+    # vectors: same Ritz pairs up to sign -> compare residuals and M-norms
+    r = residuals(p.K, p.M, sol.theta, sol.Z)
+    rr = residuals(p.K, p.M, ref.theta, ref.Z)
+    assert np.all(r < 10 * rr + 1e-12)
+    mn = np.einsum("ij,ij->j", sol.Z, p.M @ sol.Z)
+    assert np.allclose(mn, 1.0, atol=1e-12)
+
+
+def test_c1_matches_oracle(solver):
+    """Config C1: 8-node hex 12^3 (6,084 DOF), L = 4, nev = 20."""
+    p = cases.config_pencil("C1")
+    o = dict(nev=20, nLevels=4, leafSize=500)
+    ref = oracle_solve(p, R.OptionsRef(silMode=-1, **o))
+    sol = solver.solve(p.K, p.M, AmlsOptions(**o))
+    assert sol.p == ref.p
+    assert rel_err(sol.theta, ref.theta) < 1e-10
+
+
+def test_fixed_keep_matches_oracle(solver):
+    p = cases.hex_pencil(6, 5, 4, 1, seed=7)
+    o = dict(nev=12, nLevels=3, leafSize=80, fixedKeep=6)
+    ref = oracle_solve(p, R.OptionsRef(silMode=-1, **o))
+    sol = solver.solve(p.K, p.M, AmlsOptions(**o))
+    assert sol.p == ref.p
+    assert rel_err(sol.theta, ref.theta) < 1e-10
+
+
+def test_shift_matches_oracle(solver):
+    p = cases.hex_pencil(4, 4, 5, 1, seed=2)
+    o = dict(nev=10, nLevels=3, leafSize=60, shift=0.5)
+    ref = oracle_solve(p, R.OptionsRef(silMode=-1, **o))
+    sol = solver.solve(p.K, p.M, AmlsOptions(**o))
+    assert rel_err(sol.theta, ref.theta) < 1e-10
+
+
+def test_not_spd_raises(solver):
+    """A non-SPD K is reported as NotSPDError (reference P10 check), and the
+    handle stays usable afterwards."""
+    p = cases.hex_pencil(3, 3, 3, 1, seed=0)
+    K = p.K.copy()
+    K.data = -K.data
+    with pytest.raises(NotSPDError):
+        solver.solve(K, p.M, AmlsOptions(nev=5, nLevels=2, leafSize=30))
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=5, nLevels=2, leafSize=30, fixedKeep=10 ** 6))
+    wr, _ = R.smallest_eigenpairs(p.K, p.M, 5)
+    assert rel_err(sol.theta, wr) < 1e-10
+
+
+def test_invalid_arguments(solver):
+    p = cases.path_graph(50)
+    with pytest.raises(ValueError):
+        solver.solve(p.K, p.M, AmlsOptions(nev=0))
+    with pytest.raises(ValueError):
+        solver.solve(p.K, p.M, AmlsOptions(nev=5, twoPass=False))
