@@ -27,13 +27,16 @@ AMLS_ERR_NO_DEVICE = 9
 T_SLOTS = 8
 INFO_SLOTS = 16
 WORK_SLOTS = 8
-TIMING_KEYS = ["partition", "upload", "elimination", "condense", "reduced", "backtransform", "total"]
+TIMING_KEYS = ["partition", "upload", "elimination", "condense", "reduced", "backtransform", "total",
+               "device"]
+PROF_CATS = ["cholesky", "trsm", "gemm", "front_update", "tridiag", "bisect", "inverse_iter",
+             "eigvec_backtransform", "other"]
 
 # every function the header declares (checked by the CPU tests)
 EXPORTS = [
     "amls_options_default", "amls_create", "amls_destroy", "amls_last_error", "amls_partition",
     "amls_solve", "amls_analyze", "amls_solve_values", "amls_info", "amls_work",
-    "amls_sygvx_batched",
+    "amls_sygvx_batched", "amls_set_profiling", "amls_kernel_times", "amls_category_work",
 ]
 
 
@@ -71,6 +74,9 @@ def lib() -> C.CDLL:
         L.amls_solve_values.argtypes = [P, P, P, C.c_int32, P, P, C.c_int32,
                                         C.POINTER(C.c_int64), P]
         L.amls_info.argtypes = [P, P]
+        L.amls_set_profiling.argtypes = [P, C.c_int32]
+        L.amls_kernel_times.argtypes = [P, P, P]
+        L.amls_category_work.argtypes = [P, P, P]
         L.amls_work.argtypes = [P, P]
         L.amls_sygvx_batched.argtypes = [P, C.c_int32, P, P, P, P, C.c_int32, C.c_int64,
                                          C.c_int64, C.c_double, C.c_double, P, P, P, P, P, P]

@@ -136,3 +136,27 @@ extern "C" int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n
         return AMLS_OK;
     });
 }
+
+extern "C" int amls_set_profiling(amls_handle h, int32_t on) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->setProfiling(on != 0);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_kernel_times(amls_handle h, double* ms, int64_t* launches) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->kernelTimes(ms, launches);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_category_work(amls_handle h, double* flops, double* bytes) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->categoryWork(flops, bytes);
+        return AMLS_OK;
+    });
+}

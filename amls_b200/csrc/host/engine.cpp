@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <numeric>
 #include <stdexcept>
@@ -62,9 +63,14 @@ double secs(Clock::time_point a, Clock::time_point b) {
 // kernels launched only from here
 cudaError_t launchGemmBatched(const GemmDesc*, const TileRef*, int, cudaStream_t);
 
+// Every kernel launch goes through LAUNCH: it counts launches and, when
+// kernel profiling is on, brackets the launch with CUDA events on the
+// engine stream (category from the launcher's name).
 #define LAUNCH(call)                                   \
     do {                                               \
+        const int cat_ = profBegin(#call);             \
         cudaCheck((call), #call);                      \
+        profEnd(cat_);                                 \
         ++launches_;                                   \
     } while (0)
 
@@ -83,9 +89,72 @@ Engine::Engine(int device) : device_(device) {
 
 Engine::~Engine() {
     cudaSetDevice(device_);
+    for (cudaEvent_t e : evPool_) cudaEventDestroy(e);
+    if (evSolve0_) cudaEventDestroy(evSolve0_);
+    if (evSolve1_) cudaEventDestroy(evSolve1_);
     if (stream_) {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
+    }
+}
+
+int Engine::profBegin(const char* text) {
+    if (!profiling_) return -1;
+    static const char* keys[kProfCats] = {"launchChol",   "launchTrsm",        "launchGemm",
+                                          "launchFrontUp", "launchTridiag",     "launchBisect",
+                                          "launchInverse", "launchBackTransform", ""};
+    int cat = kProfCats - 1;
+    for (int c = 0; c < kProfCats - 1; ++c)
+        if (std::strstr(text, keys[c])) {
+            cat = c;
+            break;
+        }
+    if (evUsed_ + 2 > evPool_.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            cudaCheck(cudaEventCreate(&e), "cudaEventCreate");
+            evPool_.push_back(e);
+        }
+    }
+    cudaCheck(cudaEventRecord(evPool_[evUsed_], stream_), "cudaEventRecord");
+    evCat_.push_back(cat);
+    return cat;
+}
+
+void Engine::profEnd(int cat) {
+    if (cat < 0) return;
+    cudaCheck(cudaEventRecord(evPool_[evUsed_ + 1], stream_), "cudaEventRecord");
+    evUsed_ += 2;
+}
+
+void Engine::profCollect() {
+    if (!profiling_ || evUsed_ == 0) return;
+    cudaCheck(cudaStreamSynchronize(stream_), "profile");
+    for (size_t k = 0; k + 1 < evUsed_; k += 2) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, evPool_[k], evPool_[k + 1]);
+        const int c = evCat_[k / 2];
+        profMs_[c] += ms;
+        profCount_[c] += 1;
+    }
+    evUsed_ = 0;
+    evCat_.clear();
+}
+
+void Engine::setProfiling(bool on) {
+    profiling_ = on;
+    for (int c = 0; c < kProfCats; ++c) {
+        profMs_[c] = 0;
+        profCount_[c] = 0;
+    }
+    evUsed_ = 0;
+    evCat_.clear();
+}
+
+void Engine::kernelTimes(double* ms, int64_t* counts) const {
+    for (int c = 0; c < kProfCats; ++c) {
+        if (ms) ms[c] = profMs_[c];
+        if (counts) counts[c] = profCount_[c];
     }
 }
 
@@ -423,7 +492,20 @@ void Engine::buildStatic() {
     }
     sblob_.upload(staticBlob_, stream_);
 
-    // ---- ledger: elimination flops/bytes ----
+    // ---- ledger: elimination flops/bytes (total and per kernel category) ----
+    for (int c = 0; c < kProfCats; ++c) elimCatF_[c] = elimCatB_[c] = 0;
+    for (const Node& nd : nodes_) {
+        const double nn = static_cast<double>(nd.n), s = static_cast<double>(nd.S.size());
+        elimCatF_[0] += nn * nn * nn / 3.0 + s * nn * nn;               // Cholesky
+        elimCatB_[0] += 8.0 * 2.0 * (nn + s) * nn;
+        elimCatF_[1] += (nn + s) * nn * nn + nn * nn * nn;               // TRSMs (G, C)
+        elimCatB_[1] += 8.0 * (2.0 * (nn + s) * nn + 2.0 * nn * nn + nn * nn);
+        elimCatF_[2] += 2.0 * s * nn * nn;                               // R GEMM
+        elimCatB_[2] += 8.0 * (2.0 * s * nn + nn * nn + s * nn);
+        elimCatF_[3] += 3.0 * s * s * nn;                                // extend-add
+        elimCatB_[3] += 8.0 * (2.0 * s * nn + 2.0 * s * s);
+        elimCatB_[8] += 8.0 * (2.0 * (nn + s) * nn + 2.0 * nn * nn);     // assembly, transposes
+    }
     double fe = 0, be = 0;
     for (const Node& nd : nodes_) {
         const double nn = static_cast<double>(nd.n), s = static_cast<double>(nd.S.size());
@@ -525,6 +607,14 @@ void Engine::tridiagonalizeAll(cudaStream_t s) {
     }
     const size_t oGo = b.add(groupOf), oGf = b.add(groupFirst), oGs = b.add(groupSize), oPo = b.add(pOff);
     b.upload(tlBlob_, s);
+    for (const auto& e : small) {
+        catF_[4] += 4.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
+        catB_[4] += 8.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
+    }
+    for (const auto& e : large) {
+        catF_[4] += 4.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
+        catB_[4] += 8.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
+    }
     if (!small.empty()) LAUNCH(launchTridiagSmall(b.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
     if (!large.empty()) {
         redP_.ensure(sizeof(double) * static_cast<size_t>(pTot));
@@ -685,6 +775,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     const double* wDev = wPool_.as<double>();
 
     double fc = 0, bc = 0;
+    const double fcEig = 0.0;
     for (int l = 0; l <= maxLevel_; ++l) {
         std::vector<CopyDesc> cp;
         std::vector<TrsmDesc> tr;
@@ -793,11 +884,19 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i1D), b.dev<TileRef>(T.i1T), T.ni1T, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i2D), b.dev<TileRef>(T.i2T), T.ni2T, s));
     }
-    // ledger (local eig: bisection + inverse iteration + back-transform)
+    // ledger (local eig: bisection + inverse iteration + back-transform;
+    // tridiagonalisation counted once per solve)
     for (int i = 0; i < N; ++i) {
         const double nn = static_cast<double>(nodes_[static_cast<size_t>(i)].n), kk = P.k[static_cast<size_t>(i)];
         fc += 4.0 * nn * nn * kk;
+        catF_[5] += 60.0 * 6.0 * nn * kk;
+        catF_[6] += 4.0 * 12.0 * nn * kk;
+        catB_[6] += 8.0 * 6.0 * nn * kk;
+        catF_[7] += 4.0 * nn * nn * kk;
+        catB_[7] += 8.0 * (nn * nn / 2.0 + 2.0 * nn * kk);
     }
+    catF_[2] += fc - fcEig;   // projection GEMMs / TRSMs share the GEMM and TRSM pipes
+    catB_[2] += bc;
     work_[2] += fc;
     work_[3] += bc;
     cudaCheck(cudaStreamSynchronize(s), "condense");
@@ -856,6 +955,13 @@ int Engine::reducedSolve(Pass& P, int want, cudaStream_t s) {
     P.theta.resize(static_cast<size_t>(want));
     for (int j = 0; j < want; ++j) P.theta[static_cast<size_t>(j)] = 1.0 / nu[static_cast<size_t>(j)];
     const double pp = static_cast<double>(p);
+    catF_[4] += 4.0 / 3.0 * pp * pp * pp;
+    catB_[4] += 8.0 / 3.0 * pp * pp * pp;
+    catF_[5] += 60.0 * 6.0 * pp * want;
+    catF_[6] += 4.0 * 12.0 * pp * want;
+    catB_[6] += 8.0 * 6.0 * pp * want;
+    catF_[7] += 4.0 * pp * pp * want;
+    catB_[7] += 8.0 * (pp * pp / 2.0 + 2.0 * pp * want);
     work_[4] += 4.0 / 3.0 * pp * pp * pp + 4.0 * pp * pp * want;
     work_[5] += 8.0 * pp * pp * pp / 3.0;
     return want;
@@ -928,6 +1034,9 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
     LAUNCH(launchMNorm(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n_, invDev_.as<int64_t>(), zt, m,
                        norms_.as<double>(), s));
     LAUNCH(launchUnpermute(zt, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
+    catF_[2] += fb;
+    catB_[2] += 8.0 * 3.0 * m * static_cast<double>(n_);
+    catB_[8] += 8.0 * (12.0 * nnzM_ + 3.0 * m * static_cast<double>(n_));
     work_[6] += fb + 4.0 * static_cast<double>(nnzM_) * m;
     work_[7] += 8.0 * (2.0 * m * n_ * 3 + 12.0 * nnzM_);
     cudaCheck(cudaStreamSynchronize(s), "backtransform");
@@ -945,8 +1054,17 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     cudaStream_t s = stream_;
     launches_ = 0;
     for (int t = 2; t < AMLS_WORK_SLOTS; ++t) work_[t] = 0;
+    for (int c = 0; c < kProfCats; ++c) {
+        catF_[c] = elimCatF_[c];
+        catB_[c] = elimCatB_[c];
+    }
     tridiagDone_ = false;
     const auto t0 = Clock::now();
+    if (!evSolve0_) {
+        cudaCheck(cudaEventCreate(&evSolve0_), "cudaEventCreate");
+        cudaCheck(cudaEventCreate(&evSolve1_), "cudaEventCreate");
+    }
+    cudaCheck(cudaEventRecord(evSolve0_, s), "cudaEventRecord");
     cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
     if (valuesOnDevice) {
         cudaCheck(cudaMemcpyAsync(kVal_.as<double>(), kv, sizeof(double) * nnzK_, cudaMemcpyDeviceToDevice, s), "values");
@@ -1015,8 +1133,10 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
         if (recover)
             cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * want * n_, cudaMemcpyDeviceToHost, s), "Z");
     }
+    cudaCheck(cudaEventRecord(evSolve1_, s), "cudaEventRecord");
     cudaCheck(cudaStreamSynchronize(s), "outputs");
     const auto t6 = Clock::now();
+    profCollect();
     if (pOut) *pOut = P.p;
     if (timing) {
         timing[AMLS_T_UPLOAD] = secs(t0, t1);
@@ -1025,6 +1145,7 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
         timing[AMLS_T_REDUCED] = tRed;
         timing[AMLS_T_BACKTRANSFORM] = secs(t4, t5) + secs(t5, t6);
         timing[AMLS_T_TOTAL] = secs(t0, t6);
+        timing[AMLS_T_DEVICE] = elapsed(evSolve0_, evSolve1_);
     }
 }
 
@@ -1232,6 +1353,13 @@ void Engine::info(int64_t* out) const {
     cudaMemGetInfo(&freeB, &totB);
     out[5] = static_cast<int64_t>(totB - freeB);
     out[6] = launches_;
+}
+
+void Engine::categoryWork(double* flops, double* bytes) const {
+    for (int c = 0; c < kProfCats; ++c) {
+        if (flops) flops[c] = catF_[c];
+        if (bytes) bytes[c] = catB_[c];
+    }
 }
 
 void Engine::work(double* out) const {

@@ -52,6 +52,12 @@ public:
                       double* V, int64_t* m);
 
     void info(int64_t* out) const;
+    // per-category kernel timing with CUDA events on the engine stream
+    static constexpr int kProfCats = 9;
+    void setProfiling(bool on);
+    void kernelTimes(double* ms, int64_t* counts) const;
+    // algorithmic flops / bytes of the last numeric solve per kernel category
+    void categoryWork(double* flops, double* bytes) const;
     void work(double* out) const;
     bool analyzed() const { return analyzed_; }
 
@@ -91,6 +97,9 @@ private:
     void selectEigen(std::vector<EigDesc>& descs, int mode, int want, double thr, bool tridiag,
                      cudaStream_t s);
     double elapsed(cudaEvent_t a, cudaEvent_t b);
+    int profBegin(const char* text);
+    void profEnd(int cat);
+    void profCollect();
 
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
@@ -148,9 +157,20 @@ private:
     std::vector<int64_t> panelOff_;                // per node (doubles), -1 none
     std::vector<int64_t> yOff_;                    // per node (doubles into yPool_)
 
+    // kernel profiling
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> evPool_;
+    size_t evUsed_ = 0;
+    std::vector<int> evCat_;
+    double profMs_[kProfCats] = {0};
+    int64_t profCount_[kProfCats] = {0};
+    cudaEvent_t evSolve0_ = nullptr, evSolve1_ = nullptr;
+
     // diagnostics / ledger
     int64_t pA_ = 0, pFinal_ = 0, launches_ = 0;
     double work_[AMLS_WORK_SLOTS] = {0};
+    double catF_[kProfCats] = {0}, catB_[kProfCats] = {0};
+    double elimCatF_[kProfCats] = {0}, elimCatB_[kProfCats] = {0};
 };
 
 }  // namespace amls_b200

@@ -342,10 +342,16 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
     const int n = D.n;
     if (j >= k || n <= 0) return;
     const int tid = threadIdx.x;
-    // T norm and cluster tolerance (dstein: ortol = 1e-3 * onenrm)
+    // T norm and cluster tolerance.  LAPACK's dstein groups eigenvalues
+    // closer than 1e-3 |T|; that makes clusters of hundreds of the reduced
+    // problem's eigenvalues and serialises them.  Vectors of eigenvalues
+    // separated by g come out of inverse iteration orthogonal to about
+    // eps |T| / g, so grouping only gaps below 1e-6 |T| keeps every pair
+    // orthogonal to ~1e-10 while the clusters stay small and run in
+    // parallel (one CTA each).
     double lo, hi, pivmin, tnorm;
     gershgorin(D.d, D.e, n, lo, hi, pivmin, tnorm);
-    const double ortol = 1e-3 * tnorm;
+    const double ortol = 1e-6 * tnorm;
     // cluster start: j is a start if j == 0 or |w[j] - w[j-1]| > ortol
     if (j > 0 && fabs(D.w[j] - D.w[j - 1]) <= ortol) return;
     int jend = j + 1;

@@ -123,6 +123,46 @@ class AmlsSolver:
         return Solution(theta[:nev].copy(), None if Z is None else Z.T.copy(), int(p.value),
                         dict(zip(_lib.TIMING_KEYS, timing.tolist())), self.info())
 
+    # ---- split form: analysis once, numeric solves on resident values ----
+    def analyze(self, K, M, opt: AmlsOptions) -> None:
+        kp, kc, _ = _csr_arrays(K)
+        mp, mc, _ = _csr_arrays(M)
+        self._n = K.shape[0]
+        self._nev = max(0, min(int(opt.nev), self._n))
+        o = opt.to_c()
+        _lib.check(_lib.lib().amls_analyze(self._h, self._n, _lib.ptr(kp), _lib.ptr(kc),
+                                           _lib.ptr(mp), _lib.ptr(mc), C.byref(o)))
+
+    def solve_values(self, k_val_ptr: int, m_val_ptr: int, values_on_device: bool,
+                     theta_ptr: int, z_ptr: int | None, outputs_on_device: bool) -> dict:
+        """Numeric solve on the analysed pattern; pointers are raw addresses
+        (device addresses when the *_on_device flags are set)."""
+        p = C.c_int64(0)
+        timing = np.zeros(_lib.T_SLOTS, np.float64)
+        _lib.check(_lib.lib().amls_solve_values(
+            self._h, C.c_void_p(k_val_ptr), C.c_void_p(m_val_ptr), 1 if values_on_device else 0,
+            C.c_void_p(theta_ptr), None if z_ptr is None else C.c_void_p(z_ptr),
+            1 if outputs_on_device else 0, C.byref(p), _lib.ptr(timing)))
+        out = dict(zip(_lib.TIMING_KEYS, timing.tolist()))
+        out["p"] = int(p.value)
+        return out
+
+    def set_profiling(self, on: bool) -> None:
+        _lib.check(_lib.lib().amls_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(len(_lib.PROF_CATS), np.float64)
+        cnt = np.zeros(len(_lib.PROF_CATS), np.int64)
+        _lib.check(_lib.lib().amls_kernel_times(self._h, _lib.ptr(ms), _lib.ptr(cnt)))
+        return {k: (float(a), int(b)) for k, a, b in zip(_lib.PROF_CATS, ms, cnt)}
+
+    def category_work(self) -> dict:
+        """Algorithmic (flops, bytes) of the last solve per kernel category."""
+        f = np.zeros(len(_lib.PROF_CATS), np.float64)
+        b = np.zeros(len(_lib.PROF_CATS), np.float64)
+        _lib.check(_lib.lib().amls_category_work(self._h, _lib.ptr(f), _lib.ptr(b)))
+        return {k: (float(x), float(y)) for k, x, y in zip(_lib.PROF_CATS, f, b)}
+
     def info(self) -> dict:
         buf = np.zeros(_lib.INFO_SLOTS, np.int64)
         _lib.check(_lib.lib().amls_info(self._h, _lib.ptr(buf)))

@@ -1,0 +1,355 @@
+"""Benchmark: AMLS solve time of the 27-node hex elasticity pencil on a
+14^3 element cube (70,644 DOF, ~12.4M nnz per matrix), lowest 500
+eigenpairs, METIS nested dissection to 8 levels, eta = 2, two-pass
+truncation, FP64 - on one B200 (replicas on N GPUs).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: the pencil's pattern is analysed once (partition, permutation,
+symbolic fill: host work that depends only on the sparsity); each timed step
+is one numeric solve from K and M values already resident in HBM to theta and
+Z in HBM, timed with CUDA events on the solver's stream (amls_solve_values).
+The L2 is flushed (a 256 MiB write) between timed steps.  `e2e` is the
+public C-ABI call amls_solve with host CSR arrays in and host theta/Z out,
+including partition, host->device and device->host copies, timed with the
+host clock around the synchronous call.
+
+Reference arm (--impl reference): the CPU restatement of the reference
+algorithm (oracle/) on the host cores, on a bounded sample of the same
+workload - the sub-pencil of one depth-3 subtree of the same partition tree
+(about 1/8 of the cube) solved end to end with nev scaled by its size -
+scaled to the full workload by the algorithmic work model in
+oracle/workmodel.py.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "AMLS solve s at n≈70k,k=500: mixed vs FP64 on 1 B200 at rel-λ err≤1e-8"
+CONFIGS = {
+    "C1": dict(nev=20, nLevels=4, workload="C1: 8-node hex elasticity, 12^3 elements, 6,084 DOF, nev 20"),
+    "C2": dict(nev=100, nLevels=6, workload="C2: 27-node hex elasticity, 7^3 elements, 9,450 DOF, nev 100"),
+    "C4": dict(nev=50, nLevels=6, workload="C4: 27-node hex elasticity, 10^3 elements, 26,460 DOF, nev 50"),
+    "C5": dict(nev=500, nLevels=8, workload="C5: 27-node hex elasticity, 14^3 elements, 70,644 DOF, nev 500"),
+}
+
+
+def workload(name):
+    c = CONFIGS[name]
+    return dict(workload=c["workload"], nev=c["nev"], nLevels=c["nLevels"], leafSize=500, eta=2.0,
+                seed=0, precision="fp64", refinement="none",
+                l2="flushed between timed steps (256 MiB write)")
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled every 200 ms during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for k, v in zip(names, s[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from amls_b200 import AmlsOptions, AmlsSolver, cases
+
+    dev = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(dev)
+    cfg = CONFIGS[args.config]
+    p = cases.config_pencil(args.config, seed=0)
+    n, nev = p.n, cfg["nev"]
+    opt = AmlsOptions(nev=nev, nLevels=cfg["nLevels"], leafSize=500, thresholdFactor=2.0,
+                      verbosity=0)
+    s = AmlsSolver(dev)
+    s.analyze(p.K, p.M, opt)
+    kv = torch.from_numpy(np.ascontiguousarray(p.K.data)).cuda()
+    mv = torch.from_numpy(np.ascontiguousarray(p.M.data)).cuda()
+    theta = torch.zeros(nev, dtype=torch.float64, device="cuda")
+    Z = torch.zeros(nev * n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        return s.solve_values(kv.data_ptr(), mv.data_ptr(), True, theta.data_ptr(),
+                              Z.data_ptr(), True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    s.set_profiling(True)
+    dev_times = []
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = step()
+            dev_times.append(r["device"])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    ktimes = s.kernel_times()
+    s.set_profiling(False)
+    info = s.info()
+    work = s.work()
+    t_step = float(np.mean(dev_times))
+    if dist:
+        tt = torch.tensor([t_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+
+    # e2e through the public C ABI with host buffers
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 2))
+    e2e = []
+    sol = None
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sol = s.solve(p.K, p.M, opt)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    h2d = sum(a.nbytes for a in (p.K.indptr.astype(np.int64), p.K.indices, p.K.data,
+                                 p.M.indptr.astype(np.int64), p.M.indices, p.M.data))
+    d2h = nev * 8 + n * nev * 8
+    e2e_t = float(np.mean(e2e)) if e2e else None
+    if dist and e2e_t is not None:
+        tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+
+    # roofline of the dominant kernel category
+    pk, src = peaks()
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    dom_ms, dom_launches = ktimes[dom]
+    roof = dominant_roofline(dom, dom_ms / max(args.steps, 1), dom_launches / max(args.steps, 1),
+                             work, info, pk, src, s)
+    line = {
+        "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded hex-elasticity pencil)",
+        "config": dict(workload(args.config), parallelism="replicas" if world > 1 else "single GPU",
+                       p_final=info["p"], p_passA=info["p_passA"], tree_nodes=info["tree_nodes"]),
+        "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(info["launches"]),
+        "roofline": roof,
+        "clocks": clk.summary(),
+        "wall_s_per_step": wall / max(args.steps, 1),
+        "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in ktimes.items()},
+        "phase_s_last_e2e": sol.timing if sol is not None else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu and args.config == "C5":
+        line["cpu_baseline"] = cpu_sample(args)
+    return line
+
+
+def dominant_roofline(cat, ms, launches, work, info, pk, src, s):
+    """Roofline of the dominant kernel category from the engine's ledger."""
+    from amls_b200 import _lib
+    led = s.category_work()
+    flops, byts = led.get(cat, (0.0, 0.0))
+    t = ms * 1e-3
+    tensor_bound = cat in ("gemm", "front_update", "cholesky", "trsm")
+    if tensor_bound:
+        peak = pk.get("fp64_tflops") or 40.0
+        psrc = "nominal B200 FP64 (no measured FP64 peak)" if not pk.get("fp64_tflops") else src
+        ach = flops / t / 1e12 if t > 0 else 0.0
+        return {"bound": "tensor", "kernel": cat, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "traffic": None, "peak_source": psrc,
+                "launches_per_step": launches, "ms_per_step": ms}
+    peak = pk.get("hbm_gbs", 6650.0)
+    ach = byts / t / 1e9 if t > 0 else 0.0
+    del _lib, work, info
+    return {"bound": "hbm", "kernel": cat, "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "traffic": None, "peak_source": src,
+            "launches_per_step": launches, "ms_per_step": ms}
+
+
+# --------------------------------------------------------------------------
+# reference arm: oracle on a bounded sample, scaled by the work model
+# --------------------------------------------------------------------------
+
+def cpu_sample(args, depth=3):
+    import scipy.sparse as sp
+
+    from amls_b200 import cases
+    from amls_b200.solver import recursive_bisection
+    from oracle import amls_ref as R
+    from oracle import workmodel as WM
+    from oracle.tree import Tree
+
+    p = cases.config_pencil("C5", seed=0)
+    perm, t = recursive_bisection(p.K, p.M, 8, 500)
+    tree = Tree.from_arrays(**t)
+    # first node at the given depth (root = depth 0), following left children
+    node = tree.root()
+    for _ in range(depth):
+        if not tree.children[node]:
+            break
+        node = tree.children[node][0]
+    sub_nodes = []
+    stack = [node]
+    while stack:
+        x = stack.pop()
+        sub_nodes.append(x)
+        stack.extend(tree.children[x])
+    idx = np.sort(np.concatenate([tree.indices[x] for x in sub_nodes]))
+    loc = {old: new for new, old in enumerate(idx.tolist())}
+    remap = {x: j for j, x in enumerate(sorted(sub_nodes))}
+    sub = Tree(parent=[remap[tree.parent[x]] if x != node else -1 for x in sorted(sub_nodes)],
+               role=[tree.role[x] if x != node else (2 if tree.children[x] else 0)
+                     for x in sorted(sub_nodes)],
+               children=[[remap[c] for c in tree.children[x]] for x in sorted(sub_nodes)],
+               indices=[np.array([loc[v] for v in tree.indices[x].tolist()], dtype=np.int64)
+                        for x in sorted(sub_nodes)])
+    Ks = sp.csr_matrix(p.K[idx, :][:, idx])
+    Ms = sp.csr_matrix(p.M[idx, :][:, idx])
+    nev_s = max(10, int(round(500 * len(idx) / p.n)))
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    sol = R.amls_solve_ref(Ks, Ms, sub, R.OptionsRef(nev=nev_s, nLevels=8 - depth, leafSize=500,
+                                                      silMode=0))
+    t_s = time.perf_counter() - t0
+    w_s = WM.amls_work(Ks, Ms, sub, sol.p, sol.p_passA)
+    scale_p = p.n / len(idx)
+    w_f = WM.amls_work(p.K, p.M, tree, int(sol.p * scale_p), int(sol.p_passA * scale_p))
+    return {"value": t_s * w_f / w_s, "unit": "s", "cores": cores, "kind": "port",
+            "sample": (f"oracle (reference algorithm restated, numpy/scipy FP64, BLAS threads = "
+                       f"host cores) on the sub-pencil of one depth-{depth} subtree of the same "
+                       f"partition ({len(idx)} DOF, nev {nev_s}), {t_s:.2f} s, scaled by the "
+                       f"algorithmic work model ratio {w_f / w_s:.1f}")}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    times = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        last = cpu_sample(args)
+        if i >= args.warmup:
+            times.append(last["value"])
+    v = float(np.mean(times)) if times else last["value"]
+    last["value"] = v
+    return {
+        "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic (seeded hex-elasticity pencil)", "config": workload("C5"),
+        "cpu_baseline": last,
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="C5", choices=["C1", "C2", "C4", "C5"],
+                    help="workload (C5 is the benchmark; smaller ones for profiling)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the e2e leg (profiling runs)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as d
+        torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+        d.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = d
+    line = run_ours(args, rank, world, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -62,7 +62,8 @@ typedef struct amls_options {
 #define AMLS_T_CONDENSE 3      /* local eigensolves + projection (both passes)   */
 #define AMLS_T_REDUCED 4       /* reduced eigensolve(s)                          */
 #define AMLS_T_BACKTRANSFORM 5 /* back-transform, un-permute, M-normalise        */
-#define AMLS_T_TOTAL 6
+#define AMLS_T_TOTAL 6         /* host wall clock of the call                    */
+#define AMLS_T_DEVICE 7        /* CUDA-event time of the numeric solve on the handle's stream */
 #define AMLS_T_SLOTS 8
 
 typedef struct amls_handle_s* amls_handle;
@@ -137,6 +138,21 @@ int amls_info(amls_handle h, int64_t* info);
  *   work[6] fp64 flops, back-transform   [7] bytes, back-transform */
 #define AMLS_WORK_SLOTS 8
 int amls_work(amls_handle h, double* work);
+
+/* Kernel profiling: when on, every kernel launch of the handle is bracketed
+ * by CUDA events on its stream and the times are summed per category:
+ *   0 Cholesky (diag+panel) 1 TRSM 2 batched GEMM 3 front extend-add
+ *   4 tridiagonalisation 5 bisection 6 inverse iteration 7 eigenvector
+ *   back-transform 8 other (assembly, transposes, norms)
+ * amls_kernel_times returns milliseconds and launch counts accumulated since
+ * the last amls_set_profiling call. */
+#define AMLS_PROF_CATS 9
+int amls_set_profiling(amls_handle h, int32_t on);
+int amls_kernel_times(amls_handle h, double* ms, int64_t* launches);
+/* Algorithmic work of the last numeric solve per kernel category (same
+ * categories): FP64 flops and the minimum bytes each category must move,
+ * from the host ledger (tree + symbolic fronts), not from counters. */
+int amls_category_work(amls_handle h, double* flops, double* bytes);
 
 /* Batched dense generalized symmetric-definite eigensolver on the GPU,
  * lowest eigenpairs of (K_b, M_b) for b = 0..batch-1.  Replaces
