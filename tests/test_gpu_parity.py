@@ -142,3 +142,17 @@ def test_invalid_arguments(solver):
         solver.solve(p.K, p.M, AmlsOptions(nev=0))
     with pytest.raises(ValueError):
         solver.solve(p.K, p.M, AmlsOptions(nev=5, twoPass=False))
+
+
+def test_c5_matches_oracle_golden(solver):
+    """Full-size workload (27-node hex 14^3, 70,644 DOF, nev 500, L 8): the
+    GPU theta equal the oracle's golden theta (tests/golden/make_c5_golden.py)
+    within 1e-10, with the same reduced sizes."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c5_oracle.npz"))
+    p = cases.config_pencil("C5", seed=0)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=500, nLevels=8, leafSize=500,
+                                             recoverVectors=False))
+    assert sol.p == int(g["p"])
+    assert sol.info["p_passA"] == int(g["p_passA"])
+    assert rel_err(sol.theta, g["theta"]) < 1e-10
