@@ -170,6 +170,28 @@ int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n, const int
                        double lo, double hi, const int64_t* cap, const int64_t* w_off,
                        double* w, const int64_t* v_off, double* V, int64_t* m);
 
+/* Allocation-free dense generalized eigensolver (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: code inside a
+ * CUDA graph capture, hosts whose memory pool owns every allocation, or
+ * loops that must not enter the allocator.  Lowest k eigenpairs of one dense
+ * pencil (K, M), M positive definite, of order n <= AMLS_NOALLOC_MAX_N:
+ * same semantics as amls_sygvx_batched in index mode (il = 1, iu = k).
+ *   K, M   device pointers, n x n column-major (read only)
+ *   w      device pointer, k eigenvalues ascending
+ *   V      device pointer, n x k M-orthonormal eigenvectors, column-major
+ *   *m     host: number of eigenpairs returned
+ *   stream CUDA stream (cudaStream_t) or NULL for the default stream
+ * No handle, and no cudaMalloc/cudaFree or other allocating call: every
+ * intermediate lives in a fixed-size device array inside the library
+ * (about 1.5 MB, held on each GPU that loads the library until exit).  The
+ * first call on a device looks up that array's address (make it before any
+ * stream capture).  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  The call is synchronous on
+ * `stream`.  Sizes beyond the limit return AMLS_ERR_INVALID_ARGUMENT. */
+#define AMLS_NOALLOC_MAX_N 128
+int amls_sygvx_lowest_noalloc(int64_t n, const double* K, const double* M, int64_t k,
+                              double* w, double* V, int64_t* m, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
