@@ -37,7 +37,7 @@ EXPORTS = [
     "amls_options_default", "amls_create", "amls_destroy", "amls_last_error", "amls_partition",
     "amls_solve", "amls_analyze", "amls_solve_values", "amls_info", "amls_work",
     "amls_sygvx_batched", "amls_set_profiling", "amls_kernel_times", "amls_category_work",
-    "amls_sygvx_lowest_noalloc",
+    "amls_sygvx_lowest_noalloc", "amls_sensitivities",
 ]
 NOALLOC_MAX_N = 128
 
@@ -48,7 +48,8 @@ class Options(C.Structure):
         ("nLevels", C.c_int32), ("twoPass", C.c_int32), ("leafSize", C.c_int64),
         ("thresholdFactor", C.c_double), ("fixedKeep", C.c_int64), ("nev", C.c_int64),
         ("denseProjectedMax", C.c_int64), ("shift", C.c_double), ("numThreads", C.c_int32),
-        ("recoverVectors", C.c_int32), ("verbosity", C.c_int32), ("reserved0", C.c_int32),
+        ("recoverVectors", C.c_int32), ("verbosity", C.c_int32), ("refine", C.c_int32),
+        ("refineMaxIter", C.c_int32), ("refineExtra", C.c_int32), ("refineTol", C.c_double),
     ]
 
 
@@ -79,6 +80,8 @@ def lib() -> C.CDLL:
         L.amls_set_profiling.argtypes = [P, C.c_int32]
         L.amls_kernel_times.argtypes = [P, P, P]
         L.amls_category_work.argtypes = [P, P, P]
+        L.amls_sensitivities.argtypes = [P, C.c_int64, C.c_int32, P, P, P, P, C.c_double, P, P,
+                                         P, P, P]
         L.amls_sygvx_lowest_noalloc.argtypes = [C.c_int64, P, P, C.c_int64, P, P,
                                                 C.POINTER(C.c_int64), P]
         L.amls_work.argtypes = [P, P]

@@ -32,6 +32,10 @@ extern "C" int amls_options_default(amls_options* opt) {
     opt->numThreads = 0;
     opt->recoverVectors = 1;
     opt->verbosity = 1;
+    opt->refine = 0;
+    opt->refineMaxIter = 60;
+    opt->refineExtra = -1;
+    opt->refineTol = 1e-9;
     return AMLS_OK;
 }
 

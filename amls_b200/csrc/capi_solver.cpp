@@ -160,3 +160,17 @@ extern "C" int amls_category_work(amls_handle h, double* flops, double* bytes) {
         return AMLS_OK;
     });
 }
+
+extern "C" int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, const int64_t* dofmap,
+                                  const double* Kbar, const double* Mbar, const double* weights,
+                                  double gapTol, double* gE, double* gRho, double* dE, double* dRho,
+                                  int32_t* simple) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (nelem <= 0 || !dofmap || !Kbar || !Mbar)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "amls_sensitivities: bad element data");
+        h->eng->sensitivities(nelem, ndofe, dofmap, Kbar, Mbar, weights, gapTol, gE, gRho, dE, dRho,
+                              simple);
+        return AMLS_OK;
+    });
+}

@@ -1028,12 +1028,6 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
         LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
     }
-    // M-normalise and un-permute
-    norms_.ensure(sizeof(double) * static_cast<size_t>(m));
-    zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
-    LAUNCH(launchMNorm(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n_, invDev_.as<int64_t>(), zt, m,
-                       norms_.as<double>(), s));
-    LAUNCH(launchUnpermute(zt, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
     catF_[2] += fb;
     catB_[2] += 8.0 * 3.0 * m * static_cast<double>(n_);
     catB_[8] += 8.0 * (12.0 * nnzM_ + 3.0 * m * static_cast<double>(n_));
@@ -1117,11 +1111,29 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     if (P.p > opt_.denseProjectedMax && opt_.verbosity > 0)
         std::fprintf(stderr, "[amls_b200] warning: p=%lld exceeds denseProjectedMax=%lld (dense solve used)\n",
                      static_cast<long long>(P.p), static_cast<long long>(opt_.denseProjectedMax));
-    const int want = reducedSolve(P, static_cast<int>(std::min<int64_t>(nev, P.p)), s);
+    int64_t nq = std::min<int64_t>(nev, P.p);
+    if (opt_.refine) {
+        const int64_t extra = opt_.refineExtra >= 0 ? opt_.refineExtra : nev / 2 + 16;
+        nq = std::min<int64_t>(P.p, std::min<int64_t>(n_, nev + extra));
+    }
+    const int got = reducedSolve(P, static_cast<int>(nq), s);
+    const int want = static_cast<int>(std::min<int64_t>(nev, got));
     const auto t4 = Clock::now();
     tRed += secs(t3, t4);
     const bool recover = opt_.recoverVectors && Z != nullptr;
-    if (recover) backtransform(P, want, s);
+    refineIters_ = 0;
+    refineNq_ = 0;
+    if (opt_.refine) {
+        backtransform(P, got, s);
+        refineNq_ = got;
+        refineIters_ = refine(ztPool_.as<double>(), got, want, P.theta, s);
+        P.theta.resize(static_cast<size_t>(want));
+        if (recover) finalizeVectors(ztPool_.as<double>(), got, want, s);
+    } else if (recover) {
+        backtransform(P, want, s);
+        finalizeVectors(ztPool_.as<double>(), want, want, s);
+    }
+    P.theta.resize(static_cast<size_t>(want));
     const auto t5 = Clock::now();
     // outputs
     if (outputsOnDevice) {
@@ -1137,6 +1149,8 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     cudaCheck(cudaStreamSynchronize(s), "outputs");
     const auto t6 = Clock::now();
     profCollect();
+    lastTheta_ = P.theta;
+    lastHasVectors_ = recover;
     if (pOut) *pOut = P.p;
     if (timing) {
         timing[AMLS_T_UPLOAD] = secs(t0, t1);
@@ -1342,6 +1356,58 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
     (void)ko;
 }
 
+void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+                           const double* Mbar, const double* weights, double gapTol, double* gE,
+                           double* gRho, double* dE, double* dRho, int32_t* simple) {
+    if (!lastHasVectors_ || lastTheta_.empty())
+        throw AmlsError(AMLS_ERR_INVALID_ARGUMENT,
+                        "sensitivities need a preceding solve with recovered eigenvectors");
+    if (nd <= 0 || nd > 96) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element DOF count must be 1..96");
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t s = stream_;
+    const int nm = static_cast<int>(lastTheta_.size());
+    // simple-eigenvalue test (relative gap to the neighbours above gapTol)
+    std::vector<double> w(static_cast<size_t>(nm));
+    for (int k = 0; k < nm; ++k) {
+        const double lk = lastTheta_[static_cast<size_t>(k)];
+        double gap = 1e300;
+        if (k > 0) gap = std::min(gap, std::fabs(lk - lastTheta_[static_cast<size_t>(k - 1)]));
+        if (k + 1 < nm) gap = std::min(gap, std::fabs(lastTheta_[static_cast<size_t>(k + 1)] - lk));
+        const bool ok = gap > gapTol * std::fabs(lk);
+        if (simple) simple[k] = ok ? 1 : 0;
+        w[static_cast<size_t>(k)] = ok ? (weights ? weights[k] : 0.0) : std::nan("");
+    }
+    int64_t* dDof = static_cast<int64_t*>(senDof_.ensure(sizeof(int64_t) * nelem * nd));
+    double* dEl = static_cast<double*>(senEl_.ensure(sizeof(double) * (2 * nd * nd + 2 * nm)));
+    const size_t outN = static_cast<size_t>(nelem) * (2 + (dE ? nm : 0) + (dRho ? nm : 0));
+    double* dOut = static_cast<double*>(senOut_.ensure(sizeof(double) * outN));
+    cudaCheck(cudaMemcpyAsync(dDof, dofmap, sizeof(int64_t) * nelem * nd, cudaMemcpyHostToDevice, s), "dofmap");
+    cudaCheck(cudaMemcpyAsync(dEl, Kbar, sizeof(double) * nd * nd, cudaMemcpyHostToDevice, s), "Kbar");
+    cudaCheck(cudaMemcpyAsync(dEl + nd * nd, Mbar, sizeof(double) * nd * nd, cudaMemcpyHostToDevice, s), "Mbar");
+    cudaCheck(cudaMemcpyAsync(dEl + 2 * nd * nd, lastTheta_.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "theta");
+    cudaCheck(cudaMemcpyAsync(dEl + 2 * nd * nd + nm, w.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "weights");
+    double* oE = dOut;
+    double* oR = dOut + nelem;
+    double* odE = dE ? dOut + 2 * nelem : nullptr;
+    double* odR = dRho ? dOut + 2 * nelem + (dE ? nelem * nm : 0) : nullptr;
+    LAUNCH(launchSensitivity(nelem, nd, dDof, dEl, dEl + nd * nd, zOut_.as<double>(), n_, nm,
+                             dEl + 2 * nd * nd, dEl + 2 * nd * nd + nm, oE, oR, odE, odR, s));
+    if (gE) cudaCheck(cudaMemcpyAsync(gE, oE, sizeof(double) * nelem, cudaMemcpyDeviceToHost, s), "gE");
+    if (gRho) cudaCheck(cudaMemcpyAsync(gRho, oR, sizeof(double) * nelem, cudaMemcpyDeviceToHost, s), "gRho");
+    if (dE) cudaCheck(cudaMemcpyAsync(dE, odE, sizeof(double) * nelem * nm, cudaMemcpyDeviceToHost, s), "dE");
+    if (dRho) cudaCheck(cudaMemcpyAsync(dRho, odR, sizeof(double) * nelem * nm, cudaMemcpyDeviceToHost, s), "dRho");
+    cudaCheck(cudaStreamSynchronize(s), "sensitivities");
+}
+
+void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
+    norms_.ensure(sizeof(double) * static_cast<size_t>(m));
+    zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
+    LAUNCH(launchMNorm(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n_, invDev_.as<int64_t>(), zt, ldz,
+                       m, norms_.as<double>(), s));
+    LAUNCH(launchUnpermute(zt, ldz, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
+    cudaCheck(cudaStreamSynchronize(s), "finalize");
+}
+
 void Engine::info(int64_t* out) const {
     int64_t ft = frontTotal_;
     out[0] = static_cast<int64_t>(nodes_.size());
@@ -1353,6 +1419,8 @@ void Engine::info(int64_t* out) const {
     cudaMemGetInfo(&freeB, &totB);
     out[5] = static_cast<int64_t>(totB - freeB);
     out[6] = launches_;
+    out[7] = refineIters_;
+    out[8] = refineNq_;
 }
 
 void Engine::categoryWork(double* flops, double* bytes) const {

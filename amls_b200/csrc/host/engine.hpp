@@ -51,6 +51,10 @@ public:
                       const int64_t* cap, const int64_t* wOff, double* w, const int64_t* vOff,
                       double* V, int64_t* m);
 
+    // per-element sensitivities of the last solve's eigenpairs
+    void sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+                       const double* Mbar, const double* weights, double gapTol, double* gE,
+                       double* gRho, double* dE, double* dRho, int32_t* simple);
     void info(int64_t* out) const;
     // per-category kernel timing with CUDA events on the engine stream
     static constexpr int kProfCats = 9;
@@ -91,7 +95,13 @@ private:
     void tridiagonalizeAll(cudaStream_t s);
     void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
     int reducedSolve(Pass& P, int want, cudaStream_t s);
+    // z^T (m x n, permuted order) into ztPool_
     void backtransform(const Pass& P, int m, cudaStream_t s);
+    // M-normalise the first m rows of zt (ld ldz) and un-permute into zOut_
+    void finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s);
+    void denseGenEigDev(double* K, double* M, int n, int want, double* w, double* V, int64_t ldv,
+                        cudaStream_t s);
+    int refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s);
     void checkStatus(const char* phase);
     // generic selected-eigenpair driver over prepared EigDesc tables
     void selectEigen(std::vector<EigDesc>& descs, int mode, int want, double thr, bool tridiag,
@@ -156,6 +166,14 @@ private:
     const int32_t* rowSDev_ = nullptr;             // panel rows of S_i (device, static)
     std::vector<int64_t> panelOff_;                // per node (doubles), -1 none
     std::vector<int64_t> yOff_;                    // per node (doubles into yPool_)
+
+    // refinement and the device dense eigensolver
+    DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_;
+    DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
+    int refineIters_ = 0, refineNq_ = 0;
+    std::vector<double> lastTheta_;                // eigenvalues of the last solve
+    bool lastHasVectors_ = false;
+    DevBuf senDof_, senEl_, senW_, senOut_;
 
     // kernel profiling
     bool profiling_ = false;

@@ -1,0 +1,357 @@
+// FP64 refinement of the AMLS eigenpairs and the device-resident dense
+// generalized eigensolver it uses.
+//
+// The elimination leaves the exact block factorisation K = L L^T (diagonal
+// blocks L_ii, off-diagonal rows L_Si of every front), so K^-1 can be applied
+// to a block of vectors with two tree sweeps: forward (levels bottom-up)
+// x_i = L_ii^-1 r_i, r_S -= L_Si x_i, and backward (levels top-down)
+// x_i = L_ii^-T (x_i - L_Si^T x_S).  The refinement is the subspace
+// iteration of AMLS-SIMb (papers/Improving_eigenpairs...md:288-420) on
+// nq = nev + extra vectors with T = K^-1 M, accelerated by a Chebyshev
+// filter: each outer iteration forms Y_c = C_c(2 T / a - I) Q, the unwanted
+// part of T's spectrum being [0, a] with a = 1 / (largest Ritz value), then
+//   X = T Y_c,  Kc = X^T (M Y_c),  Mc = X^T M X,  Kc c = theta Mc c,  Q <- X c
+// until the relative error of every wanted Ritz value, estimated from the
+// geometric contraction of successive changes, is below refineTol.
+// Vectors are kept transposed (nq x n, one contiguous column per DOF, in the
+// permuted order), the layout of the back-transform.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "host/engine.hpp"
+
+namespace amls_b200 {
+
+namespace {
+constexpr int kT = kGemmTile;
+int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+}  // namespace
+
+#define LAUNCH(call)                                   \
+    do {                                               \
+        const int cat_ = profBegin(#call);             \
+        cudaCheck((call), #call);                      \
+        profEnd(cat_);                                 \
+        ++launches_;                                   \
+    } while (0)
+
+// smallest `want` eigenpairs of (K, M), n x n column-major on the device;
+// K and M are overwritten.  w[want] ascending, V (n x want, ld ldv).
+void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, double* V,
+                            int64_t ldv, cudaStream_t s) {
+    const int64_t nn = n;
+    double* E = static_cast<double*>(dgE_.ensure(sizeof(double) * nn * nn));
+    double* Y = static_cast<double*>(dgY_.ensure(sizeof(double) * nn * want));
+    double* Yt = static_cast<double*>(dgYt_.ensure(sizeof(double) * nn * want));
+    double* d = static_cast<double*>(dgD_.ensure(sizeof(double) * 3 * nn));
+    double* work = static_cast<double*>(dgWork_.ensure(sizeof(double) * 6 * nn * want));
+    int* kOut = static_cast<int*>(dgK_.ensure(sizeof(int) * 4));
+    std::vector<TileRef> rowT, rowK, sq, yk, ky;
+    for (int r = 0; r < n; r += kTrsmRows) rowT.push_back({0, r, 0, 0});
+    for (int r = 0; r < want; r += kTrsmRows) rowK.push_back({0, r, 0, 0});
+    for (int j = 0; j < n; j += 32)
+        for (int i = 0; i < n; i += 32) sq.push_back({0, i, j, 0});
+    for (int j = 0; j < want; j += 32)
+        for (int i = 0; i < n; i += 32) yk.push_back({0, i, j, 0});
+    for (int j = 0; j < n; j += 32)
+        for (int i = 0; i < want; i += 32) ky.push_back({0, i, j, 0});
+    FrontDesc f{M, nn, n, n, -2, 0}, fe{E, nn, n, n, -2, 0};
+    TrsmDesc t1{M, nn, K, nn, n, n, 0, 0}, t2{M, nn, E, nn, n, n, 0, 0},
+        t3{M, nn, Yt, want, n, want, 0, 1};
+    CopyDesc c1{K, nn, E, nn, n, n}, c2{Y, nn, Yt, want, n, want}, c3{Yt, want, V, ldv, want, n};
+    EigDesc ed{};
+    ed.A = E;
+    ed.lda = nn;
+    ed.d = d;
+    ed.e = d + nn;
+    ed.tau = d + 2 * nn;
+    ed.n = n;
+    ed.id = -2;
+    ed.w = w;
+    ed.Y = Y;
+    ed.ldy = nn;
+    ed.kcap = want;
+    ed.kOut = kOut;
+    ed.work = work;
+    Blob b;
+    const size_t oF = b.add(&f, 1), oFe = b.add(&fe, 1), oT1 = b.add(&t1, 1), oT2 = b.add(&t2, 1),
+                 oT3 = b.add(&t3, 1), oC1 = b.add(&c1, 1), oC2 = b.add(&c2, 1), oC3 = b.add(&c3, 1),
+                 oE = b.add(&ed, 1), oRow = b.add(rowT), oK = b.add(rowK), oSq = b.add(sq),
+                 oYk = b.add(yk), oKy = b.add(ky);
+    std::vector<int> gOf, gFirst{0}, gSize;
+    std::vector<int64_t> pOff{0};
+    int nCta = 0;
+    if (n > 384) {
+        nCta = tridiagLargeMaxCtas(n);
+        gOf.assign(static_cast<size_t>(nCta), 0);
+        gSize.push_back(nCta);
+    }
+    const size_t oGo = b.add(gOf), oGf = b.add(gFirst), oGs = b.add(gSize), oPo = b.add(pOff);
+    b.upload(dgBlob_, s);
+    const FrontDesc* dF = b.dev<FrontDesc>(oF);
+    for (int jb = 0; jb * kCholBlock < n; ++jb) {
+        LAUNCH(launchCholDiag(dF, 1, jb, status_.as<int>(), s));
+        LAUNCH(launchCholPanel(dF, 1, jb, cdiv2(n, kTrsmRows), s));
+    }
+    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
+    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC1), b.dev<TileRef>(oSq), static_cast<int>(sq.size()), s));
+    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT2), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
+    LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
+    const EigDesc* dE = b.dev<EigDesc>(oE);
+    if (n <= 384) LAUNCH(launchTridiagSmall(dE, 1, s));
+    else {
+        dgP_.ensure(sizeof(double) * nn);
+        LAUNCH(launchTridiagLargeGroups(dE, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
+                                        dgP_.as<double>(), b.dev<int64_t>(oPo), n, s));
+    }
+    LAUNCH(launchBisect(dE, 1, 2, want, 0.0, want, nullptr, s));
+    LAUNCH(launchInverseIter(dE, 1, want, nullptr, s));
+    LAUNCH(launchBackTransform(dE, 1, want, s));
+    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC2), b.dev<TileRef>(oYk), static_cast<int>(yk.size()), s));
+    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT3), b.dev<TileRef>(oK), static_cast<int>(rowK.size()), s));
+    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC3), b.dev<TileRef>(oKy), static_cast<int>(ky.size()), s));
+    // the tables live in dgBlob_ until the stream passes this point
+    cudaCheck(cudaStreamSynchronize(s), "dense eigensolve");
+    const double nd = n;
+    catF_[4] += 4.0 / 3.0 * nd * nd * nd;
+    catB_[4] += 8.0 / 3.0 * nd * nd * nd;
+    catF_[0] += nd * nd * nd / 3.0;
+    catF_[1] += 2.0 * nd * nd * nd + nd * nd * want;
+}
+
+// Q (nq x n, transposed, permuted order) holds the AMLS Ritz vectors on entry
+// and the refined ones on exit; theta (host, nq) likewise.  Returns the
+// number of iterations.
+int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s) {
+    const int64_t n = n_;
+    const int64_t sz = n * nq;
+    double* R = static_cast<double*>(refR_.ensure(sizeof(double) * sz));
+    double* X = static_cast<double*>(refX_.ensure(sizeof(double) * sz));
+    double* MX = static_cast<double*>(refMX_.ensure(sizeof(double) * sz));
+    double* Kc = static_cast<double*>(refKc_.ensure(sizeof(double) * nq * nq));
+    double* Mc = static_cast<double*>(refMc_.ensure(sizeof(double) * nq * nq));
+    double* Vc = static_cast<double*>(refV_.ensure(sizeof(double) * nq * nq));
+    double* wd = static_cast<double*>(refW_.ensure(sizeof(double) * nq));
+    const double* F = kPool_.as<double>();
+
+    // ---- tables: K^-1 sweeps, Rayleigh-Ritz products, subspace update ----
+    Blob b;
+    std::vector<int32_t> ident(static_cast<size_t>(nq));
+    for (int j = 0; j < nq; ++j) ident[static_cast<size_t>(j)] = j;
+    std::vector<int64_t> colOffS;
+    std::vector<int64_t> colOffStart(nodes_.size(), 0);
+    for (int i : order_) {
+        colOffStart[static_cast<size_t>(i)] = static_cast<int64_t>(colOffS.size());
+        for (int32_t d : nodes_[static_cast<size_t>(i)].S) colOffS.push_back(static_cast<int64_t>(d) * nq);
+    }
+    Blob idx;
+    const size_t oId = idx.add(ident), oCo = idx.add(colOffS);
+    idx.upload(refIdx_, s);
+    const int32_t* dId = idx.dev<int32_t>(oId);
+    const int64_t* dCo = idx.dev<int64_t>(oCo);
+    struct Tabs {
+        size_t ftD, ftT, fgD, fgT, bgD, bgT, btD, btT;
+        int nft, nfg, nbg, nbt;
+    };
+    std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
+    double fsolve = 0;
+    for (int l = 0; l <= maxLevel_; ++l) {
+        std::vector<TrsmDesc> ft, bt;
+        std::vector<GemmDesc> fg, bg;
+        std::vector<TileRef> ftT, fgT, bgT, btT;
+        for (int i : byLevel_[static_cast<size_t>(l)]) {
+            const Node& nd = nodes_[static_cast<size_t>(i)];
+            const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
+            if (ni == 0) continue;
+            double* Xi = X + nd.off * nq;
+            TrsmDesc tf{F + nd.frontOff, nd.ld, Xi, nq, static_cast<int32_t>(ni), nq, 0, 0};
+            for (int r = 0; r < nq; r += kTrsmRows) ftT.push_back({static_cast<int32_t>(ft.size()), r, 0, 0});
+            ft.push_back(tf);
+            TrsmDesc tb = tf;
+            tb.backward = 1;
+            for (int r = 0; r < nq; r += kTrsmRows) btT.push_back({static_cast<int32_t>(bt.size()), r, 0, 0});
+            bt.push_back(tb);
+            fsolve += 2.0 * nq * ni * ni;
+            if (si > 0) {
+                GemmDesc g{};
+                g.M = nq;
+                g.N = static_cast<int32_t>(si);
+                g.K = static_cast<int32_t>(ni);
+                g.flags = kTransB | kScatter | kAtomic;
+                g.A = Xi;
+                g.lda = nq;
+                g.B = F + nd.frontOff + ni;
+                g.ldb = nd.ld;
+                g.C = X;
+                g.alpha = -1.0;
+                g.rowIdx = dId;
+                g.colOff = dCo + colOffStart[static_cast<size_t>(i)];
+                for (int jt = 0; jt < cdiv2(si, kT); ++jt)
+                    for (int it = 0; it < cdiv2(nq, kT); ++it)
+                        fgT.push_back({static_cast<int32_t>(fg.size()), it * kT, jt * kT, 0});
+                fg.push_back(g);
+                GemmDesc h{};
+                h.M = nq;
+                h.N = static_cast<int32_t>(ni);
+                h.K = static_cast<int32_t>(si);
+                h.flags = kGatherA | kAccumulate;
+                h.A = X;
+                h.lda = nq;
+                h.aMap = sIdxDev_ + nd.mapCol;
+                h.B = F + nd.frontOff + ni;
+                h.ldb = nd.ld;
+                h.C = Xi;
+                h.ldc = nq;
+                h.alpha = -1.0;
+                h.beta = 1.0;
+                for (int jt = 0; jt < cdiv2(ni, kT); ++jt)
+                    for (int it = 0; it < cdiv2(nq, kT); ++it)
+                        bgT.push_back({static_cast<int32_t>(bg.size()), it * kT, jt * kT, 0});
+                bg.push_back(h);
+                fsolve += 4.0 * nq * ni * si;
+            }
+        }
+        Tabs& T = tabs[static_cast<size_t>(l)];
+        T.ftD = b.add(ft); T.ftT = b.add(ftT); T.nft = static_cast<int>(ftT.size());
+        T.fgD = b.add(fg); T.fgT = b.add(fgT); T.nfg = static_cast<int>(fgT.size());
+        T.bgD = b.add(bg); T.bgT = b.add(bgT); T.nbg = static_cast<int>(bgT.size());
+        T.btD = b.add(bt); T.btT = b.add(btT); T.nbt = static_cast<int>(btT.size());
+    }
+    // Rayleigh-Ritz products: Kc = X R^T, Mc = X MX^T (split-K over n), Q = Vc^T X
+    const int chunk = 4096;
+    std::vector<GemmDesc> rr(2), up(1);
+    std::vector<TileRef> rrT, upT;
+    for (int q = 0; q < 2; ++q) {
+        GemmDesc& g = rr[static_cast<size_t>(q)];
+        g.M = g.N = nq;
+        g.K = static_cast<int32_t>(n);
+        g.flags = kTransB;
+        g.A = X;
+        g.lda = nq;
+        g.B = q == 0 ? R : MX;
+        g.ldb = nq;
+        g.C = q == 0 ? Kc : Mc;
+        g.ldc = nq;
+        g.alpha = 1.0;
+        g.kChunk = chunk;
+        for (int kc = 0; kc < cdiv2(n, chunk); ++kc)
+            for (int jt = 0; jt < cdiv2(nq, kT); ++jt)
+                for (int it = 0; it < cdiv2(nq, kT); ++it) rrT.push_back({q, it * kT, jt * kT, kc});
+    }
+    {
+        GemmDesc& g = up[0];
+        g.M = nq;
+        g.N = static_cast<int32_t>(n);
+        g.K = nq;
+        g.flags = kTransA;
+        g.A = Vc;
+        g.lda = nq;
+        g.B = X;
+        g.ldb = nq;
+        g.C = Q;
+        g.ldc = nq;
+        g.alpha = 1.0;
+        for (int jt = 0; jt < cdiv2(n, kT); ++jt)
+            for (int it = 0; it < cdiv2(nq, kT); ++it) upT.push_back({0, it * kT, jt * kT, 0});
+    }
+    FrontDesc sym[2] = {{Kc, nq, nq, nq, -3, 0}, {Mc, nq, nq, nq, -3, 0}};
+    const size_t oRR = b.add(rr), oRRT = b.add(rrT), oUP = b.add(up), oUPT = b.add(upT),
+                 oSym = b.add(sym, 2);
+    b.upload(refBlob_, s);
+
+    const double dn = static_cast<double>(n), dq = nq;
+    // the K^-1 M application on Y (nq x n): R = M Y, X = K^-1 R
+    auto applyT = [&](const double* Y) {
+        LAUNCH(launchSpmmT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n,
+                           permDev_.as<int64_t>(), invDev_.as<int64_t>(), Y, nq, R, s));
+        cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+        for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
+            const Tabs& T = tabs[static_cast<size_t>(l)];
+            LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
+        }
+        for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
+            const Tabs& T = tabs[static_cast<size_t>(l)];
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
+            LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
+        }
+        catF_[8] += 2.0 * nnzM_ * dq;
+        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
+        catF_[1] += fsolve / 2;
+        catF_[2] += fsolve / 2;
+    };
+    // Chebyshev recurrence buffers (degree = refine - 1)
+    const int cheb = std::max(0, opt_.refine - 1);
+    double* Y1 = cheb >= 1 ? static_cast<double*>(refY1_.ensure(sizeof(double) * sz)) : nullptr;
+    double* Y2 = cheb >= 2 ? static_cast<double*>(refY2_.ensure(sizeof(double) * sz)) : nullptr;
+    std::vector<double> prev(theta.begin(), theta.end());
+    std::vector<double> prevChange(static_cast<size_t>(nev), -1.0);
+    int it = 0;
+    for (; it < std::max(1, opt_.refineMaxIter); ++it) {
+        // filter: Y_c = C_c(2 T / a - I) Q on the damped interval [0, a] of
+        // T = K^-1 M, a = 1 / (largest Ritz value), then X = T Y_c
+        const double a = 1.0 / prev.back();
+        const double sc = 2.0 / a;
+        const double* Yc = Q;
+        if (cheb >= 1) {
+            double* Ym1 = Q;
+            double* Yk = Y1;
+            applyT(Q);
+            LAUNCH(launchAxpby3(sz, sc, X, -1.0, Q, 0.0, nullptr, Y1, s));     // Y1 = s T Q - Q
+            for (int k = 1; k < cheb; ++k) {
+                double* Yn = (k == 1) ? Y2 : (Ym1 == Q ? Y2 : Ym1);
+                applyT(Yk);
+                // Y_{k+1} = 2 (s T Y_k - Y_k) - Y_{k-1}
+                LAUNCH(launchAxpby3(sz, 2.0 * sc, X, -2.0, Yk, -1.0, Ym1, Yn, s));
+                Ym1 = Yk;
+                Yk = Yn;
+            }
+            Yc = Yk;
+        }
+        applyT(Yc);                                      // X = T Y_c, R = M Y_c = K X
+        LAUNCH(launchSpmmT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n,
+                           permDev_.as<int64_t>(), invDev_.as<int64_t>(), X, nq, MX, s));
+        cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
+        cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
+        LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
+        denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT), static_cast<int>(upT.size()), s));
+        std::vector<double> th(static_cast<size_t>(nq));
+        cudaCheck(cudaMemcpyAsync(th.data(), wd, sizeof(double) * nq, cudaMemcpyDeviceToHost, s), "theta");
+        cudaCheck(cudaStreamSynchronize(s), "refine");
+        catF_[8] += 2.0 * nnzM_ * dq;
+        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
+        catF_[2] += 3.0 * 2.0 * dn * dq * dq;
+        catB_[2] += 8.0 * (5.0 * dn * dq);
+        // error estimate per wanted value: change * r / (1 - r), r the observed
+        // contraction of the change (geometric convergence)
+        double est = 0.0;
+        for (int j = 0; j < nev; ++j) {
+            const double ch = std::fabs(th[static_cast<size_t>(j)] - prev[static_cast<size_t>(j)]) /
+                              std::fabs(th[static_cast<size_t>(j)]);
+            const double pc = prevChange[static_cast<size_t>(j)];
+            double e;
+            if (pc <= 0.0) e = (it == 0) ? 1.0 : ch;    // no ratio yet
+            else {
+                const double rr = std::min(0.95, ch / pc);
+                e = ch * std::max(rr, 0.05) / (1.0 - rr);
+            }
+            est = std::max(est, std::max(e, ch * 1e-3));
+            prevChange[static_cast<size_t>(j)] = ch;
+        }
+        prev = th;
+        if (opt_.verbosity > 1)
+            std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e\n", it + 1, est);
+        if (est <= opt_.refineTol) {
+            ++it;
+            break;
+        }
+    }
+    theta = prev;
+    checkStatus("refinement");
+    return it;
+}
+
+}  // namespace amls_b200

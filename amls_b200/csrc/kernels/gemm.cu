@@ -19,7 +19,7 @@ struct RegTile {
     double a[4], b[4];
 };
 
-__device__ __forceinline__ void loadA(const GemmDesc& D, int m0, int k0, double (&r)[4]) {
+__device__ __forceinline__ void loadA(const GemmDesc& D, int m0, int k0, int kEnd, double (&r)[4]) {
     const int tid = threadIdx.x;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -29,7 +29,7 @@ __device__ __forceinline__ void loadA(const GemmDesc& D, int m0, int k0, double 
         else { i = idx % TM; k = idx / TM; }
         const int gi = m0 + i, gk = k0 + k;
         double v = 0.0;
-        if (gi < D.M && gk < D.K) {
+        if (gi < D.M && gk < kEnd) {
             if (D.flags & kTransA) v = D.A[gk + (int64_t)gi * D.lda];
             else if (D.flags & kGatherA) v = D.A[gi + (int64_t)D.aMap[gk] * D.lda];
             else v = D.A[gi + (int64_t)gk * D.lda];
@@ -50,7 +50,7 @@ __device__ __forceinline__ void storeA(const GemmDesc& D, const double (&r)[4], 
     }
 }
 
-__device__ __forceinline__ void loadB(const GemmDesc& D, int n0, int k0, double (&r)[4]) {
+__device__ __forceinline__ void loadB(const GemmDesc& D, int n0, int k0, int kEnd, double (&r)[4]) {
     const int tid = threadIdx.x;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -60,7 +60,7 @@ __device__ __forceinline__ void loadB(const GemmDesc& D, int n0, int k0, double 
         else { k = idx % TK; j = idx / TK; }
         const int gj = n0 + j, gk = k0 + k;
         double v = 0.0;
-        if (gj < D.N && gk < D.K) {
+        if (gj < D.N && gk < kEnd) {
             if (D.flags & kTransB) v = D.B[gj + (int64_t)gk * D.ldb];
             else v = D.B[gk + (int64_t)gj * D.ldb];
         }
@@ -95,20 +95,23 @@ __global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restri
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
 
+    // split-K: this CTA covers k in [kBeg, kEnd) (the whole K when kChunk = 0)
+    const int kBeg = D.kChunk > 0 ? t.pad * D.kChunk : 0;
+    const int kEnd = D.kChunk > 0 ? min(D.K, kBeg + D.kChunk) : D.K;
     double ra[4], rb[4];
     int cur = 0;
-    if (D.K > 0) {
-        loadA(D, m0, 0, ra);
-        loadB(D, n0, 0, rb);
+    if (kEnd > kBeg) {
+        loadA(D, m0, kBeg, kEnd, ra);
+        loadB(D, n0, kBeg, kEnd, rb);
         storeA(D, ra, As[0]);
         storeB(D, rb, Bs[0]);
     }
     __syncthreads();
-    for (int k0 = 0; k0 < D.K; k0 += TK) {
-        const bool more = k0 + TK < D.K;
+    for (int k0 = kBeg; k0 < kEnd; k0 += TK) {
+        const bool more = k0 + TK < kEnd;
         if (more) {
-            loadA(D, m0, k0 + TK, ra);
-            loadB(D, n0, k0 + TK, rb);
+            loadA(D, m0, k0 + TK, kEnd, ra);
+            loadB(D, n0, k0 + TK, kEnd, rb);
         }
 #pragma unroll
         for (int kk = 0; kk < TK; ++kk) {
@@ -148,7 +151,8 @@ __global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restri
                 else *dst = v;
             } else {
                 double* dst = D.C + row + (int64_t)col * D.ldc;
-                if (D.flags & kAccumulate) *dst = v + D.beta * (*dst);
+                if (D.kChunk > 0) atomicAdd(dst, v);   // split-K partial (C pre-zeroed)
+                else if (D.flags & kAccumulate) *dst = v + D.beta * (*dst);
                 else *dst = v;
             }
         }

@@ -42,6 +42,8 @@ struct GemmDesc {
     const int32_t* aMap;
     const double* rowScale;
     const double* colScale;
+    int32_t kChunk;        // > 0: split-K, tile's TileRef.pad = chunk index, dense C
+    int32_t pad0;          // accumulated with atomics (caller zeroes C first)
 };
 
 struct TileRef {
@@ -168,13 +170,27 @@ cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* ou
                              const int64_t* dstOff, const int32_t* len, int nSeg,
                              cudaStream_t s);
 // M-norms of the columns of X under the original M (CSR rp/ci/v), with X
-// held transposed in permuted order: x[o, j] = zt[j + inv[o]*m].
+// held transposed in permuted order: x[o, j] = zt[j + inv[o]*ldz], j < m.
 cudaError_t launchMNorm(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* inv, const double* zt, int m, double* norms,
+                        const int64_t* inv, const double* zt, int64_t ldz, int m, double* norms,
                         cudaStream_t s);
-// Z[perm[d] + j*n] = zt[j + d*m] / sqrt(norms[j]).
-cudaError_t launchUnpermute(const double* zt, int m, int64_t n, const int64_t* perm,
+// Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]), j < m.
+cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
                             const double* norms, double* Z, cudaStream_t s);
+// Rt[:, d] = (P M P^T Q)[d, :]^T in the transposed layout (see misc.cu).
+cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
+                        const int64_t* perm, const int64_t* inv, const double* Qt, int m,
+                        double* Rt, cudaStream_t s);
+// Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
+// (n x nmodes, original order): see sensitivity.cu.  weight[k] NaN marks a
+// non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.
+cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+                              const double* Mbar, const double* X, int64_t n, int nmodes,
+                              const double* lambda, const double* weight, double* gE,
+                              double* gRho, double* dE, double* dRho, cudaStream_t s);
+// out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
+cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
+                         double c, const double* z, double* out, cudaStream_t s);
 // out[i] = 1 / in[i]   (reciprocals, for eigenvalue maps)
 cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s);
 

@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(256) mnormKernel(const int64_t* __restrict__ r
                                                    const int32_t* __restrict__ ci,
                                                    const double* __restrict__ v, int64_t n,
                                                    const int64_t* __restrict__ inv,
-                                                   const double* __restrict__ zt, int m, int j0,
-                                                   double* __restrict__ norms) {
+                                                   const double* __restrict__ zt, int64_t ldz,
+                                                   int m, int j0, double* __restrict__ norms) {
     constexpr int T = 16;
     __shared__ double part[8][T * 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -171,14 +171,14 @@ __global__ void __launch_bounds__(256) mnormKernel(const int64_t* __restrict__ r
         for (int t = 0; t < T; ++t) row[t] = 0.0;
         for (int64_t e = rp[d]; e < rp[d + 1]; ++e) {
             const double a = v[e];
-            const double* zc = zt + inv[ci[e]] * m;
+            const double* zc = zt + inv[ci[e]] * ldz;
 #pragma unroll
             for (int t = 0; t < T; ++t) {
                 const int j = j0 + lane + 32 * t;
                 if (j < m) row[t] = fma(a, zc[j], row[t]);
             }
         }
-        const double* zd = zt + inv[d] * m;
+        const double* zd = zt + inv[d] * ldz;
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             const int j = j0 + lane + 32 * t;
@@ -197,20 +197,20 @@ __global__ void __launch_bounds__(256) mnormKernel(const int64_t* __restrict__ r
 }
 
 cudaError_t launchMNorm(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* inv, const double* zt, int m, double* norms,
+                        const int64_t* inv, const double* zt, int64_t ldz, int m, double* norms,
                         cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * (size_t)m, s);
     if (e != cudaSuccess) return e;
     for (int j0 = 0; j0 < m; j0 += 512) {
-        mnormKernel<<<gridFor(n * 32, 256), 256, 0, s>>>(rp, ci, v, n, inv, zt, m, j0, norms);
+        mnormKernel<<<gridFor(n * 32, 256), 256, 0, s>>>(rp, ci, v, n, inv, zt, ldz, m, j0, norms);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
-// Z[perm[d] + j*n] = zt[j + d*m] / sqrt(norms[j]); 32 x 32 tiles (d, j).
-__global__ void unpermuteKernel(const double* __restrict__ zt, int m, int64_t n,
+// Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]); 32 x 32 tiles (d, j).
+__global__ void unpermuteKernel(const double* __restrict__ zt, int64_t ldz, int m, int64_t n,
                                 const int64_t* __restrict__ perm, const double* __restrict__ norms,
                                 double* __restrict__ Z) {
     __shared__ double t[32][33];
@@ -220,7 +220,7 @@ __global__ void unpermuteKernel(const double* __restrict__ zt, int m, int64_t n,
     for (int r = ty; r < 32; r += 8) {
         const int64_t d = d0 + r;
         const int j = j0 + tx;
-        t[r][tx] = (d < n && j < m) ? zt[j + d * m] : 0.0;
+        t[r][tx] = (d < n && j < m) ? zt[j + d * ldz] : 0.0;
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
@@ -233,11 +233,11 @@ __global__ void unpermuteKernel(const double* __restrict__ zt, int m, int64_t n,
     }
 }
 
-cudaError_t launchUnpermute(const double* zt, int m, int64_t n, const int64_t* perm,
+cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
                             const double* norms, double* Z, cudaStream_t s) {
     if (n <= 0 || m <= 0) return cudaSuccess;
     dim3 grid((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
-    unpermuteKernel<<<grid, 256, 0, s>>>(zt, m, n, perm, norms, Z);
+    unpermuteKernel<<<grid, 256, 0, s>>>(zt, ldz, m, n, perm, norms, Z);
     return cudaGetLastError();
 }
 
@@ -249,6 +249,80 @@ __global__ void reciprocalKernel(const double* __restrict__ in, double* __restri
 cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     reciprocalKernel<<<(n + 255) / 256, 256, 0, s>>>(in, out, n);
+    return cudaGetLastError();
+}
+
+// SpMM in the transposed layout: for every permuted row d (original row
+// o = perm[d]) Rt[:, d] = sum_e M[o, c_e] * Qt[:, inv[c_e]], with Qt and Rt
+// m x n column-major (ld = m): one CTA per row at a time, the row's
+// (value, column) pairs staged in shared memory, threads over the m
+// contiguous entries of each referenced column.
+__global__ void __launch_bounds__(128) spmmTKernel(const int64_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ ci,
+                                                   const double* __restrict__ v, int64_t n,
+                                                   const int64_t* __restrict__ perm,
+                                                   const int64_t* __restrict__ inv,
+                                                   const double* __restrict__ Qt, int m,
+                                                   double* __restrict__ Rt) {
+    constexpr int kStage = 512;
+    __shared__ double sv[kStage];
+    __shared__ int64_t sc[kStage];
+    for (int64_t d = blockIdx.x; d < n; d += gridDim.x) {
+        const int64_t o = perm[d];
+        const int64_t e0 = rp[o], e1 = rp[o + 1];
+        for (int j0 = 0; j0 < m; j0 += 4 * 128) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int64_t eb = e0; eb < e1; eb += kStage) {
+                const int cnt = (int)((e1 - eb) < kStage ? (e1 - eb) : kStage);
+                __syncthreads();
+                for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+                    sv[t] = v[eb + t];
+                    sc[t] = inv[ci[eb + t]] * (int64_t)m;
+                }
+                __syncthreads();
+                for (int t = 0; t < cnt; ++t) {
+                    const double a = sv[t];
+                    const double* q = Qt + sc[t];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int j = j0 + threadIdx.x + 128 * u;
+                        if (j < m) acc[u] = fma(a, q[j], acc[u]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + threadIdx.x + 128 * u;
+                if (j < m) Rt[j + d * (int64_t)m] = acc[u];
+            }
+        }
+    }
+}
+
+cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
+                        const int64_t* perm, const int64_t* inv, const double* Qt, int m,
+                        double* Rt, cudaStream_t s) {
+    if (n <= 0 || m <= 0) return cudaSuccess;
+    spmmTKernel<<<gridFor(n * 128, 128), 128, 0, s>>>(rp, ci, v, n, perm, inv, Qt, m, Rt);
+    return cudaGetLastError();
+}
+
+// out = a*x + b*y (+ c*z when z is given), elementwise
+__global__ void axpby3Kernel(int64_t n, double a, const double* __restrict__ x, double b,
+                             const double* __restrict__ y, double c, const double* __restrict__ z,
+                             double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double v = a * x[i] + b * y[i];
+        if (z) v += c * z[i];
+        out[i] = v;
+    }
+}
+
+cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
+                         double c, const double* z, double* out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    axpby3Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, a, x, b, y, c, z, out);
     return cudaGetLastError();
 }
 

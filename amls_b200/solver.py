@@ -31,6 +31,12 @@ class AmlsOptions:
     numThreads: int = 0
     recoverVectors: bool = True
     verbosity: int = 0
+    # FP64 refinement (not in the reference): subspace iteration with the
+    # elimination's exact K factorisation + Rayleigh-Ritz
+    refine: int = 0            # 0 off; k >= 1: K^-1 M applications per Rayleigh-Ritz step
+    refineMaxIter: int = 60
+    refineExtra: int = -1
+    refineTol: float = 1e-9
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -46,6 +52,10 @@ class AmlsOptions:
         o.numThreads = int(self.numThreads)
         o.recoverVectors = 1 if self.recoverVectors else 0
         o.verbosity = int(self.verbosity)
+        o.refine = (3 if self.refine is True else int(self.refine))
+        o.refineMaxIter = int(self.refineMaxIter)
+        o.refineExtra = int(self.refineExtra)
+        o.refineTol = float(self.refineTol)
         return o
 
 
@@ -120,6 +130,7 @@ class AmlsSolver:
                                          _lib.ptr(mp), _lib.ptr(mc), _lib.ptr(mv), C.byref(o),
                                          _lib.ptr(theta), _lib.ptr(Z), C.byref(p),
                                          _lib.ptr(timing)))
+        self._last_nev = nev
         return Solution(theta[:nev].copy(), None if Z is None else Z.T.copy(), int(p.value),
                         dict(zip(_lib.TIMING_KEYS, timing.tolist())), self.info())
 
@@ -147,6 +158,33 @@ class AmlsSolver:
         out["p"] = int(p.value)
         return out
 
+    def sensitivities(self, pencil, weights=None, per_mode: bool = False, gap_tol: float = 1e-6):
+        """Per-element eigenvalue sensitivities of the last solve's eigenpairs
+        for a hex pencil (K = sum E_e Kbar, M = sum rho_e Mbar).  Returns
+        dict(gE, gRho, simple[, dE, dRho]) with gE/gRho the gradient of
+        sum_k w_k lambda_k over simple modes (zeros without weights) and
+        dE/dRho of shape (nelem, nev) when per_mode."""
+        dm = np.ascontiguousarray(pencil.dofmap, dtype=np.int64)
+        nelem, nd = dm.shape
+        Kb = np.asfortranarray(pencil.Kbar, dtype=np.float64).ravel(order="F")
+        Mb = np.asfortranarray(pencil.Mbar, dtype=np.float64).ravel(order="F")
+        nev = self._last_nev
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        gE = np.zeros(nelem)
+        gR = np.zeros(nelem)
+        simple = np.zeros(nev, np.int32)
+        dE = np.zeros((nev, nelem)) if per_mode else None
+        dR = np.zeros((nev, nelem)) if per_mode else None
+        _lib.check(_lib.lib().amls_sensitivities(
+            self._h, nelem, nd, _lib.ptr(dm), _lib.ptr(Kb), _lib.ptr(Mb), _lib.ptr(w),
+            float(gap_tol), _lib.ptr(gE), _lib.ptr(gR), _lib.ptr(dE), _lib.ptr(dR),
+            _lib.ptr(simple)))
+        out = dict(gE=gE, gRho=gR, simple=simple.astype(bool))
+        if per_mode:
+            out["dE"] = dE.T.copy()
+            out["dRho"] = dR.T.copy()
+        return out
+
     def set_profiling(self, on: bool) -> None:
         _lib.check(_lib.lib().amls_set_profiling(self._h, 1 if on else 0))
 
@@ -167,7 +205,7 @@ class AmlsSolver:
         buf = np.zeros(_lib.INFO_SLOTS, np.int64)
         _lib.check(_lib.lib().amls_info(self._h, _lib.ptr(buf)))
         keys = ["tree_nodes", "levels", "p_passA", "p", "front_doubles", "device_bytes",
-                "launches"]
+                "launches", "refine_iters", "refine_nq"]
         return {k: int(v) for k, v in zip(keys, buf)}
 
     def work(self) -> dict:

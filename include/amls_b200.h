@@ -52,7 +52,19 @@ typedef struct amls_options {
     int32_t numThreads;         /* 0    host threads (partition/analysis)  */
     int32_t recoverVectors;     /* 1    */
     int32_t verbosity;          /* 1    */
-    int32_t reserved0;
+    /* FP64 refinement of the AMLS eigenpairs (no counterpart in the
+     * reference, which stops at the AMLS Ritz pairs): subspace iteration
+     * with T = K^-1 M applied through the exact block factorisation of K
+     * that the elimination produced (AMLS-SIMb,
+     * papers/Improving_eigenpairs...md:288-420), Chebyshev-filtered, with a
+     * Rayleigh-Ritz step per outer iteration.  refine = 0: off; refine = k:
+     * each outer iteration applies T k times (a degree k-1 Chebyshev filter
+     * on the unwanted interval [0, 1/theta_max] followed by one T step). */
+    int32_t refine;             /* 0    */
+    int32_t refineMaxIter;      /* 60   outer iterations */
+    int32_t refineExtra;        /* extra subspace vectors beyond nev; -1 = nev/2 + 16 */
+    double refineTol;           /* 1e-9: target relative eigenvalue error, estimated
+                                   from the geometric contraction of the Ritz values */
 } amls_options;
 
 /* slots of the timing array filled by amls_solve (seconds) */
@@ -61,7 +73,7 @@ typedef struct amls_options {
 #define AMLS_T_ELIMINATION 2   /* front assembly, factorisation, Schur/congruence */
 #define AMLS_T_CONDENSE 3      /* local eigensolves + projection (both passes)   */
 #define AMLS_T_REDUCED 4       /* reduced eigensolve(s)                          */
-#define AMLS_T_BACKTRANSFORM 5 /* back-transform, un-permute, M-normalise        */
+#define AMLS_T_BACKTRANSFORM 5 /* back-transform, refinement, un-permute, M-normalise */
 #define AMLS_T_TOTAL 6         /* host wall clock of the call                    */
 #define AMLS_T_DEVICE 7        /* CUDA-event time of the numeric solve on the handle's stream */
 #define AMLS_T_SLOTS 8
@@ -126,7 +138,8 @@ int amls_solve_values(amls_handle h, const double* k_val, const double* m_val,
 /* Diagnostics of the last analysis/solve on the handle:
  *   info[0] tree nodes, [1] levels, [2] p of pass A, [3] p of the final pass,
  *   [4] sum of front sizes (doubles), [5] device bytes in use,
- *   [6] kernel launches in the last numeric solve */
+ *   [6] kernel launches in the last numeric solve,
+ *   [7] refinement iterations, [8] refinement subspace size */
 #define AMLS_INFO_SLOTS 16
 int amls_info(amls_handle h, int64_t* info);
 
@@ -169,6 +182,26 @@ int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n, const int
                        const double* K, const double* M, int32_t mode, int64_t il, int64_t iu,
                        double lo, double hi, const int64_t* cap, const int64_t* w_off,
                        double* w, const int64_t* v_off, double* V, int64_t* m);
+
+/* Per-element eigenvalue sensitivities of the last amls_solve /
+ * amls_solve_values on the handle (no counterpart in the reference).  For a
+ * pencil assembled from one reference element pair with per-element scales,
+ * K = sum_e E_e Kbar, M = sum_e rho_e Mbar, and the solve's M-normalised
+ * eigenvectors x_k (kept on the device):
+ *   dlambda_k/dE_e = x_{k,e}^T Kbar x_{k,e},
+ *   dlambda_k/drho_e = -lambda_k x_{k,e}^T Mbar x_{k,e}
+ * (adjoint form, simple eigenvalues only).  Inputs (host):
+ *   dofmap[nelem * ndofe]   global DOF of each element DOF, -1 = constrained
+ *   Kbar, Mbar [ndofe^2]     column-major element matrices (ndofe <= 96)
+ *   weights[nev] or NULL     w_k of the weighted sum sum_k w_k lambda_k
+ *   gapTol                   modes with relative gap <= gapTol are not simple
+ * Outputs (host, NULL to skip): gE[nelem], gRho[nelem] the gradient of
+ * sum_k w_k lambda_k over the simple modes; dE, dRho [nelem * nev]
+ * (column-major, NaN for non-simple modes); simple[nev] 1/0. */
+int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, const int64_t* dofmap,
+                       const double* Kbar, const double* Mbar, const double* weights,
+                       double gapTol, double* gE, double* gRho, double* dE, double* dRho,
+                       int32_t* simple);
 
 /* Allocation-free dense generalized eigensolver (no counterpart in the
  * reference).  For callers that cannot allocate device memory: code inside a

@@ -156,3 +156,25 @@ def test_c5_matches_oracle_golden(solver):
     assert sol.p == int(g["p"])
     assert sol.info["p_passA"] == int(g["p_passA"])
     assert rel_err(sol.theta, g["theta"]) < 1e-10
+
+
+@pytest.mark.parametrize("case,refine", [("hex8_8", 1), ("hex8_8", 3), ("hex27_4", 3)])
+def test_refinement_reaches_exact_eigenvalues(solver, case, refine):
+    """FP64 refinement (subspace iteration with the elimination's exact K
+    factorisation + Rayleigh-Ritz) brings the AMLS Ritz values to the exact
+    eigenvalues: relative error <= 1e-8 against dense LAPACK dsygvd."""
+    if case == "hex8_8":
+        p = cases.hex_pencil(8, 8, 8, 1, seed=5)
+        o = dict(nev=40, nLevels=4, leafSize=200)
+    else:
+        p = cases.hex_pencil(4, 4, 4, 2, seed=6)
+        o = dict(nev=30, nLevels=4, leafSize=200)
+    wr, _ = R.LapackDense.solve_all(p.K.toarray(), p.M.toarray())
+    plain = solver.solve(p.K, p.M, AmlsOptions(**o))
+    sol = solver.solve(p.K, p.M, AmlsOptions(refine=refine, **o))
+    assert rel_err(plain.theta, wr[:o["nev"]]) > 1e-6          # AMLS alone is approximate
+    assert rel_err(sol.theta, wr[:o["nev"]]) < 1e-8
+    assert sol.info["refine_iters"] >= 1
+    assert residuals(p.K, p.M, sol.theta, sol.Z).max() < 1e-6
+    mn = np.einsum("ij,ij->j", sol.Z, p.M @ sol.Z)
+    assert np.allclose(mn, 1.0, atol=1e-12)
