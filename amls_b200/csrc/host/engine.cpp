@@ -30,6 +30,10 @@ void trsmTiles(std::vector<TileRef>& t, int desc, int64_t rows) {
     for (int i = 0; i < cdiv(rows, kTrsmRows); ++i) t.push_back({desc, i * kTrsmRows, 0, 0});
 }
 
+void trsmTiles64(std::vector<TileRef>& t, int desc, int64_t rows) {
+    for (int i = 0; i < cdiv(rows, kTrsmRows64); ++i) t.push_back({desc, i * kTrsmRows64, 0, 0});
+}
+
 void copyTiles(std::vector<TileRef>& t, int desc, int64_t r, int64_t c) {
     for (int j = 0; j < cdiv(c, 32); ++j)
         for (int i = 0; i < cdiv(r, 32); ++i) t.push_back({desc, i * 32, j * 32, 0});
@@ -264,7 +268,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
         for (int a : nd.anc) isAnc[static_cast<size_t>(a)] = 0;
     }
     // layout
-    frontTotal_ = eigTotal_ = vecTotal_ = 0;
+    frontTotal_ = eigTotal_ = vecTotal_ = invTotal_ = 0;
     for (int i : order_) {
         Node& nd = nodes_[static_cast<size_t>(i)];
         nd.ld = nd.n + static_cast<int64_t>(nd.S.size());
@@ -274,6 +278,8 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
         eigTotal_ += nd.n * nd.n;
         nd.vecOff = vecTotal_;
         vecTotal_ += nd.n;
+        nd.invOff = invTotal_;
+        invTotal_ += static_cast<int64_t>(cdiv(nd.n, 64)) * 4096;
     }
     // CSR destinations in the fronts
     auto dstMap = [&](const int64_t* rp, const int32_t* ci, std::vector<int64_t>& out) {
@@ -320,6 +326,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     dPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     ePool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     tauPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
+    invPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(invTotal_, 1)));
     buildStatic();
     cudaCheck(cudaStreamSynchronize(stream_), "analyze");
     analyzed_ = true;
@@ -388,8 +395,8 @@ void Engine::buildStatic() {
     for (int l = 0; l <= maxLevel_; ++l) {
         LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
         std::vector<FrontDesc> fk, fm, fsym;
-        std::vector<TrsmDesc> td, cd;
-        std::vector<TileRef> tt, ct, copyT, rt, ut;
+        std::vector<TrsmDesc> td, cd, idd;
+        std::vector<TileRef> tt, ct, copyT, rt, ut, it, symT;
         std::vector<CopyDesc> cp;
         std::vector<GemmDesc> rg;
         std::vector<FrontUpdDesc> ud;
@@ -411,9 +418,21 @@ void Engine::buildStatic() {
             fe.ld = nd.n;
             fe.n = fe.rows = static_cast<int32_t>(nd.n);
             fe.node = i;
+            for (int bj = 0; bj < cdiv(nd.n, 32); ++bj)
+                for (int bi = bj; bi < cdiv(nd.n, 32); ++bi)
+                    symT.push_back({static_cast<int32_t>(fsym.size()), bi, bj, 0});
             fsym.push_back(fe);
             maxN = std::max(maxN, nd.n);
             maxRows = std::max(maxRows, nd.ld);
+            double* invP = invPool_.as<double>() + nd.invOff;
+            // inverses of the 64x64 diagonal blocks of L_ii
+            TrsmDesc iv{};
+            iv.L = kP + nd.frontOff;
+            iv.ldl = nd.ld;
+            iv.n = static_cast<int32_t>(nd.n);
+            iv.inv = invP;
+            for (int J = 0; J < cdiv(nd.n, 64); ++J) it.push_back({static_cast<int32_t>(idd.size()), J, 0, 0});
+            idd.push_back(iv);
             // G <- G L^-T (all n + s rows)
             TrsmDesc t{};
             t.L = kP + nd.frontOff;
@@ -422,7 +441,8 @@ void Engine::buildStatic() {
             t.ldx = nd.ld;
             t.n = static_cast<int32_t>(nd.n);
             t.r = static_cast<int32_t>(nd.ld);
-            trsmTiles(tt, static_cast<int>(td.size()), nd.ld);
+            t.inv = invP;
+            trsmTiles64(tt, static_cast<int>(td.size()), nd.ld);
             td.push_back(t);
             // eig <- (G_ii L^-T)^T
             CopyDesc c{};
@@ -440,7 +460,8 @@ void Engine::buildStatic() {
             t2.X = eP + nd.eigOff;
             t2.ldx = nd.n;
             t2.n = t2.r = static_cast<int32_t>(nd.n);
-            trsmTiles(ct, static_cast<int>(cd.size()), nd.n);
+            t2.inv = invP;
+            trsmTiles64(ct, static_cast<int>(cd.size()), nd.n);
             cd.push_back(t2);
             if (s > 0) {
                 // R = Q - L_Si C / 2  (in place in the M front's lower block)
@@ -474,6 +495,11 @@ void Engine::buildStatic() {
         L.frontK = sblob_.add(fk);
         L.frontM = sblob_.add(fm);
         L.symDesc = sblob_.add(fsym);
+        L.symTiles = sblob_.add(symT);
+        L.nSymTiles = static_cast<int>(symT.size());
+        L.invDesc = sblob_.add(idd);
+        L.invTiles = sblob_.add(it);
+        L.nInvTiles = static_cast<int>(it.size());
         L.trsmDesc = sblob_.add(td);
         L.trsmTiles = sblob_.add(tt);
         L.nTrsmTiles = static_cast<int>(tt.size());
@@ -532,13 +558,16 @@ void Engine::eliminate(cudaStream_t s) {
             LAUNCH(launchCholDiag(fk, L.nFront, jb, st, s));
             LAUNCH(launchCholPanel(fk, L.nFront, jb, L.maxRowTiles, s));
         }
-        LAUNCH(launchTrsmRows(sblob_.dev<TrsmDesc>(L.trsmDesc), sblob_.dev<TileRef>(L.trsmTiles),
-                              L.nTrsmTiles, s));
+        LAUNCH(launchInvDiag(sblob_.dev<TrsmDesc>(L.invDesc), sblob_.dev<TileRef>(L.invTiles),
+                             L.nInvTiles, s));
+        LAUNCH(launchTrsmRows64(sblob_.dev<TrsmDesc>(L.trsmDesc), sblob_.dev<TileRef>(L.trsmTiles),
+                                L.nTrsmTiles, s));
         LAUNCH(launchTransposeBatched(sblob_.dev<CopyDesc>(L.tDesc), sblob_.dev<TileRef>(L.tTiles),
                                       L.nTTiles, s));
-        LAUNCH(launchTrsmRows(sblob_.dev<TrsmDesc>(L.cDesc), sblob_.dev<TileRef>(L.cTiles),
-                              L.nCTiles, s));
-        LAUNCH(launchSymmetrize(sblob_.dev<FrontDesc>(L.symDesc), L.nFront, s));
+        LAUNCH(launchTrsmRows64(sblob_.dev<TrsmDesc>(L.cDesc), sblob_.dev<TileRef>(L.cTiles),
+                                L.nCTiles, s));
+        LAUNCH(launchSymmetrizeTiles(sblob_.dev<FrontDesc>(L.symDesc), sblob_.dev<TileRef>(L.symTiles),
+                                     L.nSymTiles, s));
         LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.rDesc), sblob_.dev<TileRef>(L.rTiles),
                                  L.nRTiles, s));
         LAUNCH(launchFrontUpdate(sblob_.dev<FrontUpdDesc>(L.uDesc), sblob_.dev<TileRef>(L.uTiles),
@@ -810,7 +839,8 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                 t.ldx = Ki;
                 t.n = static_cast<int32_t>(ni);
                 t.r = static_cast<int32_t>(Ki);
-                trsmTiles(trT, static_cast<int>(tr.size()), Ki);
+                t.inv = invPool_.as<double>() + nd.invOff;
+                trsmTiles64(trT, static_cast<int>(tr.size()), Ki);
                 tr.push_back(t);
                 fc += static_cast<double>(Ki) * ni * ni;
                 if (ki > 0) {
@@ -866,9 +896,11 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
 
     // ---- local eigenpairs (largest nu of C_i) ----
     const EigDesc* dd = b.dev<EigDesc>(oDescs);
-    LAUNCH(launchBisect(dd, N, mode == 0 ? 0 : 1, want, thr, maxK, nullptr, s));
+    int maxNodeN = 1;
+    for (const Node& nd : nodes_) maxNodeN = std::max<int>(maxNodeN, static_cast<int>(nd.n));
+    LAUNCH(launchBisectWarp(dd, N, mode == 0 ? 0 : 1, want, thr, maxK, s));
     LAUNCH(launchInverseIter(dd, N, maxK, nullptr, s));
-    LAUNCH(launchBackTransform(dd, N, maxK, s));
+    LAUNCH(launchBackTransformSmem(dd, N, maxK, maxNodeN, s));
 
     // ---- projection ----
     LAUNCH(launchZero(panel, panelTot, s));
@@ -877,7 +909,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelTabs& T = tabs[static_cast<size_t>(l)];
         LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(T.cpD), b.dev<TileRef>(T.cpT), T.ncpT, s));
-        LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.trD), b.dev<TileRef>(T.trT), T.ntrT, s));
+        LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.trD), b.dev<TileRef>(T.trT), T.ntrT, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.ng1T, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.ng2T, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.midD), b.dev<TileRef>(T.midT), T.nmidT, s));
@@ -903,7 +935,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
 }
 
 // largest `want` eigenpairs of the reduced matrix; fills P.theta ascending
-int Engine::reducedSolve(Pass& P, int want, cudaStream_t s) {
+int Engine::reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors) {
     const int64_t p = P.p;
     want = static_cast<int>(std::min<int64_t>(want, p));
     redD_.ensure(sizeof(double) * static_cast<size_t>(p));
@@ -946,9 +978,11 @@ int Engine::reducedSolve(Pass& P, int want, cudaStream_t s) {
         LAUNCH(launchTridiagLargeGroups(dd, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         redP_.as<double>(), b.dev<int64_t>(oPo), static_cast<int>(p), s));
     }
-    LAUNCH(launchBisect(dd, 1, 0, want, 0.0, want, nullptr, s));
-    LAUNCH(launchInverseIter(dd, 1, want, nullptr, s));
-    LAUNCH(launchBackTransform(dd, 1, want, s));
+    LAUNCH(launchBisectWarp(dd, 1, 0, want, 0.0, want, s));
+    if (vectors) {
+        LAUNCH(launchInverseIter(dd, 1, want, nullptr, s));
+        LAUNCH(launchBackTransformSmem(dd, 1, want, static_cast<int>(p), s));
+    }
     std::vector<double> nu(static_cast<size_t>(want));
     cudaCheck(cudaMemcpyAsync(nu.data(), redW_.as<double>(), sizeof(double) * want, cudaMemcpyDeviceToHost, s), "theta");
     cudaCheck(cudaStreamSynchronize(s), "reduced");
@@ -1011,7 +1045,8 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
             t.n = static_cast<int32_t>(ni);
             t.r = m;
             t.backward = 1;
-            trsmTiles(tT, static_cast<int>(tr.size()), m);
+            t.inv = invPool_.as<double>() + nd.invOff;
+            trsmTiles64(tT, static_cast<int>(tr.size()), m);
             tr.push_back(t);
             fb += 2.0 * m * ni * (ki + si) + static_cast<double>(m) * ni * ni;
         }
@@ -1026,7 +1061,7 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
         const Tabs& T = tabs[static_cast<size_t>(l)];
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.n1, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
-        LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
+        LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
     }
     catF_[2] += fb;
     catB_[2] += 8.0 * 3.0 * m * static_cast<double>(n_);
@@ -1093,7 +1128,7 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
         condense(0, static_cast<int>(k0), 0.0, A, s);
         pA_ = A.p;
         const auto ta = Clock::now();
-        const int got = reducedSolve(A, static_cast<int>(std::min<int64_t>(nev, A.p)), s);
+        const int got = reducedSolve(A, static_cast<int>(std::min<int64_t>(nev, A.p)), s, false);
         tRed += secs(ta, Clock::now());
         if (got < nev)
             throw AmlsError(AMLS_ERR_NUMERIC, "pass A reduced problem too small (p < nev); reduce nLevels or grow leafSize");

@@ -77,6 +77,7 @@ private:
         int64_t eigOff = 0;          // doubles into the eig matrix pool (n*n)
         int64_t vecOff = 0;          // doubles into d/e/tau pools (n)
         int64_t pathPrefix = 0;      // sum of ancestor sizes (panel rows)
+        int64_t invOff = 0;          // doubles into invPool_ (64x64 diagonal-block inverses)
         // extend-add maps (offsets into the static int arrays)
         int64_t mapCol = 0;          // pmin/colOff/rowBase start (|S| entries)
         int64_t rowS = 0;            // panel row index of each S entry (|S| entries)
@@ -94,7 +95,7 @@ private:
     void eliminate(cudaStream_t s);
     void tridiagonalizeAll(cudaStream_t s);
     void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
-    int reducedSolve(Pass& P, int want, cudaStream_t s);
+    int reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors = true);
     // z^T (m x n, permuted order) into ztPool_
     void backtransform(const Pass& P, int m, cudaStream_t s);
     // M-normalise the first m rows of zt (ld ldz) and un-permute into zOut_
@@ -125,10 +126,10 @@ private:
     std::vector<std::vector<int>> byLevel_;
     int maxLevel_ = 0;
     std::vector<int32_t> owner_;                   // permuted index -> node
-    int64_t frontTotal_ = 0, eigTotal_ = 0, vecTotal_ = 0;
+    int64_t frontTotal_ = 0, eigTotal_ = 0, vecTotal_ = 0, invTotal_ = 0;
 
     // static device data
-    DevBuf kPool_, mPool_, eigPool_, dPool_, ePool_, tauPool_;
+    DevBuf kPool_, mPool_, eigPool_, dPool_, ePool_, tauPool_, invPool_;
     DevBuf kVal_, mVal_, kDst_, mDst_;             // CSR values and their front destinations
     DevBuf mRp_, mCi_, invDev_, permDev_;          // original M CSR pattern, maps
     DevBuf staticInts_;                            // extend-add and panel maps
@@ -139,13 +140,16 @@ private:
     struct LevelPlan {
         size_t frontK = 0, frontM = 0;             // FrontDesc tables
         int nFront = 0, maxBlocks = 0, maxRowTiles = 0;
+        size_t invDesc = 0, invTiles = 0;           // 64x64 diagonal-block inverses
+        int nInvTiles = 0;
         size_t trsmDesc = 0, trsmTiles = 0;
         int nTrsmTiles = 0;
         size_t tDesc = 0, tTiles = 0;              // transpose G_ii -> eig matrix
         int nTTiles = 0;
         size_t cDesc = 0, cTiles = 0;              // TRSM on eig matrix
         int nCTiles = 0;
-        size_t symDesc = 0;                        // symmetrize eig matrices
+        size_t symDesc = 0, symTiles = 0;          // symmetrize eig matrices
+        int nSymTiles = 0;
         size_t rDesc = 0, rTiles = 0;              // R = Q - L C / 2
         int nRTiles = 0;
         size_t uDesc = 0, uTiles = 0;              // extend-add

@@ -105,9 +105,9 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
         LAUNCH(launchTridiagLargeGroups(dE, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         dgP_.as<double>(), b.dev<int64_t>(oPo), n, s));
     }
-    LAUNCH(launchBisect(dE, 1, 2, want, 0.0, want, nullptr, s));
+    LAUNCH(launchBisectWarp(dE, 1, 2, want, 0.0, want, s));
     LAUNCH(launchInverseIter(dE, 1, want, nullptr, s));
-    LAUNCH(launchBackTransform(dE, 1, want, s));
+    LAUNCH(launchBackTransformSmem(dE, 1, want, n, s));
     LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC2), b.dev<TileRef>(oYk), static_cast<int>(yk.size()), s));
     LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT3), b.dev<TileRef>(oK), static_cast<int>(rowK.size()), s));
     LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC3), b.dev<TileRef>(oKy), static_cast<int>(ky.size()), s));
@@ -165,12 +165,13 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
             if (ni == 0) continue;
             double* Xi = X + nd.off * nq;
-            TrsmDesc tf{F + nd.frontOff, nd.ld, Xi, nq, static_cast<int32_t>(ni), nq, 0, 0};
-            for (int r = 0; r < nq; r += kTrsmRows) ftT.push_back({static_cast<int32_t>(ft.size()), r, 0, 0});
+            TrsmDesc tf{F + nd.frontOff, nd.ld, Xi, nq, static_cast<int32_t>(ni), nq, 0, 0,
+                        invPool_.as<double>() + nd.invOff};
+            for (int r = 0; r < nq; r += kTrsmRows64) ftT.push_back({static_cast<int32_t>(ft.size()), r, 0, 0});
             ft.push_back(tf);
             TrsmDesc tb = tf;
             tb.backward = 1;
-            for (int r = 0; r < nq; r += kTrsmRows) btT.push_back({static_cast<int32_t>(bt.size()), r, 0, 0});
+            for (int r = 0; r < nq; r += kTrsmRows64) btT.push_back({static_cast<int32_t>(bt.size()), r, 0, 0});
             bt.push_back(tb);
             fsolve += 2.0 * nq * ni * ni;
             if (si > 0) {
@@ -268,13 +269,13 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
+            LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
             LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
         }
         for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
             LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
-            LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
+            LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
         }
         catF_[8] += 2.0 * nnzM_ * dq;
         catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;

@@ -100,9 +100,16 @@ struct TrsmDesc {
     int64_t ldx;
     int32_t n, r;
     int32_t rowTiles, backward;
+    double* inv;            // trsmRows64 / invDiag: inverses of the 64x64 diagonal blocks
 };
 constexpr int kTrsmRows = 32;
 cudaError_t launchTrsmRows(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
+// Same operation with 64-row tiles (TileRef.m0 = first row), register-tiled,
+// diagonal blocks applied through inv (see launchInvDiag).
+constexpr int kTrsmRows64 = 64;
+cudaError_t launchTrsmRows64(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
+// inv + 4096*J = (L_JJ)^-1 for the 64x64 diagonal blocks J (TileRef.m0 = J).
+cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
 
 // ------------------------------------------------------- eigensolver ----
 // Symmetric tridiagonalisation (Householder), in place.  A (n x n, full
@@ -143,6 +150,11 @@ cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int* status
                               cudaStream_t s);
 // Y <- Q Y with Q = H_0 ... H_{n-3} (back-transform of tridiagonal vectors).
 cudaError_t launchBackTransform(const EigDesc* d, int nDesc, int maxK, cudaStream_t s);
+// Same with columns and reflectors staged in shared memory (maxN = largest n).
+cudaError_t launchBackTransformSmem(const EigDesc* d, int nDesc, int maxK, int maxN, cudaStream_t s);
+// Bisection with one warp per eigenvalue (32-point multisection per round).
+cudaError_t launchBisectWarp(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
+                             cudaStream_t s);
 
 // --------------------------------------------------------------- misc ---
 // Zero a list of (pointer, count) ranges.
@@ -155,6 +167,9 @@ cudaError_t launchScatterAdd(const double* vals, const int64_t* dst, int64_t nnz
 cudaError_t launchSetDiagonal(double* C, const double* w, int64_t p, cudaStream_t s);
 // Symmetrise a batch of square blocks: A = (A + A^T)/2.
 cudaError_t launchSymmetrize(const FrontDesc* d, int nDesc, cudaStream_t s);
+// Symmetrise 32x32 tile pairs listed in tiles (desc, bi, bj with bi >= bj).
+cudaError_t launchSymmetrizeTiles(const FrontDesc* d, const TileRef* tiles, int nTiles,
+                                  cudaStream_t s);
 // Transpose-copy: out(c x r) = in(r x c)^T  for a batch.
 struct CopyDesc {
     const double* in;

@@ -526,4 +526,108 @@ cudaError_t launchBackTransform(const EigDesc* d, int nDesc, int maxK, cudaStrea
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------
+// bisection with one warp per eigenvalue: each round evaluates 32 Sturm
+// counts at equally spaced points of the current bracket (multisection),
+// narrowing it 32-fold per round instead of 2-fold.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) bisectWarpKernel(const EigDesc* __restrict__ descs, int mode) {
+    const int b = blockIdx.y;
+    const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const EigDesc D = descs[b];
+    const int k = *D.kOut;
+    if (j >= k) return;
+    const int n = D.n;
+    const int t = (mode <= 1) ? (n - j) : (j + 1);
+    double lo, hi, pivmin, tn;
+    gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
+    for (int it = 0; it < 40; ++it) {
+        if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+        const double x = lo + (hi - lo) * (lane + 1) / 33.0;
+        const bool ge = sturmLess(D.d, D.e, n, x, pivmin) >= t;   // lambda_t < x
+        const unsigned m = __ballot_sync(0xffffffffu, ge);
+        // first lane whose point is above lambda_t
+        const int f = m ? __ffs(m) - 1 : 32;
+        const double nlo = (f == 0) ? lo : lo + (hi - lo) * f / 33.0;
+        const double nhi = (f == 32) ? hi : lo + (hi - lo) * (f + 1) / 33.0;
+        if (!(nhi < hi || nlo > lo)) break;   // no progress at this resolution
+        lo = nlo;
+        hi = nhi;
+    }
+    if (lane == 0) D.w[j] = 0.5 * (lo + hi);
+}
+
+cudaError_t launchBisectWarp(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
+                             cudaStream_t s) {
+    if (nDesc <= 0) return cudaSuccess;
+    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || maxK <= 0) return e;
+    dim3 grid((maxK + 7) / 8, nDesc);
+    bisectWarpKernel<<<grid, 256, 0, s>>>(d, mode);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// eigenvector back-transform with the columns and the reflector in shared
+// memory: a CTA owns `cols` columns (one warp each); per reflector the CTA
+// stages v_k once, each warp forms its dot product and update in shared
+// memory.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) backTransformSmemKernel(const EigDesc* __restrict__ descs,
+                                                                int cols, int maxN) {
+    extern __shared__ double sb[];
+    const int b = blockIdx.y;
+    const EigDesc D = descs[b];
+    const int k = *D.kOut;
+    const int c0 = blockIdx.x * cols;
+    if (c0 >= k) return;
+    const int n = D.n;
+    const int nc = min(cols, k - c0);
+    double* sv = sb;                  // maxN
+    double* sy = sb + maxN;           // cols x maxN
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int e = threadIdx.x; e < nc * n; e += blockDim.x) {
+        const int c = e / n, i = e % n;
+        sy[c * maxN + i] = D.Y[i + (int64_t)(c0 + c) * D.ldy];
+    }
+    for (int kk = n - 3; kk >= 0; --kk) {
+        const double tau = D.tau[kk];
+        if (tau == 0.0) continue;
+        const int m = n - kk - 1;
+        const double* v = D.A + (kk + 1) + (int64_t)kk * D.lda;
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) sv[i] = v[i];
+        __syncthreads();
+        for (int c = wid; c < nc; c += nw) {
+            double* y = sy + c * maxN + kk + 1;
+            double s = 0.0;
+            for (int i = lane; i < m; i += 32) s += sv[i] * y[i];
+            s = warpSum<32>(s) * tau;
+            for (int i = lane; i < m; i += 32) y[i] -= s * sv[i];
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nc * n; e += blockDim.x) {
+        const int c = e / n, i = e % n;
+        D.Y[i + (int64_t)(c0 + c) * D.ldy] = sy[c * maxN + i];
+    }
+}
+
+cudaError_t launchBackTransformSmem(const EigDesc* d, int nDesc, int maxK, int maxN, cudaStream_t s) {
+    if (nDesc <= 0 || maxK <= 0 || maxN <= 0) return cudaSuccess;
+    const int budget = 200 * 1024 / 8;                  // doubles of shared memory
+    int cols = budget / maxN - 1;
+    if (cols > 8) cols = 8;
+    if (cols < 1) return launchBackTransform(d, nDesc, maxK, s);
+    const size_t smem = sizeof(double) * (size_t)maxN * (cols + 1);
+    cudaError_t e = cudaFuncSetAttribute(backTransformSmemKernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((maxK + cols - 1) / cols, nDesc);
+    backTransformSmemKernel<<<grid, 256, smem, s>>>(d, cols, maxN);
+    return cudaGetLastError();
+}
+
 }  // namespace amls_b200

@@ -178,3 +178,15 @@ def test_refinement_reaches_exact_eigenvalues(solver, case, refine):
     assert residuals(p.K, p.M, sol.theta, sol.Z).max() < 1e-6
     mn = np.einsum("ij,ij->j", sol.Z, p.M @ sol.Z)
     assert np.allclose(mn, 1.0, atol=1e-12)
+
+
+def test_c5_refined_matches_exact(solver):
+    """Full-size workload with FP64 refinement: all 500 eigenvalues within
+    1e-8 relative of the exact ones (shift-invert Lanczos golden,
+    tests/golden/make_c5_golden.py)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c5_exact.npz"))["theta"]
+    p = cases.config_pencil("C5", seed=0)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=500, nLevels=8, leafSize=500, refine=3,
+                                             recoverVectors=False))
+    assert rel_err(sol.theta, g[:500]) < 1e-8
