@@ -7,6 +7,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <exception>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <numeric>
 #include <stdexcept>
@@ -281,10 +285,30 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
         nd.invOff = invTotal_;
         invTotal_ += static_cast<int64_t>(cdiv(nd.n, 64)) * 4096;
     }
-    // CSR destinations in the fronts
+    // CSR destinations in the fronts (rows split over host threads)
+    std::function<void(const int64_t*, const int32_t*, std::vector<int64_t>&, int64_t, int64_t)> rowsDst;
     auto dstMap = [&](const int64_t* rp, const int32_t* ci, std::vector<int64_t>& out) {
         out.assign(static_cast<size_t>(rp[n]), -1);
-        for (int64_t old = 0; old < n; ++old) {
+        unsigned nt = std::thread::hardware_concurrency();
+        nt = std::max(1u, std::min(nt, 64u));
+        std::vector<std::thread> th;
+        std::exception_ptr err;
+        std::mutex errMu;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                try {
+                    rowsDst(rp, ci, out, n * t / nt, n * (t + 1) / nt);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lk(errMu);
+                    err = std::current_exception();
+                }
+            });
+        for (auto& x : th) x.join();
+        if (err) std::rethrow_exception(err);
+    };
+    auto rowsDstBody = [&](const int64_t* rp, const int32_t* ci, std::vector<int64_t>& out,
+                           int64_t rowBeg, int64_t rowEnd) {
+        for (int64_t old = rowBeg; old < rowEnd; ++old) {
             const int64_t r = inv_[static_cast<size_t>(old)];
             for (int64_t e = rp[old]; e < rp[old + 1]; ++e) {
                 const int64_t c = inv_[static_cast<size_t>(ci[e])];
@@ -302,6 +326,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
             }
         }
     };
+    rowsDst = rowsDstBody;
     dstMap(kp, kc, hostKDst_);
     dstMap(mp, mc, hostMDst_);
 
@@ -646,7 +671,7 @@ void Engine::tridiagonalizeAll(cudaStream_t s) {
     }
     if (!small.empty()) LAUNCH(launchTridiagSmall(b.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
     if (!large.empty()) {
-        redP_.ensure(sizeof(double) * static_cast<size_t>(pTot));
+        redP_.ensure(sizeof(double) * static_cast<size_t>(2 * pTot));
         LAUNCH(launchTridiagLargeGroups(b.dev<EigDesc>(oL), b.dev<int>(oGo), b.dev<int>(oGf),
                                         b.dev<int>(oGs), static_cast<int>(groupOf.size()),
                                         redP_.as<double>(), b.dev<int64_t>(oPo), maxLargeN, s));
@@ -974,7 +999,7 @@ int Engine::reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors) {
     const EigDesc* dd = b.dev<EigDesc>(o);
     if (p <= kSmallEig) LAUNCH(launchTridiagSmall(dd, 1, s));
     else {
-        redP_.ensure(sizeof(double) * static_cast<size_t>(p));
+        redP_.ensure(sizeof(double) * static_cast<size_t>(2 * p));
         LAUNCH(launchTridiagLargeGroups(dd, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         redP_.as<double>(), b.dev<int64_t>(oPo), static_cast<int>(p), s));
     }
@@ -1356,7 +1381,7 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
     LAUNCH(launchSymmetrize(B.dev<FrontDesc>(ofE), nb, s));
     if (!small.empty()) LAUNCH(launchTridiagSmall(B.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
     if (!large.empty()) {
-        pbuf.ensure(sizeof(double) * (pTot + 1));
+        pbuf.ensure(sizeof(double) * (2 * pTot + 1));
         LAUNCH(launchTridiagLargeGroups(B.dev<EigDesc>(oL), B.dev<int>(oGo), B.dev<int>(oGf), B.dev<int>(oGs),
                                         static_cast<int>(gOf.size()), pbuf.as<double>(), B.dev<int64_t>(oPo),
                                         maxLargeN, s));
@@ -1433,6 +1458,19 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const d
     if (dRho) cudaCheck(cudaMemcpyAsync(dRho, odR, sizeof(double) * nelem * nm, cudaMemcpyDeviceToHost, s), "dRho");
     cudaCheck(cudaStreamSynchronize(s), "sensitivities");
 }
+
+// device arrays of the nodes' eig-pool offsets and sizes (post-order)
+const int64_t* Engine::eigOffsDev() {
+    std::vector<int64_t> v;
+    for (int i : order_) v.push_back(nodes_[static_cast<size_t>(i)].eigOff);
+    for (int i : order_) v.push_back(nodes_[static_cast<size_t>(i)].n);
+    int64_t* d = static_cast<int64_t*>(nodeOffDev_.ensure(sizeof(int64_t) * v.size()));
+    cudaCheck(cudaMemcpyAsync(d, v.data(), sizeof(int64_t) * v.size(), cudaMemcpyHostToDevice, stream_), "offsets");
+    cudaCheck(cudaStreamSynchronize(stream_), "offsets");
+    return d;
+}
+
+const int64_t* Engine::nodeSizesDev() { return nodeOffDev_.as<int64_t>() + order_.size(); }
 
 void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
     norms_.ensure(sizeof(double) * static_cast<size_t>(m));

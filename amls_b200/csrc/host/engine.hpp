@@ -172,8 +172,11 @@ private:
     std::vector<int64_t> yOff_;                    // per node (doubles into yPool_)
 
     // refinement and the device dense eigensolver
-    DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_;
+    DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
+    DevBuf refT_, refU_, refUBlob_, nodeOffDev_;
+    const int64_t* eigOffsDev();
+    const int64_t* nodeSizesDev();
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;

@@ -4,18 +4,21 @@
 // (libmetis_static.a, METIS 5 API, 64-bit idx_t established at run time by
 // METIS_SetDefaultOptions filling 40 x 8 bytes).  The graph construction and
 // the recursion restate src/partition/metis_partitioner.cpp:
-//   * extractGraph (:20-45): adjacency of |K|+|M| without self loops, built by
-//     inserting into one std::unordered_set per vertex while walking columns
-//     in ascending order, and emitted in the set's iteration order - the same
-//     container and insertion sequence, hence the same order with libstdc++;
+//   * extractGraph (:20-45): adjacency of |K|+|M| without self loops, emitted
+//     in the iteration order of one std::unordered_set per vertex filled in
+//     the reference's insertion order (see extractGraph below);
 //   * inducedSubgraph (:48-73): neighbour lists sorted;
-//   * bisect (:80-106): PartGraphRecursive (result unused) then
-//     ComputeVertexSeparator, both with options seed 42;
+//   * bisect (:80-106): ComputeVertexSeparator with options seed 42.  The
+//     reference first calls PartGraphRecursive and never reads its result;
+//     METIS re-seeds its generator from the options at the start of every
+//     API call, so dropping that call leaves the separator unchanged (checked
+//     on the benchmark pencils: identical permutations) and saves its time;
 //   * recursion (:110-160) and perm = post-order concatenation (:168-175).
 #include "tree.hpp"
 
 #include <algorithm>
 #include <functional>
+#include <thread>
 #include <numeric>
 #include <stdexcept>
 #include <unordered_set>
@@ -23,10 +26,6 @@
 extern "C" {
 // METIS 5 public prototypes (idx_t = int64_t in the linked library).
 int METIS_SetDefaultOptions(int64_t* options);
-int METIS_PartGraphRecursive(int64_t* nvtxs, int64_t* ncon, int64_t* xadj, int64_t* adjncy,
-                             int64_t* vwgt, int64_t* vsize, int64_t* adjwgt, int64_t* nparts,
-                             void* tpwgts, void* ubvec, int64_t* options, int64_t* edgecut,
-                             int64_t* part);
 int METIS_ComputeVertexSeparator(int64_t* nvtxs, int64_t* xadj, int64_t* adjncy, int64_t* vwgt,
                                  int64_t* options, int64_t* sepsize, int64_t* part);
 }
@@ -42,38 +41,65 @@ struct Csr {
     std::vector<int64_t> xadj, adjncy;
 };
 
-// Pattern of K + M column by column (the matrices are symmetric, so CSR row c
-// is CSC column c).  Row indices of the union are visited in ascending order.
+// Adjacency of |K| + |M| without self loops.  The reference inserts, for
+// every column c in ascending order and every row r of that column, r into
+// nbr[c] and c into nbr[r] (metis_partitioner.cpp:20-45).  For a symmetric
+// pattern the inserts reaching one vertex's set are exactly its neighbours
+// in ascending order (repeats are no-ops that leave the container
+// untouched), so each set is built here from the vertex's sorted neighbour
+// list - in parallel over vertices - with the same container and insertion
+// sequence, hence the same iteration order with libstdc++.
 Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
                  const int32_t* mc) {
-    std::vector<std::unordered_set<int64_t>> nbr(static_cast<size_t>(n));
-    std::vector<int64_t> col;
-    for (int64_t c = 0; c < n; ++c) {
-        col.clear();
-        int64_t a = kp[c], ae = kp[c + 1], b = mp[c], be = mp[c + 1];
-        while (a < ae || b < be) {  // sorted merge = union pattern of column c
+    std::vector<int64_t> deg(static_cast<size_t>(n) + 1, 0);
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt == 0) nt = 1;
+    if (nt > 64) nt = 64;
+    if (n < 4096) nt = 1;
+    auto forRange = [&](auto&& fn) {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                const int64_t b = n * t / nt, e = n * (t + 1) / nt;
+                fn(b, e);
+            });
+        for (auto& x : th) x.join();
+    };
+    // neighbours of v = union of row v of K and of M (sorted merge), minus v
+    auto forNeighbours = [&](int64_t v, auto&& visit) {
+        int64_t a = kp[v], ae = kp[v + 1], b = mp[v], be = mp[v + 1];
+        while (a < ae || b < be) {
             int64_t r;
             if (b >= be || (a < ae && kc[a] < mc[b])) r = kc[a++];
             else if (a >= ae || mc[b] < kc[a]) r = mc[b++];
             else { r = kc[a]; ++a; ++b; }
-            col.push_back(r);
+            if (r != v) visit(r);
         }
-        for (int64_t r : col) {
-            if (r == c) continue;
-            nbr[static_cast<size_t>(r)].insert(c);
-            nbr[static_cast<size_t>(c)].insert(r);
+    };
+    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(n));
+    forRange([&](int64_t b, int64_t e) {
+        std::vector<int64_t> sorted;
+        for (int64_t v = b; v < e; ++v) {
+            sorted.clear();
+            forNeighbours(v, [&](int64_t r) { sorted.push_back(r); });
+            std::unordered_set<int64_t> set;
+            for (int64_t r : sorted) set.insert(r);
+            auto& out = lists[static_cast<size_t>(v)];
+            out.assign(set.begin(), set.end());
         }
-    }
+    });
     Csr g;
     g.xadj.assign(static_cast<size_t>(n) + 1, 0);
     for (int64_t i = 0; i < n; ++i)
         g.xadj[static_cast<size_t>(i) + 1] =
-            g.xadj[static_cast<size_t>(i)] + static_cast<int64_t>(nbr[static_cast<size_t>(i)].size());
+            g.xadj[static_cast<size_t>(i)] + static_cast<int64_t>(lists[static_cast<size_t>(i)].size());
     g.adjncy.resize(static_cast<size_t>(g.xadj.back()));
-    for (int64_t i = 0; i < n; ++i) {
-        int64_t p = g.xadj[static_cast<size_t>(i)];
-        for (int64_t j : nbr[static_cast<size_t>(i)]) g.adjncy[static_cast<size_t>(p++)] = j;
-    }
+    forRange([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i)
+            std::copy(lists[static_cast<size_t>(i)].begin(), lists[static_cast<size_t>(i)].end(),
+                      g.adjncy.begin() + g.xadj[static_cast<size_t>(i)]);
+    });
+    (void)deg;
     return g;
 }
 
@@ -103,15 +129,10 @@ std::vector<int64_t> bisect(Csr g) {
     const int64_t n = static_cast<int64_t>(g.xadj.size()) - 1;
     std::vector<int64_t> part(static_cast<size_t>(n), 0);
     if (n == 0) return part;
-    int64_t nvtxs = n, ncon = 1, nparts = 2, edgecut = 0;
-    std::vector<int64_t> where(static_cast<size_t>(n), 0);
+    int64_t nvtxs = n;
     int64_t opts[kMetisNOptions];
     METIS_SetDefaultOptions(opts);
     opts[kMetisOptionSeed] = 42;
-    if (METIS_PartGraphRecursive(&nvtxs, &ncon, g.xadj.data(), g.adjncy.data(), nullptr, nullptr,
-                                 nullptr, &nparts, nullptr, nullptr, opts, &edgecut,
-                                 where.data()) != kMetisOk)
-        throw std::runtime_error("METIS_PartGraphRecursive failed");
     int64_t sepsize = 0;
     if (METIS_ComputeVertexSeparator(&nvtxs, g.xadj.data(), g.adjncy.data(), nullptr, opts,
                                      &sepsize, part.data()) != kMetisOk)

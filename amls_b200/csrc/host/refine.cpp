@@ -7,7 +7,9 @@
 // x_i = L_ii^-1 r_i, r_S -= L_Si x_i, and backward (levels top-down)
 // x_i = L_ii^-T (x_i - L_Si^T x_S).  The refinement is the subspace
 // iteration of AMLS-SIMb (papers/Improving_eigenpairs...md:288-420) on
-// nq = nev + extra vectors with T = K^-1 M, accelerated by a Chebyshev
+// nq = nev + extra vectors with T = K^-1 M (the diagonal blocks applied as
+// block-triangular GEMMs with U_i = L_ii^-T, computed once per refinement),
+// accelerated by a Chebyshev
 // filter: each outer iteration forms Y_c = C_c(2 T / a - I) Q, the unwanted
 // part of T's spectrum being [0, a] with a = 1 / (largest Ritz value), then
 //   X = T Y_c,  Kc = X^T (M Y_c),  Mc = X^T M X,  Kc c = theta Mc c,  Q <- X c
@@ -25,6 +27,7 @@ namespace amls_b200 {
 
 namespace {
 constexpr int kT = kGemmTile;
+constexpr int kTB = kGemmTileBig;
 int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 }  // namespace
 
@@ -47,9 +50,11 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     double* d = static_cast<double*>(dgD_.ensure(sizeof(double) * 3 * nn));
     double* work = static_cast<double*>(dgWork_.ensure(sizeof(double) * 6 * nn * want));
     int* kOut = static_cast<int*>(dgK_.ensure(sizeof(int) * 4));
-    std::vector<TileRef> rowT, rowK, sq, yk, ky;
-    for (int r = 0; r < n; r += kTrsmRows) rowT.push_back({0, r, 0, 0});
-    for (int r = 0; r < want; r += kTrsmRows) rowK.push_back({0, r, 0, 0});
+    double* inv = static_cast<double*>(dgInv_.ensure(sizeof(double) * (size_t)((n + 63) / 64) * 4096));
+    std::vector<TileRef> rowT, rowK, sq, yk, ky, invT;
+    for (int r = 0; r < n; r += kTrsmRows64) rowT.push_back({0, r, 0, 0});
+    for (int r = 0; r < want; r += kTrsmRows64) rowK.push_back({0, r, 0, 0});
+    for (int J = 0; J < (n + 63) / 64; ++J) invT.push_back({0, J, 0, 0});
     for (int j = 0; j < n; j += 32)
         for (int i = 0; i < n; i += 32) sq.push_back({0, i, j, 0});
     for (int j = 0; j < want; j += 32)
@@ -57,8 +62,8 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     for (int j = 0; j < n; j += 32)
         for (int i = 0; i < want; i += 32) ky.push_back({0, i, j, 0});
     FrontDesc f{M, nn, n, n, -2, 0}, fe{E, nn, n, n, -2, 0};
-    TrsmDesc t1{M, nn, K, nn, n, n, 0, 0}, t2{M, nn, E, nn, n, n, 0, 0},
-        t3{M, nn, Yt, want, n, want, 0, 1};
+    TrsmDesc t1{M, nn, K, nn, n, n, 0, 0, inv}, t2{M, nn, E, nn, n, n, 0, 0, inv},
+        t3{M, nn, Yt, want, n, want, 0, 1, inv};
     CopyDesc c1{K, nn, E, nn, n, n}, c2{Y, nn, Yt, want, n, want}, c3{Yt, want, V, ldv, want, n};
     EigDesc ed{};
     ed.A = E;
@@ -78,7 +83,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     const size_t oF = b.add(&f, 1), oFe = b.add(&fe, 1), oT1 = b.add(&t1, 1), oT2 = b.add(&t2, 1),
                  oT3 = b.add(&t3, 1), oC1 = b.add(&c1, 1), oC2 = b.add(&c2, 1), oC3 = b.add(&c3, 1),
                  oE = b.add(&ed, 1), oRow = b.add(rowT), oK = b.add(rowK), oSq = b.add(sq),
-                 oYk = b.add(yk), oKy = b.add(ky);
+                 oYk = b.add(yk), oKy = b.add(ky), oInvT = b.add(invT);
     std::vector<int> gOf, gFirst{0}, gSize;
     std::vector<int64_t> pOff{0};
     int nCta = 0;
@@ -94,14 +99,15 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
         LAUNCH(launchCholDiag(dF, 1, jb, status_.as<int>(), s));
         LAUNCH(launchCholPanel(dF, 1, jb, cdiv2(n, kTrsmRows), s));
     }
-    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
+    LAUNCH(launchInvDiag(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oInvT), static_cast<int>(invT.size()), s));
+    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
     LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC1), b.dev<TileRef>(oSq), static_cast<int>(sq.size()), s));
-    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT2), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
+    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT2), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
     LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
     const EigDesc* dE = b.dev<EigDesc>(oE);
     if (n <= 384) LAUNCH(launchTridiagSmall(dE, 1, s));
     else {
-        dgP_.ensure(sizeof(double) * nn);
+        dgP_.ensure(sizeof(double) * 2 * nn);
         LAUNCH(launchTridiagLargeGroups(dE, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         dgP_.as<double>(), b.dev<int64_t>(oPo), n, s));
     }
@@ -109,7 +115,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     LAUNCH(launchInverseIter(dE, 1, want, nullptr, s));
     LAUNCH(launchBackTransformSmem(dE, 1, want, n, s));
     LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC2), b.dev<TileRef>(oYk), static_cast<int>(yk.size()), s));
-    LAUNCH(launchTrsmRows(b.dev<TrsmDesc>(oT3), b.dev<TileRef>(oK), static_cast<int>(rowK.size()), s));
+    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT3), b.dev<TileRef>(oK), static_cast<int>(rowK.size()), s));
     LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC3), b.dev<TileRef>(oKy), static_cast<int>(ky.size()), s));
     // the tables live in dgBlob_ until the stream passes this point
     cudaCheck(cudaStreamSynchronize(s), "dense eigensolve");
@@ -133,7 +139,35 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     double* Mc = static_cast<double*>(refMc_.ensure(sizeof(double) * nq * nq));
     double* Vc = static_cast<double*>(refV_.ensure(sizeof(double) * nq * nq));
     double* wd = static_cast<double*>(refW_.ensure(sizeof(double) * nq));
+    double* Tm = static_cast<double*>(refT_.ensure(sizeof(double) * sz));
+    double* U = static_cast<double*>(refU_.ensure(sizeof(double) * std::max<int64_t>(eigTotal_, 1)));
     const double* F = kPool_.as<double>();
+
+    // U_i = L_ii^-T (upper triangular, n_i x n_i at eigOff) for every node:
+    // identity, then one row-panel TRSM  U <- U L^-T.  K^-1 is then applied
+    // with block-triangular GEMMs, which keep all SMs busy on the large
+    // separators where a row-panel TRSM has only a few row tiles.
+    {
+        Blob ub;
+        std::vector<TrsmDesc> ud;
+        std::vector<TileRef> uT;
+        for (int i : order_) {
+            const Node& nd = nodes_[static_cast<size_t>(i)];
+            if (nd.n == 0) continue;
+            TrsmDesc t{F + nd.frontOff, nd.ld, U + nd.eigOff, nd.n, static_cast<int32_t>(nd.n),
+                       static_cast<int32_t>(nd.n), 0, 0, invPool_.as<double>() + nd.invOff};
+            for (int r0 = 0; r0 < nd.n; r0 += kTrsmRows64) uT.push_back({static_cast<int32_t>(ud.size()), r0, 0, 0});
+            ud.push_back(t);
+        }
+        const size_t oD = ub.add(ud), oT = ub.add(uT);
+        ub.upload(refUBlob_, s);
+        const int64_t* dOffs = eigOffsDev();
+        const int64_t* dSizes = nodeSizesDev();
+        LAUNCH(launchIdentityBlocks(U, dOffs, dSizes, static_cast<int>(order_.size()), s));
+        LAUNCH(launchTrsmRows64(ub.dev<TrsmDesc>(oD), ub.dev<TileRef>(oT), static_cast<int>(uT.size()), s));
+        cudaCheck(cudaStreamSynchronize(s), "U = L^-T");
+        for (const Node& nd : nodes_) catF_[1] += static_cast<double>(nd.n) * nd.n * nd.n;
+    }
 
     // ---- tables: K^-1 sweeps, Rayleigh-Ritz products, subspace update ----
     Blob b;
@@ -157,7 +191,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
     double fsolve = 0;
     for (int l = 0; l <= maxLevel_; ++l) {
-        std::vector<TrsmDesc> ft, bt;
+        std::vector<GemmDesc> ft, bt;
         std::vector<GemmDesc> fg, bg;
         std::vector<TileRef> ftT, fgT, bgT, btT;
         for (int i : byLevel_[static_cast<size_t>(l)]) {
@@ -165,13 +199,41 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
             if (ni == 0) continue;
             double* Xi = X + nd.off * nq;
-            TrsmDesc tf{F + nd.frontOff, nd.ld, Xi, nq, static_cast<int32_t>(ni), nq, 0, 0,
-                        invPool_.as<double>() + nd.invOff};
-            for (int r = 0; r < nq; r += kTrsmRows64) ftT.push_back({static_cast<int32_t>(ft.size()), r, 0, 0});
+            double* Ti = Tm + nd.off * nq;
+            const double* Ui = U + nd.eigOff;
+            // forward: T_i = X_i U_i  (= (L_ii^-1 x_i)^T)
+            GemmDesc tf{};
+            tf.M = nq;
+            tf.N = static_cast<int32_t>(ni);
+            tf.K = static_cast<int32_t>(ni);
+            tf.flags = kTriKUpTo;
+            tf.A = Xi;
+            tf.lda = nq;
+            tf.B = Ui;
+            tf.ldb = ni;
+            tf.C = Ti;
+            tf.ldc = nq;
+            tf.alpha = 1.0;
+            for (int jt = 0; jt < cdiv2(ni, kTB); ++jt)
+                for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                    ftT.push_back({static_cast<int32_t>(ft.size()), it * kTB, jt * kTB, 0});
             ft.push_back(tf);
-            TrsmDesc tb = tf;
-            tb.backward = 1;
-            for (int r = 0; r < nq; r += kTrsmRows64) btT.push_back({static_cast<int32_t>(bt.size()), r, 0, 0});
+            // backward: X_i = T_i U_i^T  (= (L_ii^-T t_i)^T)
+            GemmDesc tb{};
+            tb.M = nq;
+            tb.N = static_cast<int32_t>(ni);
+            tb.K = static_cast<int32_t>(ni);
+            tb.flags = kTransB | kTriKFrom;
+            tb.A = Ti;
+            tb.lda = nq;
+            tb.B = Ui;
+            tb.ldb = ni;
+            tb.C = Xi;
+            tb.ldc = nq;
+            tb.alpha = 1.0;
+            for (int jt = 0; jt < cdiv2(ni, kTB); ++jt)
+                for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                    btT.push_back({static_cast<int32_t>(bt.size()), it * kTB, jt * kTB, 0});
             bt.push_back(tb);
             fsolve += 2.0 * nq * ni * ni;
             if (si > 0) {
@@ -180,7 +242,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 g.N = static_cast<int32_t>(si);
                 g.K = static_cast<int32_t>(ni);
                 g.flags = kTransB | kScatter | kAtomic;
-                g.A = Xi;
+                g.A = Tm + nd.off * nq;
                 g.lda = nq;
                 g.B = F + nd.frontOff + ni;
                 g.ldb = nd.ld;
@@ -188,9 +250,9 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 g.alpha = -1.0;
                 g.rowIdx = dId;
                 g.colOff = dCo + colOffStart[static_cast<size_t>(i)];
-                for (int jt = 0; jt < cdiv2(si, kT); ++jt)
-                    for (int it = 0; it < cdiv2(nq, kT); ++it)
-                        fgT.push_back({static_cast<int32_t>(fg.size()), it * kT, jt * kT, 0});
+                for (int jt = 0; jt < cdiv2(si, kTB); ++jt)
+                    for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                        fgT.push_back({static_cast<int32_t>(fg.size()), it * kTB, jt * kTB, 0});
                 fg.push_back(g);
                 GemmDesc h{};
                 h.M = nq;
@@ -202,13 +264,13 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 h.aMap = sIdxDev_ + nd.mapCol;
                 h.B = F + nd.frontOff + ni;
                 h.ldb = nd.ld;
-                h.C = Xi;
+                h.C = Tm + nd.off * nq;
                 h.ldc = nq;
                 h.alpha = -1.0;
                 h.beta = 1.0;
-                for (int jt = 0; jt < cdiv2(ni, kT); ++jt)
-                    for (int it = 0; it < cdiv2(nq, kT); ++it)
-                        bgT.push_back({static_cast<int32_t>(bg.size()), it * kT, jt * kT, 0});
+                for (int jt = 0; jt < cdiv2(ni, kTB); ++jt)
+                    for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                        bgT.push_back({static_cast<int32_t>(bg.size()), it * kTB, jt * kTB, 0});
                 bg.push_back(h);
                 fsolve += 4.0 * nq * ni * si;
             }
@@ -237,8 +299,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         g.alpha = 1.0;
         g.kChunk = chunk;
         for (int kc = 0; kc < cdiv2(n, chunk); ++kc)
-            for (int jt = 0; jt < cdiv2(nq, kT); ++jt)
-                for (int it = 0; it < cdiv2(nq, kT); ++it) rrT.push_back({q, it * kT, jt * kT, kc});
+            for (int jt = 0; jt < cdiv2(nq, kTB); ++jt)
+                for (int it = 0; it < cdiv2(nq, kTB); ++it) rrT.push_back({q, it * kTB, jt * kTB, kc});
     }
     {
         GemmDesc& g = up[0];
@@ -253,8 +315,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         g.C = Q;
         g.ldc = nq;
         g.alpha = 1.0;
-        for (int jt = 0; jt < cdiv2(n, kT); ++jt)
-            for (int it = 0; it < cdiv2(nq, kT); ++it) upT.push_back({0, it * kT, jt * kT, 0});
+        for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
+            for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({0, it * kTB, jt * kTB, 0});
     }
     FrontDesc sym[2] = {{Kc, nq, nq, nq, -3, 0}, {Mc, nq, nq, nq, -3, 0}};
     const size_t oRR = b.add(rr), oRRT = b.add(rrT), oUP = b.add(up), oUPT = b.add(upT),
@@ -269,18 +331,17 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
+            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
+            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
         }
         for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
-            LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
+            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
+            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
         }
         catF_[8] += 2.0 * nnzM_ * dq;
         catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
-        catF_[1] += fsolve / 2;
-        catF_[2] += fsolve / 2;
+        catF_[2] += fsolve;
     };
     // Chebyshev recurrence buffers (degree = refine - 1)
     const int cheb = std::max(0, opt_.refine - 1);
@@ -315,10 +376,10 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                            permDev_.as<int64_t>(), invDev_.as<int64_t>(), X, nq, MX, s));
         cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
         cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
+        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
         LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
         denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT), static_cast<int>(upT.size()), s));
+        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT), static_cast<int>(upT.size()), s));
         std::vector<double> th(static_cast<size_t>(nq));
         cudaCheck(cudaMemcpyAsync(th.data(), wd, sizeof(double) * nq, cudaMemcpyDeviceToHost, s), "theta");
         cudaCheck(cudaStreamSynchronize(s), "refine");

@@ -26,6 +26,8 @@ enum GemmFlags : int32_t {
     kRowScale = 32,     // multiply result row i by rowScale[i]
     kColScale = 64,     // multiply result column j by colScale[j]
     kAccumulate = 128,  // dense: C = alpha*AB + beta*C ; scatter: *dst += alpha*AB
+    kTriKUpTo = 256,    // op(B) upper triangular: column j uses k <= j only
+    kTriKFrom = 512,    // op(B) lower triangular: column j uses k >= j only
 };
 
 struct GemmDesc {
@@ -55,6 +57,10 @@ constexpr int kGemmTile = 64;
 
 cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
                               cudaStream_t s);
+// Same operation with 128 x 128 tiles (TileRef m0/n0 multiples of 128).
+constexpr int kGemmTileBig = 128;
+cudaError_t launchGemmBatchedBig(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
+                                 cudaStream_t s);
 
 // Extend-add update of one eliminated front (multifrontal form of the
 // reference's Schur + congruence updates):
@@ -133,7 +139,8 @@ struct EigDesc {
 cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s);
 // Cooperative multi-CTA tridiagonalisation of a batch of large matrices: the
 // grid is split into CTA groups, group g (CTAs groupFirst[g] ..
-// + groupSize[g]) works on descs[g]; p vectors at dP + dPOff[g].
+// + groupSize[g]) works on descs[g]; p accumulators at dP + 2 * dPOff[g]
+// (2 n doubles per matrix: dP must hold 2 * sum n).
 cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
                                      const int* dGroupFirst, const int* dGroupSize, int nCta,
                                      double* dP, const int64_t* dPOff, int maxN, cudaStream_t s);
@@ -206,6 +213,9 @@ cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, cons
 // out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
 cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
                          double c, const double* z, double* out, cudaStream_t s);
+// Block b (size[b] x size[b] at pool + off[b], ld size[b]) set to the identity.
+cudaError_t launchIdentityBlocks(double* pool, const int64_t* off, const int64_t* size, int nBlocks,
+                                 cudaStream_t s);
 // out[i] = 1 / in[i]   (reciprocals, for eigenvalue maps)
 cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s);
 

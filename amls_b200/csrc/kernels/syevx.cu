@@ -133,14 +133,20 @@ struct LargeArgs {
     const int* groupOf;       // CTA -> group (matrix)
     const int* groupFirst;    // first CTA of each group
     const int* groupSize;     // CTAs in each group
-    double* pbuf;             // per matrix p vectors (offsets = pOff)
+    double* pbuf;             // per matrix 2 n doubles of p accumulators (offsets 2 * pOff)
     const int64_t* pOff;
     int maxN;
 };
 
 __global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
-    extern __shared__ double sv[];   // v (maxN)
+    // Work per column step is split into units (column j of the trailing
+    // matrix, 256-row segment) handed out over all warps of the group: the
+    // symmetric mat-vec p = tau A22 v accumulates per-unit partial dot
+    // products into p with atomics (p double-buffered by step parity and
+    // cleared one step ahead), and the rank-2 update walks the same units.
+    extern __shared__ double sv[];   // v (maxN), then w (maxN)
     __shared__ double red[32];
+    constexpr int SEG = 256;
     cg::grid_group grid = cg::this_grid();
     const int g = a.groupOf[blockIdx.x];
     const int rank = blockIdx.x - a.groupFirst[g];
@@ -149,13 +155,20 @@ __global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
     const int n = D.n;
     double* A = D.A;
     const int64_t lda = D.lda;
-    double* p = a.pbuf + a.pOff[g];
+    double* pb[2] = {a.pbuf + 2 * a.pOff[g], a.pbuf + 2 * a.pOff[g] + n};
+    double* sw = sv + a.maxN;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     const int gw = rank * nw + wid, GW = gsize * nw;
+    const int gt = rank * blockDim.x + tid, GT = gsize * blockDim.x;
+    // p buffers start cleared
+    for (int i = gt; i < 2 * n; i += GT) a.pbuf[2 * a.pOff[g] + i] = 0.0;
+    grid.sync();
     for (int k = 0; k + 2 < a.maxN; ++k) {
         const bool active = k + 2 < n;
         const int m = n - k - 1;
+        const int segs = (m + SEG - 1) / SEG;
         double* col = A + (k + 1) + (int64_t)k * lda;
+        double* p = pb[k & 1];
         HouseholderScalars h{0.0, 0.0, 0.0};
         if (active) {
             double part = 0.0;
@@ -166,30 +179,35 @@ __global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
             __syncthreads();
             if (h.tau != 0.0) {
                 const double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
-                for (int j = gw; j < m; j += GW) {
+                for (int u = gw; u < m * segs; u += GW) {
+                    const int j = u / segs, s0 = (u % segs) * SEG;
+                    const int s1 = min(m, s0 + SEG);
                     const double* cj = A22 + (int64_t)j * lda;
-                    double s = 0.0;
-                    for (int i = lane; i < m; i += 32) s += cj[i] * sv[i];
-                    s = warpSum<32>(s);
-                    if (lane == 0) p[j] = h.tau * s;
+                    double sum = 0.0;
+                    for (int i = s0 + lane; i < s1; i += 32) sum += cj[i] * sv[i];
+                    sum = warpSum<32>(sum);
+                    if (lane == 0) atomicAdd(p + j, h.tau * sum);
                 }
             }
         }
         grid.sync();
         if (active) {
+            double* pn = pb[(k + 1) & 1];
+            for (int i = gt; i < m; i += GT) pn[i] = 0.0;     // next step's accumulator
             if (h.tau != 0.0) {
                 double pv = 0.0;
                 for (int i = tid; i < m; i += blockDim.x) pv += p[i] * sv[i];
                 pv = blockSum(pv, red);
                 const double a2 = -0.5 * h.tau * pv;
+                for (int i = tid; i < m; i += blockDim.x) sw[i] = p[i] + a2 * sv[i];
+                __syncthreads();
                 double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
-                for (int j = gw; j < m; j += GW) {
+                for (int u = gw; u < m * segs; u += GW) {
+                    const int j = u / segs, s0 = (u % segs) * SEG;
+                    const int s1 = min(m, s0 + SEG);
                     double* cj = A22 + (int64_t)j * lda;
-                    const double vj = sv[j], wj = p[j] + a2 * vj;
-                    for (int i = lane; i < m; i += 32) {
-                        const double wi = p[i] + a2 * sv[i];
-                        cj[i] -= sv[i] * wj + wi * vj;
-                    }
+                    const double vj = sv[j], wj = sw[j];
+                    for (int i = s0 + lane; i < s1; i += 32) cj[i] -= sv[i] * wj + sw[i] * vj;
                 }
             }
             if (rank == 0) {
@@ -218,7 +236,7 @@ cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
                                      double* dP, const int64_t* dPOff, int maxN, cudaStream_t s) {
     LargeArgs a{dDescs, dGroupOf, dGroupFirst, dGroupSize, dP, dPOff, maxN};
     void* args[] = {&a};
-    const size_t smem = (size_t)maxN * sizeof(double);
+    const size_t smem = 2 * (size_t)maxN * sizeof(double);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(tridiagLargeKernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -231,7 +249,7 @@ int tridiagLargeMaxCtas(int maxN) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = (size_t)maxN * sizeof(double);
+    const size_t smem = 2 * (size_t)maxN * sizeof(double);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(tridiagLargeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiagLargeKernel, 256, smem);
