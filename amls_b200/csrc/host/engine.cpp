@@ -126,6 +126,7 @@ int Engine::profBegin(const char* text) {
     }
     cudaCheck(cudaEventRecord(evPool_[evUsed_], stream_), "cudaEventRecord");
     evCat_.push_back(cat);
+    evText_.push_back(text);
     return cat;
 }
 
@@ -144,9 +145,12 @@ void Engine::profCollect() {
         const int c = evCat_[k / 2];
         profMs_[c] += ms;
         profCount_[c] += 1;
+        if (opt_.verbosity >= 3)   // per-launch log: launcher name and device time
+            std::fprintf(stderr, "[amls_b200] launch %.48s %.4f ms\n", evText_[k / 2], ms);
     }
     evUsed_ = 0;
     evCat_.clear();
+    evText_.clear();
 }
 
 void Engine::setProfiling(bool on) {
@@ -337,6 +341,27 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     permDev_.ensure(sizeof(int64_t) * static_cast<size_t>(n));
     kDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzK_, 1)));
     mDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+    // groups of consecutive rows with identical M column patterns (the DOFs
+    // of one mesh node), at most kSpmmGroup rows each, for the grouped SpMM
+    {
+        std::vector<int64_t> grp;
+        int64_t r = 0;
+        while (r < n) {
+            grp.push_back(r);
+            const int64_t len = mp[r + 1] - mp[r];
+            int64_t e = r + 1;
+            while (e < n && e - r < kSpmmGroup && mp[e + 1] - mp[e] == len &&
+                   std::equal(mc + mp[r], mc + mp[r + 1], mc + mp[e]))
+                ++e;
+            r = e;
+        }
+        grp.push_back(n);
+        nGrp_ = static_cast<int64_t>(grp.size()) - 1;
+        mGrp_.ensure(sizeof(int64_t) * grp.size());
+        cudaCheck(cudaMemcpyAsync(mGrp_.as<int64_t>(), grp.data(), sizeof(int64_t) * grp.size(),
+                                  cudaMemcpyHostToDevice, stream_), "upload");
+        cudaCheck(cudaStreamSynchronize(stream_), "upload");
+    }
     cudaCheck(cudaMemcpyAsync(mRp_.as<int64_t>(), mp, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, stream_), "upload");
     cudaCheck(cudaMemcpyAsync(mCi_.as<int32_t>(), mc, sizeof(int32_t) * nnzM_, cudaMemcpyHostToDevice, stream_), "upload");
     cudaCheck(cudaMemcpyAsync(invDev_.as<int64_t>(), inv_.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, stream_), "upload");
@@ -615,6 +640,52 @@ void Engine::checkStatus(const char* phase) {
 // ---------------------------------------------------------------------------
 // eigen driver
 // ---------------------------------------------------------------------------
+// Cooperative tridiagonalisation of the matrices in `large`, in launches of at
+// most tridiagLargeMaxCtas(maxN) matrices (one CTA per SM), each matrix given
+// CTAs in proportion to n^2.  The stream is synchronised before returning
+// (the launch tables live in `blob`).
+void Engine::tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, DevBuf& blob,
+                             cudaStream_t s) {
+    size_t g0 = 0;
+    while (g0 < large.size()) {
+        int maxN = 0;
+        for (size_t g = g0; g < large.size(); ++g) maxN = std::max<int>(maxN, large[g].n);
+        const int maxCta = tridiagLargeMaxCtas(maxN);
+        if (maxCta < 1) throw AmlsError(AMLS_ERR_CUDA, "cooperative tridiagonalisation does not fit");
+        const size_t g1 = std::min(large.size(), g0 + static_cast<size_t>(maxCta));
+        const int cnt = static_cast<int>(g1 - g0);
+        std::vector<EigDesc> part(large.begin() + static_cast<std::ptrdiff_t>(g0),
+                                  large.begin() + static_cast<std::ptrdiff_t>(g1));
+        std::vector<int> groupOf, groupFirst, groupSize;
+        std::vector<int64_t> pOff;
+        int64_t pTot = 0;
+        double wsum = 0;
+        for (auto& e : part) wsum += static_cast<double>(e.n) * e.n;
+        int used = 0;
+        for (int g = 0; g < cnt; ++g) {
+            const double share = static_cast<double>(part[static_cast<size_t>(g)].n) * part[static_cast<size_t>(g)].n / wsum;
+            int c = std::max(1, static_cast<int>(std::floor(maxCta * share)));
+            c = std::max(1, std::min(c, maxCta - used - (cnt - g - 1)));
+            groupFirst.push_back(used);
+            groupSize.push_back(c);
+            for (int q = 0; q < c; ++q) groupOf.push_back(g);
+            used += c;
+            pOff.push_back(pTot);
+            pTot += part[static_cast<size_t>(g)].n;
+        }
+        Blob b;
+        const size_t oL = b.add(part), oGo = b.add(groupOf), oGf = b.add(groupFirst),
+                     oGs = b.add(groupSize), oPo = b.add(pOff);
+        b.upload(blob, s);
+        pbuf.ensure(sizeof(double) * static_cast<size_t>(kTridiagPBufs * pTot + 1));
+        LAUNCH(launchTridiagLargeGroups(b.dev<EigDesc>(oL), b.dev<int>(oGo), b.dev<int>(oGf),
+                                        b.dev<int>(oGs), used, pbuf.as<double>(), b.dev<int64_t>(oPo),
+                                        maxN, s));
+        cudaCheck(cudaStreamSynchronize(s), "tridiagonalise");
+        g0 = g1;
+    }
+}
+
 void Engine::tridiagonalizeAll(cudaStream_t s) {
     std::vector<EigDesc> small, large;
     int maxLargeN = 0;
@@ -636,30 +707,7 @@ void Engine::tridiagonalizeAll(cudaStream_t s) {
         }
     }
     Blob b;
-    const size_t oS = b.add(small), oL = b.add(large);
-    // group table for the cooperative launch
-    std::vector<int> groupOf, groupFirst, groupSize;
-    std::vector<int64_t> pOff;
-    int64_t pTot = 0;
-    if (!large.empty()) {
-        const int maxCta = tridiagLargeMaxCtas(maxLargeN);
-        double wsum = 0;
-        for (auto& e : large) wsum += static_cast<double>(e.n) * e.n;
-        int used = 0;
-        for (size_t g = 0; g < large.size(); ++g) {
-            int cnt = std::max(1, static_cast<int>(std::floor(maxCta * (static_cast<double>(large[g].n) * large[g].n) / wsum)));
-            cnt = std::min(cnt, maxCta - used - static_cast<int>(large.size() - g - 1));
-            cnt = std::max(cnt, 1);
-            groupFirst.push_back(used);
-            groupSize.push_back(cnt);
-            for (int c = 0; c < cnt; ++c) groupOf.push_back(static_cast<int>(g));
-            used += cnt;
-            pOff.push_back(pTot);
-            pTot += large[g].n;
-        }
-        if (used > maxCta) throw AmlsError(AMLS_ERR_CUDA, "too many large eigenproblems for one cooperative launch");
-    }
-    const size_t oGo = b.add(groupOf), oGf = b.add(groupFirst), oGs = b.add(groupSize), oPo = b.add(pOff);
+    const size_t oS = b.add(small);
     b.upload(tlBlob_, s);
     for (const auto& e : small) {
         catF_[4] += 4.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
@@ -669,13 +717,9 @@ void Engine::tridiagonalizeAll(cudaStream_t s) {
         catF_[4] += 4.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
         catB_[4] += 8.0 / 3.0 * e.n * static_cast<double>(e.n) * e.n;
     }
+    (void)maxLargeN;
     if (!small.empty()) LAUNCH(launchTridiagSmall(b.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
-    if (!large.empty()) {
-        redP_.ensure(sizeof(double) * static_cast<size_t>(2 * pTot));
-        LAUNCH(launchTridiagLargeGroups(b.dev<EigDesc>(oL), b.dev<int>(oGo), b.dev<int>(oGf),
-                                        b.dev<int>(oGs), static_cast<int>(groupOf.size()),
-                                        redP_.as<double>(), b.dev<int64_t>(oPo), maxLargeN, s));
-    }
+    tridiagLargeAll(large, redP_, tlLargeBlob_, s);
     // keep the blob alive until the work is done
     cudaCheck(cudaStreamSynchronize(s), "tridiagonalise");
     tridiagDone_ = true;
@@ -999,7 +1043,7 @@ int Engine::reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors) {
     const EigDesc* dd = b.dev<EigDesc>(o);
     if (p <= kSmallEig) LAUNCH(launchTridiagSmall(dd, 1, s));
     else {
-        redP_.ensure(sizeof(double) * static_cast<size_t>(2 * p));
+        redP_.ensure(sizeof(double) * static_cast<size_t>(kTridiagPBufs * p));
         LAUNCH(launchTridiagLargeGroups(dd, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         redP_.as<double>(), b.dev<int64_t>(oPo), static_cast<int>(p), s));
     }
@@ -1341,33 +1385,11 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
         copyTiles(cp3T, static_cast<int>(cp3.size()), c.c, c.r);
         cp3.push_back(r);
     }
-    std::vector<int> gOf, gFirst, gSize;
-    std::vector<int64_t> pOff;
-    int64_t pTot = 0;
-    if (!large.empty()) {
-        const int maxCta = tridiagLargeMaxCtas(maxLargeN);
-        if (static_cast<int>(large.size()) > maxCta)
-            throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "too many large matrices in one batch");
-        double wsum = 0;
-        for (auto& e : large) wsum += static_cast<double>(e.n) * e.n;
-        int used = 0;
-        for (size_t g = 0; g < large.size(); ++g) {
-            int cnt = std::max(1, static_cast<int>(std::floor(maxCta * (static_cast<double>(large[g].n) * large[g].n) / wsum)));
-            cnt = std::max(1, std::min(cnt, maxCta - used - static_cast<int>(large.size() - g - 1)));
-            gFirst.push_back(used);
-            gSize.push_back(cnt);
-            for (int c = 0; c < cnt; ++c) gOf.push_back(static_cast<int>(g));
-            used += cnt;
-            pOff.push_back(pTot);
-            pTot += large[g].n;
-        }
-    }
     Blob B;
     const size_t ofF = B.add(fF), ofE = B.add(fE), ot1 = B.add(t1), ot1T = B.add(t1T), ocp = B.add(cp),
                  ocpT = B.add(cpT), ot2 = B.add(t2), ot2T = B.add(t2T), oS = B.add(small), oL = B.add(large),
                  oA = B.add(all), ocp2 = B.add(cp2), ocp2T = B.add(cp2T), ot3 = B.add(t3), ot3T = B.add(t3T),
-                 ocp3 = B.add(cp3), ocp3T = B.add(cp3T), oGo = B.add(gOf), oGf = B.add(gFirst),
-                 oGs = B.add(gSize), oPo = B.add(pOff);
+                 ocp3 = B.add(cp3), ocp3T = B.add(cp3T);
     B.upload(blob, s);
     const int nb = static_cast<int>(fF.size());
     const int maxBlocks = cdiv(maxN, kCholBlock), maxRowTiles = cdiv(maxN, kTrsmRows);
@@ -1380,12 +1402,9 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
     LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot2), B.dev<TileRef>(ot2T), static_cast<int>(t2T.size()), s));
     LAUNCH(launchSymmetrize(B.dev<FrontDesc>(ofE), nb, s));
     if (!small.empty()) LAUNCH(launchTridiagSmall(B.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
-    if (!large.empty()) {
-        pbuf.ensure(sizeof(double) * (2 * pTot + 1));
-        LAUNCH(launchTridiagLargeGroups(B.dev<EigDesc>(oL), B.dev<int>(oGo), B.dev<int>(oGf), B.dev<int>(oGs),
-                                        static_cast<int>(gOf.size()), pbuf.as<double>(), B.dev<int64_t>(oPo),
-                                        maxLargeN, s));
-    }
+    (void)oL;
+    (void)maxLargeN;
+    tridiagLargeAll(large, pbuf, tlLargeBlob_, s);
     int maxK = 0;
     for (auto x : kc) maxK = std::max<int>(maxK, static_cast<int>(x));
     const int bmode = mode == 0 ? 2 : 3;

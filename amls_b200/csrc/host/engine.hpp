@@ -94,6 +94,7 @@ private:
     void buildStatic();
     void eliminate(cudaStream_t s);
     void tridiagonalizeAll(cudaStream_t s);
+    void tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, DevBuf& blob, cudaStream_t s);
     void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
     int reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors = true);
     // z^T (m x n, permuted order) into ztPool_
@@ -132,6 +133,8 @@ private:
     DevBuf kPool_, mPool_, eigPool_, dPool_, ePool_, tauPool_, invPool_;
     DevBuf kVal_, mVal_, kDst_, mDst_;             // CSR values and their front destinations
     DevBuf mRp_, mCi_, invDev_, permDev_;          // original M CSR pattern, maps
+    DevBuf mGrp_;                                  // row groups with one M pattern
+    int64_t nGrp_ = 0;
     DevBuf staticInts_;                            // extend-add and panel maps
     DevBuf staticBlob_;                            // level launch tables
     DevBuf status_;
@@ -165,7 +168,7 @@ private:
     // per-pass device buffers
     DevBuf yPool_, wPool_, kOutDev_, iiWork_, panelPool_, wtPool_, credPool_;
     DevBuf redY_, redW_, redWork_, redD_, redE_, redTau_, redK_, redP_;
-    DevBuf ztPool_, zOut_, norms_, sqrtTheta_, passBlob_, tlBlob_, redBlob_, idxBlob_;
+    DevBuf ztPool_, zOut_, norms_, sqrtTheta_, passBlob_, tlBlob_, redBlob_, idxBlob_, tlLargeBlob_;
     const int32_t* sIdxDev_ = nullptr;              // S_i lists (device, static)
     const int32_t* rowSDev_ = nullptr;             // panel rows of S_i (device, static)
     std::vector<int64_t> panelOff_;                // per node (doubles), -1 none
@@ -174,7 +177,7 @@ private:
     // refinement and the device dense eigensolver
     DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
-    DevBuf refT_, refU_, refUBlob_, nodeOffDev_;
+    DevBuf refT_, refU_, refUBlob_, nodeOffDev_, refMQ_;
     const int64_t* eigOffsDev();
     const int64_t* nodeSizesDev();
     int refineIters_ = 0, refineNq_ = 0;
@@ -187,6 +190,7 @@ private:
     std::vector<cudaEvent_t> evPool_;
     size_t evUsed_ = 0;
     std::vector<int> evCat_;
+    std::vector<const char*> evText_;
     double profMs_[kProfCats] = {0};
     int64_t profCount_[kProfCats] = {0};
     cudaEvent_t evSolve0_ = nullptr, evSolve1_ = nullptr;

@@ -107,7 +107,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     const EigDesc* dE = b.dev<EigDesc>(oE);
     if (n <= 384) LAUNCH(launchTridiagSmall(dE, 1, s));
     else {
-        dgP_.ensure(sizeof(double) * 2 * nn);
+        dgP_.ensure(sizeof(double) * kTridiagPBufs * nn);
         LAUNCH(launchTridiagLargeGroups(dE, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
                                         dgP_.as<double>(), b.dev<int64_t>(oPo), n, s));
     }
@@ -302,32 +302,45 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             for (int jt = 0; jt < cdiv2(nq, kTB); ++jt)
                 for (int it = 0; it < cdiv2(nq, kTB); ++it) rrT.push_back({q, it * kTB, jt * kTB, kc});
     }
-    {
-        GemmDesc& g = up[0];
+    // subspace update Q = Vc^T X and, for the next iteration's first K^-1 M
+    // application, M Q = Vc^T (M X) (a GEMM instead of a sparse product)
+    double* MQ = static_cast<double*>(refMQ_.ensure(sizeof(double) * sz));
+    up.resize(2);
+    for (int q = 0; q < 2; ++q) {
+        GemmDesc& g = up[static_cast<size_t>(q)];
         g.M = nq;
         g.N = static_cast<int32_t>(n);
         g.K = nq;
         g.flags = kTransA;
         g.A = Vc;
         g.lda = nq;
-        g.B = X;
+        g.B = q == 0 ? X : MX;
         g.ldb = nq;
-        g.C = Q;
+        g.C = q == 0 ? Q : MQ;
         g.ldc = nq;
         g.alpha = 1.0;
-        for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
-            for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({0, it * kTB, jt * kTB, 0});
     }
+    for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
+        for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({0, it * kTB, jt * kTB, 0});
+    const int nUp1 = static_cast<int>(upT.size());
+    for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
+        for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({1, it * kTB, jt * kTB, 0});
     FrontDesc sym[2] = {{Kc, nq, nq, nq, -3, 0}, {Mc, nq, nq, nq, -3, 0}};
     const size_t oRR = b.add(rr), oRRT = b.add(rrT), oUP = b.add(up), oUPT = b.add(upT),
                  oSym = b.add(sym, 2);
     b.upload(refBlob_, s);
 
     const double dn = static_cast<double>(n), dq = nq;
-    // the K^-1 M application on Y (nq x n): R = M Y, X = K^-1 R
-    auto applyT = [&](const double* Y) {
-        LAUNCH(launchSpmmT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n,
-                           permDev_.as<int64_t>(), invDev_.as<int64_t>(), Y, nq, R, s));
+    auto spmm = [&](const double* Y, double* out) {
+        LAUNCH(launchSpmmGroupT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), nGrp_,
+                                mGrp_.as<int64_t>(), invDev_.as<int64_t>(), Y, nq, out, s));
+        catF_[8] += 2.0 * nnzM_ * dq;
+        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
+    };
+    // the K^-1 M application on Y (nq x n): R = M Y (or the given M Y), X = K^-1 R
+    auto applyT = [&](const double* Y, const double* MY) {
+        if (MY) cudaCheck(cudaMemcpyAsync(R, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+        else spmm(Y, R);
         cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
@@ -339,8 +352,6 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
             LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
         }
-        catF_[8] += 2.0 * nnzM_ * dq;
-        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
         catF_[2] += fsolve;
     };
     // Chebyshev recurrence buffers (degree = refine - 1)
@@ -349,6 +360,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     double* Y2 = cheb >= 2 ? static_cast<double*>(refY2_.ensure(sizeof(double) * sz)) : nullptr;
     std::vector<double> prev(theta.begin(), theta.end());
     std::vector<double> prevChange(static_cast<size_t>(nev), -1.0);
+    bool haveMQ = false;                                 // MQ = M Q is current
     int it = 0;
     for (; it < std::max(1, opt_.refineMaxIter); ++it) {
         // filter: Y_c = C_c(2 T / a - I) Q on the damped interval [0, a] of
@@ -356,37 +368,35 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         const double a = 1.0 / prev.back();
         const double sc = 2.0 / a;
         const double* Yc = Q;
+        const double* MYc = haveMQ ? MQ : nullptr;
         if (cheb >= 1) {
             double* Ym1 = Q;
             double* Yk = Y1;
-            applyT(Q);
+            applyT(Q, MYc);
             LAUNCH(launchAxpby3(sz, sc, X, -1.0, Q, 0.0, nullptr, Y1, s));     // Y1 = s T Q - Q
             for (int k = 1; k < cheb; ++k) {
                 double* Yn = (k == 1) ? Y2 : (Ym1 == Q ? Y2 : Ym1);
-                applyT(Yk);
+                applyT(Yk, nullptr);
                 // Y_{k+1} = 2 (s T Y_k - Y_k) - Y_{k-1}
                 LAUNCH(launchAxpby3(sz, 2.0 * sc, X, -2.0, Yk, -1.0, Ym1, Yn, s));
                 Ym1 = Yk;
                 Yk = Yn;
             }
             Yc = Yk;
+            MYc = nullptr;
         }
-        applyT(Yc);                                      // X = T Y_c, R = M Y_c = K X
-        LAUNCH(launchSpmmT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n,
-                           permDev_.as<int64_t>(), invDev_.as<int64_t>(), X, nq, MX, s));
+        applyT(Yc, MYc);                                 // X = T Y_c, R = M Y_c = K X
+        spmm(X, MX);
         cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
         cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
         LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
         LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
         denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
-        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT), static_cast<int>(upT.size()), s));
         std::vector<double> th(static_cast<size_t>(nq));
         cudaCheck(cudaMemcpyAsync(th.data(), wd, sizeof(double) * nq, cudaMemcpyDeviceToHost, s), "theta");
         cudaCheck(cudaStreamSynchronize(s), "refine");
-        catF_[8] += 2.0 * nnzM_ * dq;
-        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
-        catF_[2] += 3.0 * 2.0 * dn * dq * dq;
-        catB_[2] += 8.0 * (5.0 * dn * dq);
+        catF_[2] += 2.0 * 2.0 * dn * dq * dq;
+        catB_[2] += 8.0 * (3.0 * dn * dq);
         // error estimate per wanted value: change * r / (1 - r), r the observed
         // contraction of the change (geometric convergence)
         double est = 0.0;
@@ -406,6 +416,13 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         prev = th;
         if (opt_.verbosity > 1)
             std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e\n", it + 1, est);
+        const bool last = est <= opt_.refineTol || it + 1 >= std::max(1, opt_.refineMaxIter);
+        // Q = Vc^T X, and M Q for the next iteration unless this is the last
+        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
+                                    last ? nUp1 : static_cast<int>(upT.size()), s));
+        catF_[2] += (last ? 1.0 : 2.0) * 2.0 * dn * dq * dq;
+        catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;
+        haveMQ = !last;
         if (est <= opt_.refineTol) {
             ++it;
             break;

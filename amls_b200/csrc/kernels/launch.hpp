@@ -139,8 +139,11 @@ struct EigDesc {
 cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s);
 // Cooperative multi-CTA tridiagonalisation of a batch of large matrices: the
 // grid is split into CTA groups, group g (CTAs groupFirst[g] ..
-// + groupSize[g]) works on descs[g]; p accumulators at dP + 2 * dPOff[g]
-// (2 n doubles per matrix: dP must hold 2 * sum n).
+// + groupSize[g]) works on descs[g]; p accumulators at
+// dP + kTridiagPBufs * dPOff[g] (kTridiagPBufs * n doubles per matrix: dP must
+// hold kTridiagPBufs * sum n).  One CTA of kTridiagLargeThreads per SM.
+constexpr int kTridiagPBufs = 3;
+constexpr int kTridiagLargeThreads = 1024;
 cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
                                      const int* dGroupFirst, const int* dGroupSize, int nCta,
                                      double* dP, const int64_t* dPOff, int maxN, cudaStream_t s);
@@ -203,6 +206,12 @@ cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, con
 cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
                         const int64_t* perm, const int64_t* inv, const double* Qt, int m,
                         double* Rt, cudaStream_t s);
+// The same over groups of consecutive original rows with one shared column
+// pattern (grp: ngrp + 1 row starts, groups of at most kSpmmGroup rows).
+constexpr int kSpmmGroup = 4;
+cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
+                             const int64_t* grp, const int64_t* inv, const double* Qt, int m,
+                             double* Rt, cudaStream_t s);
 // Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
 // (n x nmodes, original order): see sensitivity.cu.  weight[k] NaN marks a
 // non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.

@@ -307,6 +307,89 @@ cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, i
     return cudaGetLastError();
 }
 
+// The same product over row groups: consecutive original rows grp[g] ..
+// grp[g+1]-1 (at most kSpmmGroup) share one column pattern, as the DOFs of
+// one mesh node do, so every gathered column of Qt (m doubles from L2) feeds
+// all rows of the group.  One CTA per group, thread t owns columns
+// j0 + t + 256 u (u < U).
+template <int U>
+__global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict__ rp,
+                                                       const int32_t* __restrict__ ci,
+                                                       const double* __restrict__ v, int64_t ngrp,
+                                                       const int64_t* __restrict__ grp,
+                                                       const int64_t* __restrict__ inv,
+                                                       const double* __restrict__ Qt, int m,
+                                                       double* __restrict__ Rt) {
+    constexpr int kStage = 256;
+    __shared__ double sv[kSpmmGroup][kStage];
+    __shared__ int64_t sc[kStage];
+    for (int64_t g = blockIdx.x; g < ngrp; g += gridDim.x) {
+        const int64_t o0 = grp[g];
+        const int G = (int)(grp[g + 1] - o0);
+        const int64_t cnt = rp[o0 + 1] - rp[o0];
+        for (int j0 = 0; j0 < m; j0 += 256 * U) {
+            double acc[kSpmmGroup][U];
+#pragma unroll
+            for (int r = 0; r < kSpmmGroup; ++r)
+#pragma unroll
+                for (int u = 0; u < U; ++u) acc[r][u] = 0.0;
+            for (int64_t eb = 0; eb < cnt; eb += kStage) {
+                const int c = (int)((cnt - eb) < kStage ? (cnt - eb) : kStage);
+                __syncthreads();
+                for (int t = threadIdx.x; t < c; t += blockDim.x) {
+                    sc[t] = inv[ci[rp[o0] + eb + t]] * (int64_t)m;
+                    for (int r = 0; r < G; ++r) sv[r][t] = v[rp[o0 + r] + eb + t];
+                }
+                __syncthreads();
+#pragma unroll 2
+                for (int t = 0; t < c; ++t) {
+                    const double* q = Qt + sc[t];
+                    double x[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int j = j0 + threadIdx.x + 256 * u;
+                        x[u] = j < m ? q[j] : 0.0;
+                    }
+#pragma unroll
+                    for (int r = 0; r < kSpmmGroup; ++r)
+                        if (r < G) {
+                            const double a = sv[r][t];
+#pragma unroll
+                            for (int u = 0; u < U; ++u) acc[r][u] = fma(a, x[u], acc[r][u]);
+                        }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kSpmmGroup; ++r)
+                if (r < G) {
+                    double* out = Rt + inv[o0 + r] * (int64_t)m;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int j = j0 + threadIdx.x + 256 * u;
+                        if (j < m) out[j] = acc[r][u];
+                    }
+                }
+        }
+    }
+}
+
+cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
+                             const int64_t* grp, const int64_t* inv, const double* Qt, int m,
+                             double* Rt, cudaStream_t s) {
+    if (ngrp <= 0 || m <= 0) return cudaSuccess;
+    const int grid = gridFor(ngrp * 256, 256);
+    const int u = (m + 255) / 256;
+    if (u <= 1)
+        spmmGroupKernel<1><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+    else if (u == 2)
+        spmmGroupKernel<2><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+    else if (u == 3)
+        spmmGroupKernel<3><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+    else
+        spmmGroupKernel<4><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+    return cudaGetLastError();
+}
+
 // out = a*x + b*y (+ c*z when z is given), elementwise
 __global__ void axpby3Kernel(int64_t n, double a, const double* __restrict__ x, double b,
                              const double* __restrict__ y, double c, const double* __restrict__ z,

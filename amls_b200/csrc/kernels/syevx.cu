@@ -133,18 +133,26 @@ struct LargeArgs {
     const int* groupOf;       // CTA -> group (matrix)
     const int* groupFirst;    // first CTA of each group
     const int* groupSize;     // CTAs in each group
-    double* pbuf;             // per matrix 2 n doubles of p accumulators (offsets 2 * pOff)
+    double* pbuf;             // per matrix kTridiagPBufs * n doubles (offsets kTridiagPBufs * pOff)
     const int64_t* pOff;
     int maxN;
 };
 
-__global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
-    // Work per column step is split into units (column j of the trailing
-    // matrix, 256-row segment) handed out over all warps of the group: the
-    // symmetric mat-vec p = tau A22 v accumulates per-unit partial dot
-    // products into p with atomics (p double-buffered by step parity and
-    // cleared one step ahead), and the rank-2 update walks the same units.
-    extern __shared__ double sv[];   // v (maxN), then w (maxN)
+// One grid barrier per column.  Entering step k every CTA of the group holds
+// the reflector v_k (tau_k) in shared memory and p_k = tau_k A22 v_k is
+// complete in global memory (A22 = the trailing matrix before step k's
+// rank-2 update).  Each CTA then forms, redundantly and in the same order
+// (so all CTAs agree bit for bit),
+//   w_k = p_k - tau_k/2 (p_k . v_k) v_k,
+//   the updated first column of A22 and from it the next reflector v_{k+1};
+// after which units (column j, 256-row segment) of the next trailing matrix
+// are updated in place (A -= v w^T + w v^T) and dotted with v_{k+1} in the
+// same pass, accumulating p_{k+1} with atomics.  The trailing matrix is thus
+// read and written once per column.  Three rotating p accumulators: step k
+// reads p_k, adds into p_{k+1} and clears the buffer of p_{k+2}.  Output as
+// the one-CTA kernel: d, e, tau and the reflectors below the subdiagonal.
+__global__ void __launch_bounds__(kTridiagLargeThreads) tridiagLargeKernel(LargeArgs a) {
+    extern __shared__ double sm[];   // vA (maxN), vB (maxN), w (maxN)
     __shared__ double red[32];
     constexpr int SEG = 256;
     cg::grid_group grid = cg::this_grid();
@@ -155,79 +163,135 @@ __global__ void __launch_bounds__(256) tridiagLargeKernel(LargeArgs a) {
     const int n = D.n;
     double* A = D.A;
     const int64_t lda = D.lda;
-    double* pb[2] = {a.pbuf + 2 * a.pOff[g], a.pbuf + 2 * a.pOff[g] + n};
-    double* sw = sv + a.maxN;
+    double* pbase = a.pbuf + (int64_t)kTridiagPBufs * a.pOff[g];
+    double* vcur = sm;
+    double* vnext = sm + a.maxN;
+    double* sw = sm + 2 * a.maxN;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int bd = blockDim.x;
     const int gw = rank * nw + wid, GW = gsize * nw;
-    const int gt = rank * blockDim.x + tid, GT = gsize * blockDim.x;
-    // p buffers start cleared
-    for (int i = gt; i < 2 * n; i += GT) a.pbuf[2 * a.pOff[g] + i] = 0.0;
+    const int gt = rank * bd + tid, GT = gsize * bd;
+
+    // accumulators cleared; reflector v_0 from column 0
+    for (int i = gt; i < kTridiagPBufs * n; i += GT) pbase[i] = 0.0;
+    HouseholderScalars h{0.0, 0.0, 0.0};
+    if (n >= 3) {
+        const int m = n - 1;
+        const double* col = A + 1;
+        double part = 0.0;
+        for (int i = 1 + tid; i < m; i += bd) part += col[i] * col[i];
+        h = makeReflector(col[0], blockSum(part, red));
+        for (int i = tid; i < m; i += bd) vcur[i] = (i == 0) ? 1.0 : col[i] * h.scale;
+    }
+    grid.sync();
+    // p_0 = tau_0 A22 v_0
+    if (n >= 3 && h.tau != 0.0) {
+        const int m = n - 1, segs = (m + SEG - 1) / SEG;
+        const double* A22 = A + 1 + lda;
+        for (int u = gw; u < m * segs; u += GW) {
+            const int j = u / segs, s0 = (u % segs) * SEG;
+            const int s1 = min(m, s0 + SEG);
+            const double* cj = A22 + (int64_t)j * lda;
+            double sum = 0.0;
+#pragma unroll 4
+            for (int i = s0 + lane; i < s1; i += 32) sum += cj[i] * vcur[i];
+            sum = warpSum<32>(sum);
+            if (lane == 0) atomicAdd(pbase + j, h.tau * sum);
+        }
+    }
     grid.sync();
     for (int k = 0; k + 2 < a.maxN; ++k) {
-        const bool active = k + 2 < n;
-        const int m = n - k - 1;
-        const int segs = (m + SEG - 1) / SEG;
-        double* col = A + (k + 1) + (int64_t)k * lda;
-        double* p = pb[k & 1];
-        HouseholderScalars h{0.0, 0.0, 0.0};
-        if (active) {
-            double part = 0.0;
-            for (int i = 1 + tid; i < m; i += blockDim.x) part += col[i] * col[i];
-            const double xnorm2 = blockSum(part, red);
-            h = makeReflector(col[0], xnorm2);
-            for (int i = tid; i < m; i += blockDim.x) sv[i] = (i == 0) ? 1.0 : col[i] * h.scale;
+        if (k + 2 < n) {
+            const int m = n - k - 1;        // order of the trailing matrix B = A22
+            const int m1 = m - 1;           // order of the next one, C = B(1:, 1:)
+            const double* p = pbase + (int64_t)(k % kTridiagPBufs) * n;
+            double* B = A + (k + 1) + (int64_t)(k + 1) * lda;
+            // w = p - tau/2 (p . v) v
+            double pv = 0.0;
+            for (int i = tid; i < m; i += bd) pv += p[i] * vcur[i];
+            pv = blockSum(pv, red);
+            const double a2 = -0.5 * h.tau * pv;
+            for (int i = tid; i < m; i += bd) sw[i] = p[i] + a2 * vcur[i];
             __syncthreads();
-            if (h.tau != 0.0) {
-                const double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
-                for (int u = gw; u < m * segs; u += GW) {
-                    const int j = u / segs, s0 = (u % segs) * SEG;
-                    const int s1 = min(m, s0 + SEG);
-                    const double* cj = A22 + (int64_t)j * lda;
-                    double sum = 0.0;
-                    for (int i = s0 + lane; i < s1; i += 32) sum += cj[i] * sv[i];
-                    sum = warpSum<32>(sum);
-                    if (lane == 0) atomicAdd(p + j, h.tau * sum);
+            // updated first column of B, b0 = B(:,0) - v w0 - w v0 (v0 = 1);
+            // the next reflector is built from b0(1:)
+            const double w0 = sw[0], v0 = vcur[0];
+            const double b00 = B[0] - (v0 * w0 + w0 * v0);
+            const double alpha = B[1] - (vcur[1] * w0 + sw[1] * v0);
+            HouseholderScalars hn{0.0, 0.0, 0.0};
+            if (m1 >= 2) {
+                double part = 0.0;
+                for (int i = 2 + tid; i < m; i += bd) {
+                    const double b = B[i] - (vcur[i] * w0 + sw[i] * v0);
+                    vnext[i - 1] = b;
+                    part += b * b;
                 }
-            }
-        }
-        grid.sync();
-        if (active) {
-            double* pn = pb[(k + 1) & 1];
-            for (int i = gt; i < m; i += GT) pn[i] = 0.0;     // next step's accumulator
-            if (h.tau != 0.0) {
-                double pv = 0.0;
-                for (int i = tid; i < m; i += blockDim.x) pv += p[i] * sv[i];
-                pv = blockSum(pv, red);
-                const double a2 = -0.5 * h.tau * pv;
-                for (int i = tid; i < m; i += blockDim.x) sw[i] = p[i] + a2 * sv[i];
+                hn = makeReflector(alpha, blockSum(part, red));
+                for (int i = 1 + tid; i < m1; i += bd) vnext[i] *= hn.scale;
+                if (tid == 0) vnext[0] = 1.0;
                 __syncthreads();
-                double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
-                for (int u = gw; u < m * segs; u += GW) {
-                    const int j = u / segs, s0 = (u % segs) * SEG;
-                    const int s1 = min(m, s0 + SEG);
-                    double* cj = A22 + (int64_t)j * lda;
-                    const double vj = sv[j], wj = sw[j];
-                    for (int i = s0 + lane; i < s1; i += 32) cj[i] -= sv[i] * wj + sw[i] * vj;
-                }
             }
             if (rank == 0) {
-                for (int i = tid; i < m; i += blockDim.x) col[i] = sv[i];
+                // reflector k into column k; nothing else reads that column now
+                double* col = A + (k + 1) + (int64_t)k * lda;
+                for (int i = tid; i < m; i += bd) col[i] = vcur[i];
                 if (tid == 0) {
-                    D.d[k] = A[k + (int64_t)k * lda];
+                    if (k == 0) D.d[0] = A[0];
                     D.e[k] = h.beta;
                     D.tau[k] = h.tau;
+                    D.d[k + 1] = b00;
+                    if (m1 < 2) {           // last column step: the 2 x 2 tail
+                        D.e[k + 1] = alpha;
+                        D.tau[k + 1] = 0.0;
+                        D.d[k + 2] = B[1 + lda] - (vcur[1] * sw[1] + sw[1] * vcur[1]);
+                    }
                 }
             }
+            if (m1 >= 2) {
+                const int segs = (m1 + SEG - 1) / SEG;
+                double* C = B + 1 + lda;
+                const double* vp = vcur + 1;
+                const double* wp = sw + 1;
+                double* pn = pbase + (int64_t)((k + 1) % kTridiagPBufs) * n;
+                const bool upd = h.tau != 0.0;
+                for (int u = gw; u < m1 * segs; u += GW) {
+                    const int j = u / segs, s0 = (u % segs) * SEG;
+                    const int s1 = min(m1, s0 + SEG);
+                    double* cj = C + (int64_t)j * lda;
+                    const double vj = vp[j], wj = wp[j];
+                    double sum = 0.0;
+                    if (upd) {
+#pragma unroll 4
+                        for (int i = s0 + lane; i < s1; i += 32) {
+                            const double c = cj[i] - (vp[i] * wj + wp[i] * vj);
+                            cj[i] = c;
+                            sum += c * vnext[i];
+                        }
+                    } else {
+#pragma unroll 4
+                        for (int i = s0 + lane; i < s1; i += 32) sum += cj[i] * vnext[i];
+                    }
+                    sum = warpSum<32>(sum);
+                    if (lane == 0 && hn.tau != 0.0) atomicAdd(pn + j, hn.tau * sum);
+                }
+            }
+            // the accumulator of step k+2 (last read at step k-1)
+            double* pc = pbase + (int64_t)((k + 2) % kTridiagPBufs) * n;
+            for (int i = gt; i < n; i += GT) pc[i] = 0.0;
+            h = hn;
+            double* t = vcur;
+            vcur = vnext;
+            vnext = t;
         }
         grid.sync();
     }
-    if (rank == 0 && tid == 0) {
-        if (n >= 2) {
-            D.d[n - 2] = A[(n - 2) + (int64_t)(n - 2) * lda];
-            D.e[n - 2] = A[(n - 1) + (int64_t)(n - 2) * lda];
-            D.tau[n - 2] = 0.0;
+    if (rank == 0 && tid == 0 && n <= 2) {
+        D.d[0] = A[0];
+        if (n == 2) {
+            D.e[0] = A[1];
+            D.tau[0] = 0.0;
+            D.d[1] = A[1 + lda];
         }
-        if (n >= 1) D.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda];
     }
 }
 
@@ -236,24 +300,25 @@ cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
                                      double* dP, const int64_t* dPOff, int maxN, cudaStream_t s) {
     LargeArgs a{dDescs, dGroupOf, dGroupFirst, dGroupSize, dP, dPOff, maxN};
     void* args[] = {&a};
-    const size_t smem = 2 * (size_t)maxN * sizeof(double);
+    const size_t smem = 3 * (size_t)maxN * sizeof(double);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(tridiagLargeKernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    return cudaLaunchCooperativeKernel((void*)tridiagLargeKernel, dim3(nCta), dim3(256), args, smem, s);
+    return cudaLaunchCooperativeKernel((void*)tridiagLargeKernel, dim3(nCta),
+                                       dim3(kTridiagLargeThreads), args, smem, s);
 }
 
 int tridiagLargeMaxCtas(int maxN) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = 2 * (size_t)maxN * sizeof(double);
+    const size_t smem = 3 * (size_t)maxN * sizeof(double);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(tridiagLargeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiagLargeKernel, 256, smem);
-    if (per > 4) per = 4;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiagLargeKernel, kTridiagLargeThreads, smem);
+    if (per > 1) per = 1;
     return per * sms;
 }
 

@@ -42,6 +42,19 @@ def test_sygvx_index_matches_lapack(solver, n):
     assert res.max() < 1e-12
 
 
+def test_sygvx_many_large_in_chunks(solver):
+    """More matrices above the one-CTA size than SMs: the cooperative
+    tridiagonalisation runs in several launches; plus one matrix of order
+    1,500 sharing a launch with smaller ones."""
+    rng = np.random.default_rng(11)
+    sizes = [390 + (i % 7) for i in range(150)] + [1500]
+    Ks, Ms = zip(*[_rand_pencil(n, rng) for n in sizes])
+    out = sygvx_batched(solver, list(Ks), list(Ms), mode="index", il=1, iu=3)
+    for b in list(range(0, 150, 37)) + [149, 150]:
+        wr, _ = R.LapackDense.solve_index(Ks[b], Ms[b], 1, 3)
+        assert rel_err(out[b][0], wr) < 1e-12
+
+
 def test_sygvx_interval_batched_uneven(solver):
     rng = np.random.default_rng(5)
     sizes = [3, 17, 64, 150, 420]
