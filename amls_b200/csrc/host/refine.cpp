@@ -27,7 +27,7 @@ namespace amls_b200 {
 
 namespace {
 constexpr int kT = kGemmTile;
-constexpr int kTB = kGemmTileBig;
+constexpr int kTB = kGemmTile;
 int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 }  // namespace
 
@@ -344,13 +344,13 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
-            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
         }
         for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
-            LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
         }
         catF_[2] += fsolve;
     };
@@ -389,7 +389,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         spmm(X, MX);
         cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
         cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
-        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
         LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
         denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
         std::vector<double> th(static_cast<size_t>(nq));
@@ -418,7 +418,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e\n", it + 1, est);
         const bool last = est <= opt_.refineTol || it + 1 >= std::max(1, opt_.refineMaxIter);
         // Q = Vc^T X, and M Q for the next iteration unless this is the last
-        LAUNCH(launchGemmBatchedBig(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
                                     last ? nUp1 : static_cast<int>(upT.size()), s));
         catF_[2] += (last ? 1.0 : 2.0) * 2.0 * dn * dq * dq;
         catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;

@@ -1,12 +1,14 @@
 // Batched FP64 GEMM with gather/scatter epilogues, and the front extend-add
 // update (SYRK + SYR2K of the eliminated front, scattered into ancestors).
 //
-// B200 has no FP64 tcgen05 kind; FP64 runs on the DFMA pipe, so these are
-// register-tiled CUDA-core kernels: 64x64 output tile per CTA, 256 threads,
-// 4x4 accumulators per thread, K staged through shared memory in slices of
-// 16 with register prefetch of the next slice (one barrier per slice).
-// Thread (tx, ty) owns rows tx + 16*i and columns ty + 16*j so that the
-// epilogue stores of a warp are contiguous in a column.
+// B200 has no FP64 tcgen05 kind; its FP64 tensor-core path is the warp-level
+// DMMA (mma.sync .f64), which these kernels use: 64 x 64 output tile per CTA,
+// 8 warps as 2 (M) x 4 (N), warp tile 32 x 16 = 2 x 2 fragments of
+// m16n8k16, operands streamed global -> shared memory with cp.async through a
+// three-deep ring of K slices of 16 (one barrier per slice, no register
+// staging).  The operand layout (transposed A / B, gathered A columns) is a
+// template parameter selected per CTA from the descriptor, so the copy loops
+// carry no per-element branches.
 #include "common.cuh"
 #include "launch.hpp"
 
@@ -16,175 +18,189 @@ namespace {
 constexpr int NT = 256;
 constexpr int TM = 64, TN = 64, TK = 16;   // tiles of the front-update kernel
 
-// Register-tiled batched GEMM: tile (16*RM) x (16*RN), K slice KS, thread
-// (tx, ty) owns rows tx + 16*i and columns ty + 16*j.
-template <int RM, int RN, int KS>
-struct GemmTile {
-    static constexpr int BM = 16 * RM, BN = 16 * RN;
-    static constexpr int LA = BM * KS / NT, LB = BN * KS / NT;   // loads per thread
+constexpr int kBM = kGemmTile, kBN = kGemmTile;   // 64 x 64
+constexpr int kKs = 16;                            // K slice
+constexpr int kStages = 3;
+constexpr int kLdA = kBM + 4, kLdB = kBN + 4;      // = 4 mod 16 doubles
+constexpr int kStage = kKs * (kLdA + kLdB);        // doubles per stage
+constexpr size_t kGemmSmem = sizeof(double) * kStages * kStage;
+constexpr int kLA = kBM * kKs / NT, kLB = kBN * kKs / NT;
 
-    __device__ static void loadA(const GemmDesc& D, int m0, int k0, int kEnd, double (&r)[LA]) {
-#pragma unroll
-        for (int u = 0; u < LA; ++u) {
-            const int idx = threadIdx.x + NT * u;
-            int i, k;
-            if (D.flags & kTransA) { k = idx % KS; i = idx / KS; }
-            else { i = idx % BM; k = idx / BM; }
-            const int gi = m0 + i, gk = k0 + k;
-            double v = 0.0;
-            if (gi < D.M && gk < kEnd) {
-                if (D.flags & kTransA) v = D.A[gk + (int64_t)gi * D.lda];
-                else if (D.flags & kGatherA) v = D.A[gi + (int64_t)D.aMap[gk] * D.lda];
-                else v = D.A[gi + (int64_t)gk * D.lda];
-            }
-            r[u] = v;
-        }
-    }
-    __device__ static void storeA(const GemmDesc& D, const double (&r)[LA], double (*As)[BM + 2]) {
-#pragma unroll
-        for (int u = 0; u < LA; ++u) {
-            const int idx = threadIdx.x + NT * u;
-            int i, k;
-            if (D.flags & kTransA) { k = idx % KS; i = idx / KS; }
-            else { i = idx % BM; k = idx / BM; }
-            As[k][i] = r[u];
-        }
-    }
-    __device__ static void loadB(const GemmDesc& D, int n0, int k0, int kEnd, double (&r)[LB]) {
-#pragma unroll
-        for (int u = 0; u < LB; ++u) {
-            const int idx = threadIdx.x + NT * u;
-            int j, k;
-            if (D.flags & kTransB) { j = idx % BN; k = idx / BN; }
-            else { k = idx % KS; j = idx / KS; }
-            const int gj = n0 + j, gk = k0 + k;
-            double v = 0.0;
-            if (gj < D.N && gk < kEnd) {
-                if (D.flags & kTransB) v = D.B[gj + (int64_t)gk * D.ldb];
-                else v = D.B[gk + (int64_t)gj * D.ldb];
-            }
-            r[u] = v;
-        }
-    }
-    __device__ static void storeB(const GemmDesc& D, const double (&r)[LB], double (*Bs)[BN + 2]) {
-#pragma unroll
-        for (int u = 0; u < LB; ++u) {
-            const int idx = threadIdx.x + NT * u;
-            int j, k;
-            if (D.flags & kTransB) { j = idx % BN; k = idx / BN; }
-            else { k = idx % KS; j = idx / KS; }
-            Bs[k][j] = r[u];
-        }
-    }
-};
+__device__ __forceinline__ void dmma16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+        "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+          "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
 
-template <int RM, int RN, int KS>
-__device__ __forceinline__ void gemmTileBody(const GemmDesc* __restrict__ descs,
-                                             const TileRef* __restrict__ tiles) {
-    using G = GemmTile<RM, RN, KS>;
-    __shared__ double As[2][KS][G::BM + 2];
-    __shared__ double Bs[2][KS][G::BN + 2];
-    const TileRef t = tiles[blockIdx.x];
-    const GemmDesc D = descs[t.desc];
+// 8-byte asynchronous copy; src_size 0 writes zeros and reads nothing
+__device__ __forceinline__ void cpAsync8(double* dst, const double* src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+// one K slice of op(A) (kBM x kKs) and op(B) (kKs x kBN) into shared memory,
+// stored k-major: As[k][i], Bs[k][j]; global reads coalesced on the
+// contiguous side of each layout
+template <bool TA, bool TB, bool GA>
+__device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, int k0, int kEnd,
+                                           double* As, double* Bs) {
+#pragma unroll
+    for (int u = 0; u < kLA; ++u) {
+        const int idx = threadIdx.x + NT * u;
+        const int i = TA ? idx / kKs : idx % kBM;
+        const int k = TA ? idx % kKs : idx / kBM;
+        const int gi = m0 + i, gk = k0 + k;
+        const bool ok = gi < D.M && gk < kEnd;
+        const double* src = D.A;
+        if (ok) {
+            if (TA) src = D.A + gk + (int64_t)gi * D.lda;
+            else if (GA) src = D.A + gi + (int64_t)D.aMap[gk] * D.lda;
+            else src = D.A + gi + (int64_t)gk * D.lda;
+        }
+        cpAsync8(As + k * kLdA + i, src, ok);
+    }
+#pragma unroll
+    for (int u = 0; u < kLB; ++u) {
+        const int idx = threadIdx.x + NT * u;
+        const int j = TB ? idx % kBN : idx / kKs;
+        const int k = TB ? idx / kBN : idx % kKs;
+        const int gj = n0 + j, gk = k0 + k;
+        const bool ok = gj < D.N && gk < kEnd;
+        const double* src = D.B;
+        if (ok) src = TB ? D.B + gj + (int64_t)gk * D.ldb : D.B + gk + (int64_t)gj * D.ldb;
+        cpAsync8(Bs + k * kLdB + j, src, ok);
+    }
+}
+
+template <bool TA, bool TB, bool GA>
+__device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, double* sm) {
     const int m0 = t.m0, n0 = t.n0;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[RM][RN];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double acc[2][2][4];
 #pragma unroll
-    for (int i = 0; i < RM; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < RN; ++j) acc[i][j] = 0.0;
-    // split-K: this CTA covers k in [kBeg, kEnd) (the whole K when kChunk = 0);
-    // triangular B: only k <= last column of the tile (kTriKUpTo) or
-    // k >= first column of the tile (kTriKFrom) contribute
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+    // split-K range; triangular B restricts k to <= the tile's last column
+    // (kTriKUpTo) or >= its first column (kTriKFrom)
     int kBeg = D.kChunk > 0 ? t.pad * D.kChunk : 0;
     int kEnd = D.kChunk > 0 ? min(D.K, kBeg + D.kChunk) : D.K;
-    if (D.flags & kTriKUpTo) kEnd = min(kEnd, n0 + G::BN);
+    if (D.flags & kTriKUpTo) kEnd = min(kEnd, n0 + kBN);
     if (D.flags & kTriKFrom) kBeg = max(kBeg, n0);
-    double ra[G::LA], rb[G::LB];
-    int cur = 0;
-    if (kEnd > kBeg) {
-        G::loadA(D, m0, kBeg, kEnd, ra);
-        G::loadB(D, n0, kBeg, kEnd, rb);
-        G::storeA(D, ra, As[0]);
-        G::storeB(D, rb, Bs[0]);
+    const int nSlices = kEnd > kBeg ? (kEnd - kBeg + kKs - 1) / kKs : 0;
+#pragma unroll
+    for (int st = 0; st < kStages - 1; ++st) {
+        if (st < nSlices) {
+            double* base = sm + st * kStage;
+            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + st * kKs, kEnd, base, base + kKs * kLdA);
+        }
+        cpAsyncCommit();
     }
-    __syncthreads();
-    for (int k0 = kBeg; k0 < kEnd; k0 += KS) {
-        const bool more = k0 + KS < kEnd;
-        if (more) {
-            G::loadA(D, m0, k0 + KS, kEnd, ra);
-            G::loadB(D, n0, k0 + KS, kEnd, rb);
-        }
-#pragma unroll
-        for (int kk = 0; kk < KS; ++kk) {
-            double a[RM], b[RN];
-#pragma unroll
-            for (int i = 0; i < RM; ++i) a[i] = As[cur][kk][tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < RN; ++j) b[j] = Bs[cur][kk][ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < RM; ++i)
-#pragma unroll
-                for (int j = 0; j < RN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        if (more) {
-            G::storeA(D, ra, As[cur ^ 1]);
-            G::storeB(D, rb, Bs[cur ^ 1]);
-        }
+    for (int sl = 0; sl < nSlices; ++sl) {
+        cpAsyncWait<kStages - 2>();
         __syncthreads();
-        cur ^= 1;
-    }
-    // epilogue
+        const int nx = sl + kStages - 1;
+        if (nx < nSlices) {
+            double* base = sm + (nx % kStages) * kStage;
+            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + nx * kKs, kEnd, base, base + kKs * kLdA);
+        }
+        cpAsyncCommit();
+        const double* As = sm + (sl % kStages) * kStage;
+        const double* Bs = As + kKs * kLdA;
+        // fragments: A element (row g (+8), k tg + 4 q), B element (k tg + 4 q, col g)
+        double a[2][8], b[2][4];
 #pragma unroll
-    for (int j = 0; j < RN; ++j) {
-        const int col = n0 + ty + 16 * j;
-        if (col >= D.N) continue;
-        const double cs = (D.flags & kColScale) ? D.colScale[col] : 1.0;
+        for (int i = 0; i < 2; ++i) {
+            const int r = wm + 16 * i + g;
 #pragma unroll
-        for (int i = 0; i < RM; ++i) {
-            const int row = m0 + tx + 16 * i;
-            if (row >= D.M) continue;
-            double v = D.alpha * acc[i][j] * cs;
-            if (D.flags & kRowScale) v *= D.rowScale[row];
-            if (D.flags & kScatter) {
-                double* dst = D.C + D.colOff[col] + D.rowIdx[row];
-                if (D.flags & kAtomic) atomicAdd(dst, v);
-                else if (D.flags & kAccumulate) *dst += v;
-                else *dst = v;
-            } else {
-                double* dst = D.C + row + (int64_t)col * D.ldc;
-                if (D.kChunk > 0) atomicAdd(dst, v);   // split-K partial (C pre-zeroed)
-                else if (D.flags & kAccumulate) *dst = v + D.beta * (*dst);
-                else *dst = v;
+            for (int q = 0; q < 4; ++q) {
+                a[i][2 * q] = As[(tg + 4 * q) * kLdA + r];
+                a[i][2 * q + 1] = As[(tg + 4 * q) * kLdA + r + 8];
             }
         }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int c = wn + 8 * j + g;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[j][q] = Bs[(tg + 4 * q) * kLdB + c];
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
     }
+    cpAsyncWait<0>();
+    // epilogue: fragment (i, j) element q sits at row wm + 16 i + g + 8 (q / 2),
+    // column wn + 8 j + 2 tg + (q % 2)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int q2 = 0; q2 < 2; ++q2) {
+            const int col = n0 + wn + 8 * j + 2 * tg + q2;
+            if (col >= D.N) continue;
+            const double cs = (D.flags & kColScale) ? D.colScale[col] : 1.0;
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int row = m0 + wm + 16 * i + g + 8 * h;
+                    if (row >= D.M) continue;
+                    double v = D.alpha * acc[i][j][2 * h + q2] * cs;
+                    if (D.flags & kRowScale) v *= D.rowScale[row];
+                    if (D.flags & kScatter) {
+                        double* dst = D.C + D.colOff[col] + D.rowIdx[row];
+                        if (D.flags & kAtomic) atomicAdd(dst, v);
+                        else if (D.flags & kAccumulate) *dst += v;
+                        else *dst = v;
+                    } else {
+                        double* dst = D.C + row + (int64_t)col * D.ldc;
+                        if (D.kChunk > 0) atomicAdd(dst, v);   // split-K partial (C pre-zeroed)
+                        else if (D.flags & kAccumulate) *dst = v + D.beta * (*dst);
+                        else *dst = v;
+                    }
+                }
+        }
 }
 }  // namespace
 
 __global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restrict__ descs,
                                                         const TileRef* __restrict__ tiles) {
-    gemmTileBody<4, 4, 16>(descs, tiles);
-}
-
-// 128 x 128 tiles, 8 x 8 accumulators per thread: twice the FMAs per shared
-// memory load of the 64 x 64 variant, for the large products.
-__global__ void __launch_bounds__(NT, 1) gemmBatchedBigKernel(const GemmDesc* __restrict__ descs,
-                                                              const TileRef* __restrict__ tiles) {
-    gemmTileBody<8, 8, 8>(descs, tiles);
-}
-
-cudaError_t launchGemmBatchedBig(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
-                                 cudaStream_t s) {
-    if (nTiles <= 0) return cudaSuccess;
-    gemmBatchedBigKernel<<<nTiles, NT, 0, s>>>(dDescs, dTiles);
-    return cudaGetLastError();
+    extern __shared__ double gemmSmem[];
+    const TileRef t = tiles[blockIdx.x];
+    const GemmDesc D = descs[t.desc];
+    const bool ta = D.flags & kTransA, tb = D.flags & kTransB, ga = D.flags & kGatherA;
+    if (ga) {
+        if (tb) gemmTile<false, true, true>(D, t, gemmSmem);
+        else gemmTile<false, false, true>(D, t, gemmSmem);
+    } else if (ta) {
+        if (tb) gemmTile<true, true, false>(D, t, gemmSmem);
+        else gemmTile<true, false, false>(D, t, gemmSmem);
+    } else {
+        if (tb) gemmTile<false, true, false>(D, t, gemmSmem);
+        else gemmTile<false, false, false>(D, t, gemmSmem);
+    }
 }
 
 cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
                               cudaStream_t s) {
     if (nTiles <= 0) return cudaSuccess;
-    gemmBatchedKernel<<<nTiles, NT, 0, s>>>(dDescs, dTiles);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(gemmBatchedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kGemmSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    gemmBatchedKernel<<<nTiles, NT, kGemmSmem, s>>>(dDescs, dTiles);
     return cudaGetLastError();
 }
 

@@ -52,15 +52,12 @@ struct TileRef {
     int32_t desc, m0, n0, pad;
 };
 
-// Tile size of the batched GEMM (host builds TileRef tables with it).
+// Tile size of the batched GEMM (host builds TileRef tables with it).  One
+// descriptor table per launch may mix layouts (kTransA / kTransB / kGatherA).
 constexpr int kGemmTile = 64;
 
 cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
                               cudaStream_t s);
-// Same operation with 128 x 128 tiles (TileRef m0/n0 multiples of 128).
-constexpr int kGemmTileBig = 128;
-cudaError_t launchGemmBatchedBig(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
-                                 cudaStream_t s);
 
 // Extend-add update of one eliminated front (multifrontal form of the
 // reference's Schur + congruence updates):
