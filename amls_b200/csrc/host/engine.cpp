@@ -194,7 +194,9 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     nnzK_ = kp[n];
     nnzM_ = mp[n];
 
+    const Clock::time_point ta0 = Clock::now();
     PartitionResult pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize);
+    const Clock::time_point ta1 = Clock::now();
     perm_ = pr.perm;
     inv_.assign(static_cast<size_t>(n), 0);
     for (int64_t j = 0; j < n; ++j) inv_[static_cast<size_t>(perm_[static_cast<size_t>(j)])] = j;
@@ -331,8 +333,10 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
         }
     };
     rowsDst = rowsDstBody;
+    const Clock::time_point ta2 = Clock::now();
     dstMap(kp, kc, hostKDst_);
     dstMap(mp, mc, hostMDst_);
+    const Clock::time_point ta3 = Clock::now();
 
     // device: original M pattern (for the M-norms), maps
     mRp_.ensure(sizeof(int64_t) * static_cast<size_t>(n + 1));
@@ -377,9 +381,15 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     ePool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     tauPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     invPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(invTotal_, 1)));
+    const Clock::time_point ta4 = Clock::now();
     buildStatic();
     cudaCheck(cudaStreamSynchronize(stream_), "analyze");
     analyzed_ = true;
+    if (opt_.verbosity >= 2)
+        std::fprintf(stderr,
+                     "[amls_b200] analyze: partition %.3f s, symbolic + layout %.3f s, CSR maps %.3f s, "
+                     "uploads %.3f s, launch tables %.3f s\n",
+                     secs(ta0, ta1), secs(ta1, ta2), secs(ta2, ta3), secs(ta3, ta4), secs(ta4, Clock::now()));
 }
 
 void Engine::buildStatic() {

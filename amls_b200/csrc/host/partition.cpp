@@ -17,7 +17,10 @@
 #include "tree.hpp"
 
 #include <algorithm>
+#include <exception>
 #include <functional>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <numeric>
 #include <stdexcept>
@@ -36,6 +39,7 @@ namespace {
 constexpr int kMetisOk = 1;
 constexpr int kMetisNOptions = 40;
 constexpr int kMetisOptionSeed = 8;
+std::mutex gMetisMutex;   // METIS keeps process-wide state: one call at a time
 
 struct Csr {
     std::vector<int64_t> xadj, adjncy;
@@ -134,9 +138,13 @@ std::vector<int64_t> bisect(Csr g) {
     METIS_SetDefaultOptions(opts);
     opts[kMetisOptionSeed] = 42;
     int64_t sepsize = 0;
-    if (METIS_ComputeVertexSeparator(&nvtxs, g.xadj.data(), g.adjncy.data(), nullptr, opts,
-                                     &sepsize, part.data()) != kMetisOk)
-        throw std::runtime_error("METIS_ComputeVertexSeparator failed");
+    int rc;
+    {
+        std::lock_guard<std::mutex> lock(gMetisMutex);
+        rc = METIS_ComputeVertexSeparator(&nvtxs, g.xadj.data(), g.adjncy.data(), nullptr, opts,
+                                          &sepsize, part.data());
+    }
+    if (rc != kMetisOk) throw std::runtime_error("METIS_ComputeVertexSeparator failed");
     return part;
 }
 }  // namespace
@@ -200,40 +208,94 @@ bool SeparatorTree::validate(int64_t nTotal) const {
     return true;
 }
 
+namespace {
+// Result of the recursive bisection of one vertex set, built before any tree
+// node is created so the two halves can run concurrently.
+struct Split {
+    std::vector<int64_t> verts;               // leaf: its vertices
+    std::vector<int64_t> sep;                 // separator (empty for a leaf)
+    std::unique_ptr<Split> left, right;
+};
+
+// The top kParallelDepth levels run their two halves on two threads.  The
+// METIS library keeps process-wide state (its random generator), so its calls
+// are serialised by a mutex: concurrent calls give different separators,
+// while every call re-seeds from its own options, so the split of each
+// vertex set does not depend on the order of the serialised calls.  What
+// runs concurrently is the induced-subgraph construction and bookkeeping.
+constexpr int kParallelDepth = 3;
+
+std::unique_ptr<Split> splitRec(const Csr& g, std::vector<int64_t> verts, int depth, int nLevels,
+                                int64_t leafSize) {
+    auto out = std::make_unique<Split>();
+    const int64_t m = static_cast<int64_t>(verts.size());
+    if (m <= leafSize || depth >= nLevels || m < 4) {
+        out->verts = std::move(verts);
+        return out;
+    }
+    std::vector<int64_t> localOf;
+    Csr sub = inducedSubgraph(g, verts, localOf);
+    const std::vector<int64_t> part = bisect(std::move(sub));
+    std::vector<int64_t> side[2], sep;
+    for (int64_t i = 0; i < m; ++i) {
+        const int64_t p = part[static_cast<size_t>(i)];
+        if (p == 2) sep.push_back(verts[static_cast<size_t>(i)]);
+        else side[p].push_back(verts[static_cast<size_t>(i)]);
+    }
+    const int64_t minSide = static_cast<int64_t>(std::min(side[0].size(), side[1].size()));
+    if (sep.empty() || minSide < 2) {
+        out->verts = std::move(verts);
+        return out;
+    }
+    out->sep = std::move(sep);
+    if (depth < kParallelDepth) {
+        std::exception_ptr err;
+        std::thread t([&] {
+            try {
+                out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize);
+            } catch (...) {
+                err = std::current_exception();
+            }
+        });
+        try {
+            out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize);
+        } catch (...) {
+            t.join();
+            throw;
+        }
+        t.join();
+        if (err) std::rethrow_exception(err);
+    } else {
+        out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize);
+        out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize);
+    }
+    return out;
+}
+
+// tree nodes in the reference's creation order: separator, then the left
+// subtree, then the right one (metis_partitioner.cpp:110-160)
+int64_t buildTree(SeparatorTree& tree, Split& s) {
+    if (!s.left) return tree.addNode(NodeRole::Leaf, std::move(s.verts));
+    const int64_t sepId = tree.addNode(NodeRole::Separator, std::move(s.sep));
+    const int64_t l = buildTree(tree, *s.left);
+    const int64_t r = buildTree(tree, *s.right);
+    tree.setChildren(sepId, l, r);
+    tree.setParent(l, sepId);
+    tree.setParent(r, sepId);
+    return sepId;
+}
+}  // namespace
+
 PartitionResult recursiveBisection(int64_t n, const int64_t* kRowPtr, const int32_t* kCol,
                                    const int64_t* mRowPtr, const int32_t* mCol, int nLevels,
                                    int64_t leafSize) {
     PartitionResult res;
     if (n == 0) return res;
     const Csr g = extractGraph(n, kRowPtr, kCol, mRowPtr, mCol);
-
-    std::function<int64_t(const std::vector<int64_t>&, int)> recurse =
-        [&](const std::vector<int64_t>& verts, int depth) -> int64_t {
-        const int64_t m = static_cast<int64_t>(verts.size());
-        if (m <= leafSize || depth >= nLevels || m < 4)
-            return res.tree.addNode(NodeRole::Leaf, verts);
-        std::vector<int64_t> localOf;
-        Csr sub = inducedSubgraph(g, verts, localOf);
-        const std::vector<int64_t> part = bisect(std::move(sub));
-        std::vector<int64_t> side[2], sep;
-        for (int64_t i = 0; i < m; ++i) {
-            const int64_t p = part[static_cast<size_t>(i)];
-            if (p == 2) sep.push_back(verts[static_cast<size_t>(i)]);
-            else side[p].push_back(verts[static_cast<size_t>(i)]);
-        }
-        const int64_t minSide = static_cast<int64_t>(std::min(side[0].size(), side[1].size()));
-        if (sep.empty() || minSide < 2) return res.tree.addNode(NodeRole::Leaf, verts);
-        const int64_t sepId = res.tree.addNode(NodeRole::Separator, sep);
-        const int64_t l = recurse(side[0], depth + 1);
-        const int64_t r = recurse(side[1], depth + 1);
-        res.tree.setChildren(sepId, l, r);
-        res.tree.setParent(l, sepId);
-        res.tree.setParent(r, sepId);
-        return sepId;
-    };
     std::vector<int64_t> all(static_cast<size_t>(n));
     std::iota(all.begin(), all.end(), 0);
-    recurse(all, 0);
+    std::unique_ptr<Split> root = splitRec(g, std::move(all), 0, nLevels, leafSize);
+    buildTree(res.tree, *root);
     res.tree.relabelRoot();
     for (int64_t id : res.tree.postOrder()) {
         const auto& idx = res.tree.node(id).indices;
