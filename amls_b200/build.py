@@ -20,6 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libamls_b200.so")
+WORKER = os.path.join(HERE, "amls_metis_worker")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 METIS = os.path.join(CUDA, "targets", "x86_64-linux", "lib", "libmetis_static.a")
 
@@ -57,6 +58,7 @@ def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "**", "*.cu"), recursive=True)
                   + glob.glob(os.path.join(CSRC, "**", "*.cpp"), recursive=True))
+    srcs = [s for s in srcs if os.sep + "worker" + os.sep not in s]
     hm = _headers_mtime()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         results = list(ex.map(lambda s: _compile(s, hm, verbose), srcs))
@@ -73,6 +75,14 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    # the separator worker program (METIS calls of concurrent subtrees)
+    wsrc = os.path.join(CSRC, "worker", "metis_worker.cpp")
+    whdr = os.path.join(CSRC, "host", "metis_call.hpp")
+    if not os.path.exists(WORKER) or os.path.getmtime(WORKER) < max(os.path.getmtime(wsrc), os.path.getmtime(whdr)):
+        cmd = ["g++", *CXX_FLAGS, "-I", CSRC, wsrc, "-o", WORKER, METIS, "-lm"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"worker build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -195,7 +195,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     nnzM_ = mp[n];
 
     const Clock::time_point ta0 = Clock::now();
-    PartitionResult pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize);
+    PartitionResult pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize, opt.numThreads);
     const Clock::time_point ta1 = Clock::now();
     perm_ = pr.perm;
     inv_.assign(static_cast<size_t>(n), 0);

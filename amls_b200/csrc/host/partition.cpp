@@ -4,58 +4,57 @@
 // (libmetis_static.a, METIS 5 API, 64-bit idx_t established at run time by
 // METIS_SetDefaultOptions filling 40 x 8 bytes).  The graph construction and
 // the recursion restate src/partition/metis_partitioner.cpp:
-//   * extractGraph (:20-45): adjacency of |K|+|M| without self loops, emitted
-//     in the iteration order of one std::unordered_set per vertex filled in
-//     the reference's insertion order (see extractGraph below);
+//   * extractGraph (:20-45): adjacency of |K|+|M| without self loops;
 //   * inducedSubgraph (:48-73): neighbour lists sorted;
-//   * bisect (:80-106): ComputeVertexSeparator with options seed 42.  The
-//     reference first calls PartGraphRecursive and never reads its result;
-//     METIS re-seeds its generator from the options at the start of every
-//     API call, so dropping that call leaves the separator unchanged (checked
-//     on the benchmark pencils: identical permutations) and saves its time;
+//   * bisect (:80-106): ComputeVertexSeparator with options seed 42
+//     (metis_call.hpp).  The reference first calls PartGraphRecursive and
+//     never reads its result; METIS re-seeds its generator from the options
+//     at the start of every API call, so dropping that call leaves the
+//     separator unchanged (checked on the benchmark pencils: identical
+//     permutations) and saves its time;
 //   * recursion (:110-160) and perm = post-order concatenation (:168-175).
 #include "tree.hpp"
 
+#include <dlfcn.h>
+#include <spawn.h>
+#include <sys/socket.h>
+#include <sys/wait.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
+#include <condition_variable>
+#include <csignal>
 #include <exception>
 #include <functional>
 #include <memory>
 #include <mutex>
-#include <thread>
 #include <numeric>
 #include <stdexcept>
-#include <unordered_set>
+#include <string>
+#include <thread>
 
-extern "C" {
-// METIS 5 public prototypes (idx_t = int64_t in the linked library).
-int METIS_SetDefaultOptions(int64_t* options);
-int METIS_ComputeVertexSeparator(int64_t* nvtxs, int64_t* xadj, int64_t* adjncy, int64_t* vwgt,
-                                 int64_t* options, int64_t* sepsize, int64_t* part);
-}
+#include "host/metis_call.hpp"
+
+extern char** environ;
 
 namespace amls_b200 {
 
 namespace {
-constexpr int kMetisOk = 1;
-constexpr int kMetisNOptions = 40;
-constexpr int kMetisOptionSeed = 8;
 std::mutex gMetisMutex;   // METIS keeps process-wide state: one call at a time
 
 struct Csr {
     std::vector<int64_t> xadj, adjncy;
 };
 
-// Adjacency of |K| + |M| without self loops.  The reference inserts, for
-// every column c in ascending order and every row r of that column, r into
-// nbr[c] and c into nbr[r] (metis_partitioner.cpp:20-45).  For a symmetric
-// pattern the inserts reaching one vertex's set are exactly its neighbours
-// in ascending order (repeats are no-ops that leave the container
-// untouched), so each set is built here from the vertex's sorted neighbour
-// list - in parallel over vertices - with the same container and insertion
-// sequence, hence the same iteration order with libstdc++.
+// Adjacency of |K| + |M| without self loops (the patterns are symmetric),
+// neighbour lists sorted.  The reference builds the same sets through one
+// std::unordered_set per vertex (metis_partitioner.cpp:20-45), but every
+// graph it hands to METIS, the root's included, goes through
+// inducedSubgraph, which sorts each list (:48-73); only the sets matter.
+// Rows are processed in parallel over host threads.
 Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
                  const int32_t* mc) {
-    std::vector<int64_t> deg(static_cast<size_t>(n) + 1, 0);
     unsigned nt = std::thread::hardware_concurrency();
     if (nt == 0) nt = 1;
     if (nt > 64) nt = 64;
@@ -69,27 +68,17 @@ Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t*
             });
         for (auto& x : th) x.join();
     };
-    // neighbours of v = union of row v of K and of M (sorted merge), minus v
-    auto forNeighbours = [&](int64_t v, auto&& visit) {
-        int64_t a = kp[v], ae = kp[v + 1], b = mp[v], be = mp[v + 1];
-        while (a < ae || b < be) {
-            int64_t r;
-            if (b >= be || (a < ae && kc[a] < mc[b])) r = kc[a++];
-            else if (a >= ae || mc[b] < kc[a]) r = mc[b++];
-            else { r = kc[a]; ++a; ++b; }
-            if (r != v) visit(r);
-        }
-    };
     std::vector<std::vector<int64_t>> lists(static_cast<size_t>(n));
     forRange([&](int64_t b, int64_t e) {
-        std::vector<int64_t> sorted;
         for (int64_t v = b; v < e; ++v) {
-            sorted.clear();
-            forNeighbours(v, [&](int64_t r) { sorted.push_back(r); });
-            std::unordered_set<int64_t> set;
-            for (int64_t r : sorted) set.insert(r);
             auto& out = lists[static_cast<size_t>(v)];
-            out.assign(set.begin(), set.end());
+            out.clear();
+            for (int64_t q = kp[v]; q < kp[v + 1]; ++q)
+                if (kc[q] != v) out.push_back(kc[q]);
+            for (int64_t q = mp[v]; q < mp[v + 1]; ++q)
+                if (mc[q] != v) out.push_back(mc[q]);
+            std::sort(out.begin(), out.end());
+            out.erase(std::unique(out.begin(), out.end()), out.end());
         }
     });
     Csr g;
@@ -103,7 +92,6 @@ Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t*
             std::copy(lists[static_cast<size_t>(i)].begin(), lists[static_cast<size_t>(i)].end(),
                       g.adjncy.begin() + g.xadj[static_cast<size_t>(i)]);
     });
-    (void)deg;
     return g;
 }
 
@@ -128,25 +116,168 @@ Csr inducedSubgraph(const Csr& g, const std::vector<int64_t>& verts, std::vector
     return sub;
 }
 
-// part[v] in {0, 1, 2}; 2 = vertex separator.
-std::vector<int64_t> bisect(Csr g) {
+// In-process separator (serialised); part[v] in {0, 1, 2}, 2 = separator.
+std::vector<int64_t> bisectInProcess(Csr& g) {
     const int64_t n = static_cast<int64_t>(g.xadj.size()) - 1;
     std::vector<int64_t> part(static_cast<size_t>(n), 0);
     if (n == 0) return part;
-    int64_t nvtxs = n;
-    int64_t opts[kMetisNOptions];
-    METIS_SetDefaultOptions(opts);
-    opts[kMetisOptionSeed] = 42;
-    int64_t sepsize = 0;
     int rc;
     {
         std::lock_guard<std::mutex> lock(gMetisMutex);
-        rc = METIS_ComputeVertexSeparator(&nvtxs, g.xadj.data(), g.adjncy.data(), nullptr, opts,
-                                          &sepsize, part.data());
+        rc = metisSeparator(n, g.xadj.data(), g.adjncy.data(), part.data());
     }
     if (rc != kMetisOk) throw std::runtime_error("METIS_ComputeVertexSeparator failed");
     return part;
 }
+
+bool sendAll(int fd, const void* p, size_t bytes) {
+    const char* c = static_cast<const char*>(p);
+    while (bytes > 0) {
+        const ssize_t r = send(fd, c, bytes, MSG_NOSIGNAL);
+        if (r < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        c += r;
+        bytes -= static_cast<size_t>(r);
+    }
+    return true;
+}
+bool recvAll(int fd, void* p, size_t bytes) {
+    char* c = static_cast<char*>(p);
+    while (bytes > 0) {
+        const ssize_t r = recv(fd, c, bytes, 0);
+        if (r == 0) return false;
+        if (r < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        c += r;
+        bytes -= static_cast<size_t>(r);
+    }
+    return true;
+}
+
+// the separator worker program sits next to this library
+std::string workerPath() {
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&workerPath), &info) == 0 || !info.dli_fname) return "";
+    std::string lib = info.dli_fname;
+    const size_t k = lib.rfind('/');
+    const std::string dir = k == std::string::npos ? "." : lib.substr(0, k);
+    const std::string path = dir + "/amls_metis_worker";
+    return access(path.c_str(), X_OK) == 0 ? path : "";
+}
+
+// Separator workers: `slots` concurrent METIS calls, one in this process and
+// the rest in worker processes (each with its own METIS state).  A call on
+// a worker that fails for any reason (no worker program, a broken socket) is
+// made in this process instead; the separator is the same either way.
+class SeparatorPool {
+public:
+    explicit SeparatorPool(int slots) {
+        slots_.push_back(Slot{});              // the in-process slot
+        const std::string path = slots > 1 ? workerPath() : "";
+        for (int w = 1; w < slots && !path.empty(); ++w) {
+            int sv[2];
+            if (socketpair(AF_UNIX, SOCK_STREAM | SOCK_CLOEXEC, 0, sv) != 0) break;
+            posix_spawn_file_actions_t fa;
+            posix_spawn_file_actions_init(&fa);
+            posix_spawn_file_actions_adddup2(&fa, sv[1], 0);
+            posix_spawn_file_actions_adddup2(&fa, sv[1], 1);
+            char* argv[] = {const_cast<char*>(path.c_str()), nullptr};
+            pid_t pid = 0;
+            const int rc = posix_spawn(&pid, path.c_str(), &fa, nullptr, argv, environ);
+            posix_spawn_file_actions_destroy(&fa);
+            close(sv[1]);
+            if (rc != 0) {
+                close(sv[0]);
+                break;
+            }
+            Slot s;
+            s.pid = pid;
+            s.fd = sv[0];
+            slots_.push_back(s);
+        }
+    }
+    ~SeparatorPool() {
+        for (Slot& s : slots_)
+            if (s.fd >= 0) retire(s);
+    }
+    SeparatorPool(const SeparatorPool&) = delete;
+    SeparatorPool& operator=(const SeparatorPool&) = delete;
+
+    std::vector<int64_t> separator(Csr g) {
+        size_t k;
+        {
+            std::unique_lock<std::mutex> lock(m_);
+            cv_.wait(lock, [&] {
+                for (const Slot& s : slots_)
+                    if (!s.busy) return true;
+                return false;
+            });
+            k = slots_.size();
+            for (size_t i = slots_.size(); i-- > 0;)   // workers first
+                if (!slots_[i].busy) {
+                    k = i;
+                    break;
+                }
+            slots_[k].busy = true;
+        }
+        std::vector<int64_t> part;
+        bool done = false;
+        if (slots_[k].fd >= 0) done = remote(slots_[k], g, part);
+        std::exception_ptr err;
+        if (!done) {
+            try {
+                part = bisectInProcess(g);
+            } catch (...) {
+                err = std::current_exception();
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            slots_[k].busy = false;
+        }
+        cv_.notify_one();
+        if (err) std::rethrow_exception(err);
+        return part;
+    }
+
+private:
+    struct Slot {
+        pid_t pid = -1;
+        int fd = -1;
+        bool busy = false;
+    };
+    bool remote(Slot& s, const Csr& g, std::vector<int64_t>& part) {
+        const int64_t n = static_cast<int64_t>(g.xadj.size()) - 1;
+        const int64_t hdr[2] = {n, static_cast<int64_t>(g.adjncy.size())};
+        int64_t status = 0;
+        part.assign(static_cast<size_t>(n), 0);
+        const bool ok = sendAll(s.fd, hdr, sizeof(hdr)) &&
+                        sendAll(s.fd, g.xadj.data(), sizeof(int64_t) * g.xadj.size()) &&
+                        sendAll(s.fd, g.adjncy.data(), sizeof(int64_t) * g.adjncy.size()) &&
+                        recvAll(s.fd, &status, sizeof(status)) && status == kMetisOk &&
+                        (n == 0 || recvAll(s.fd, part.data(), sizeof(int64_t) * static_cast<size_t>(n)));
+        if (!ok) retire(s);
+        return ok;
+    }
+    static void retire(Slot& s) {
+        shutdown(s.fd, SHUT_RDWR);
+        close(s.fd);
+        s.fd = -1;
+        if (s.pid > 0) {
+            int st = 0;
+            while (waitpid(s.pid, &st, 0) < 0 && errno == EINTR) {
+            }
+        }
+        s.pid = -1;
+    }
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::vector<Slot> slots_;
+};
 }  // namespace
 
 int64_t SeparatorTree::addNode(NodeRole role, std::vector<int64_t> idx) {
@@ -217,25 +348,23 @@ struct Split {
     std::unique_ptr<Split> left, right;
 };
 
-// The top kParallelDepth levels run their two halves on two threads.  The
-// METIS library keeps process-wide state (its random generator), so its calls
-// are serialised by a mutex: concurrent calls give different separators,
-// while every call re-seeds from its own options, so the split of each
-// vertex set does not depend on the order of the serialised calls.  What
-// runs concurrently is the induced-subgraph construction and bookkeeping.
-constexpr int kParallelDepth = 3;
+// The top levels run their two halves on two threads, their METIS calls in
+// separate worker processes (SeparatorPool).  Every METIS call re-seeds from
+// its own options, so the split of each vertex set depends on nothing but
+// that vertex set: the tree is the same for any thread or worker count.
 
 std::unique_ptr<Split> splitRec(const Csr& g, std::vector<int64_t> verts, int depth, int nLevels,
-                                int64_t leafSize) {
+                                int64_t leafSize, SeparatorPool& pool, int parDepth) {
     auto out = std::make_unique<Split>();
     const int64_t m = static_cast<int64_t>(verts.size());
     if (m <= leafSize || depth >= nLevels || m < 4) {
         out->verts = std::move(verts);
         return out;
     }
+    // the root's vertex set is all of g in order: its induced subgraph is g
     std::vector<int64_t> localOf;
-    Csr sub = inducedSubgraph(g, verts, localOf);
-    const std::vector<int64_t> part = bisect(std::move(sub));
+    Csr sub = depth == 0 ? g : inducedSubgraph(g, verts, localOf);
+    const std::vector<int64_t> part = pool.separator(std::move(sub));
     std::vector<int64_t> side[2], sep;
     for (int64_t i = 0; i < m; ++i) {
         const int64_t p = part[static_cast<size_t>(i)];
@@ -248,17 +377,17 @@ std::unique_ptr<Split> splitRec(const Csr& g, std::vector<int64_t> verts, int de
         return out;
     }
     out->sep = std::move(sep);
-    if (depth < kParallelDepth) {
+    if (depth < parDepth) {
         std::exception_ptr err;
         std::thread t([&] {
             try {
-                out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize);
+                out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize, pool, parDepth);
             } catch (...) {
                 err = std::current_exception();
             }
         });
         try {
-            out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize);
+            out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize, pool, parDepth);
         } catch (...) {
             t.join();
             throw;
@@ -266,8 +395,8 @@ std::unique_ptr<Split> splitRec(const Csr& g, std::vector<int64_t> verts, int de
         t.join();
         if (err) std::rethrow_exception(err);
     } else {
-        out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize);
-        out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize);
+        out->left = splitRec(g, std::move(side[0]), depth + 1, nLevels, leafSize, pool, parDepth);
+        out->right = splitRec(g, std::move(side[1]), depth + 1, nLevels, leafSize, pool, parDepth);
     }
     return out;
 }
@@ -288,13 +417,18 @@ int64_t buildTree(SeparatorTree& tree, Split& s) {
 
 PartitionResult recursiveBisection(int64_t n, const int64_t* kRowPtr, const int32_t* kCol,
                                    const int64_t* mRowPtr, const int32_t* mCol, int nLevels,
-                                   int64_t leafSize) {
+                                   int64_t leafSize, int numThreads) {
     PartitionResult res;
     if (n == 0) return res;
     const Csr g = extractGraph(n, kRowPtr, kCol, mRowPtr, mCol);
     std::vector<int64_t> all(static_cast<size_t>(n));
     std::iota(all.begin(), all.end(), 0);
-    std::unique_ptr<Split> root = splitRec(g, std::move(all), 0, nLevels, leafSize);
+    int threads = numThreads > 0 ? numThreads : static_cast<int>(std::thread::hardware_concurrency());
+    threads = std::max(1, std::min(threads, 8));
+    int parDepth = 0;                           // 2^parDepth concurrent subtrees
+    while ((2 << parDepth) <= threads) ++parDepth;
+    SeparatorPool pool(threads);
+    std::unique_ptr<Split> root = splitRec(g, std::move(all), 0, nLevels, leafSize, pool, parDepth);
     buildTree(res.tree, *root);
     res.tree.relabelRoot();
     for (int64_t id : res.tree.postOrder()) {

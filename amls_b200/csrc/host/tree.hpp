@@ -46,12 +46,15 @@ struct PartitionResult {
 };
 
 // Recursive bisection of the graph of |K| + |M| (CSR pattern, both given),
-// METIS_PartGraphRecursive + METIS_ComputeVertexSeparator with seed 42 at each
-// level, stopping at m <= leafSize, depth >= nLevels or m < 4, or on a
-// degenerate split.  Throws std::runtime_error on a METIS failure.
+// METIS_ComputeVertexSeparator with seed 42 at each level, stopping at
+// m <= leafSize, depth >= nLevels or m < 4, or on a degenerate split.
+// numThreads (0 = hardware concurrency, at most 8) bounds the concurrent
+// subtrees; their METIS calls run in amls_metis_worker processes next to the
+// library (in this process when the program is absent).  The tree does not
+// depend on numThreads.  Throws std::runtime_error on a METIS failure.
 PartitionResult recursiveBisection(int64_t n,
                                    const int64_t* kRowPtr, const int32_t* kCol,
                                    const int64_t* mRowPtr, const int32_t* mCol,
-                                   int nLevels, int64_t leafSize);
+                                   int nLevels, int64_t leafSize, int numThreads = 0);
 
 }  // namespace amls_b200
