@@ -34,10 +34,6 @@ void trsmTiles(std::vector<TileRef>& t, int desc, int64_t rows) {
     for (int i = 0; i < cdiv(rows, kTrsmRows); ++i) t.push_back({desc, i * kTrsmRows, 0, 0});
 }
 
-void trsmTiles64(std::vector<TileRef>& t, int desc, int64_t rows) {
-    for (int i = 0; i < cdiv(rows, kTrsmRows64); ++i) t.push_back({desc, i * kTrsmRows64, 0, 0});
-}
-
 void copyTiles(std::vector<TileRef>& t, int desc, int64_t r, int64_t c) {
     for (int j = 0; j < cdiv(c, 32); ++j)
         for (int i = 0; i < cdiv(r, 32); ++i) t.push_back({desc, i * 32, j * 32, 0});
@@ -376,6 +372,12 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     mVal_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
     kPool_.ensure(sizeof(double) * static_cast<size_t>(frontTotal_));
     mPool_.ensure(sizeof(double) * static_cast<size_t>(frontTotal_));
+    gPool_.ensure(sizeof(double) * static_cast<size_t>(frontTotal_));
+    // L_ii^-1 blocks are written below the diagonal only: the rest stays zero
+    linvPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(eigTotal_, 1)));
+    linvScratch_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(eigTotal_, 1)));
+    cudaCheck(cudaMemsetAsync(linvPool_.as<double>(), 0, sizeof(double) * static_cast<size_t>(std::max<int64_t>(eigTotal_, 1)),
+                              stream_), "zero");
     eigPool_.ensure(sizeof(double) * static_cast<size_t>(eigTotal_));
     dPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     ePool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
@@ -451,14 +453,23 @@ void Engine::buildStatic() {
     levelPlans_.assign(static_cast<size_t>(maxLevel_) + 1, LevelPlan());
     double* kP = kPool_.as<double>();
     double* mP = mPool_.as<double>();
+    double* gP = gPool_.as<double>();
     double* eP = eigPool_.as<double>();
+    double* liP = linvPool_.as<double>();
+    double* lsP = linvScratch_.as<double>();
+    auto addBatch = [&](const std::vector<GemmDesc>& d, const std::vector<TileRef>& t) {
+        GemmBatch g;
+        g.desc = sblob_.add(d);
+        g.tiles = sblob_.add(t);
+        g.nTiles = static_cast<int>(t.size());
+        return g;
+    };
     for (int l = 0; l <= maxLevel_; ++l) {
         LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
         std::vector<FrontDesc> fk, fm, fsym;
-        std::vector<TrsmDesc> td, cd, idd;
-        std::vector<TileRef> tt, ct, copyT, rt, ut, it, symT;
-        std::vector<CopyDesc> cp;
-        std::vector<GemmDesc> rg;
+        std::vector<TrsmDesc> idd;
+        std::vector<TileRef> rt, ut, it, symT, wT, cT;
+        std::vector<GemmDesc> rg, wg, cg;
         std::vector<FrontUpdDesc> ud;
         int64_t maxN = 0, maxRows = 0;
         for (int i : byLevel_[static_cast<size_t>(l)]) {
@@ -485,55 +496,40 @@ void Engine::buildStatic() {
             maxN = std::max(maxN, nd.n);
             maxRows = std::max(maxRows, nd.ld);
             double* invP = invPool_.as<double>() + nd.invOff;
-            // inverses of the 64x64 diagonal blocks of L_ii
+            double* linvP = liP + nd.eigOff;
+            // inverses of the 64x64 diagonal blocks of L_ii, placed on the
+            // diagonal of L_ii^-1 (the doubling below completes it)
             TrsmDesc iv{};
             iv.L = kP + nd.frontOff;
             iv.ldl = nd.ld;
+            iv.X = linvP;
+            iv.ldx = nd.n;
             iv.n = static_cast<int32_t>(nd.n);
             iv.inv = invP;
             for (int J = 0; J < cdiv(nd.n, 64); ++J) it.push_back({static_cast<int32_t>(idd.size()), J, 0, 0});
             idd.push_back(iv);
-            // G <- G L^-T (all n + s rows)
-            TrsmDesc t{};
-            t.L = kP + nd.frontOff;
-            t.ldl = nd.ld;
-            t.X = mP + nd.frontOff;
-            t.ldx = nd.ld;
-            t.n = static_cast<int32_t>(nd.n);
-            t.r = static_cast<int32_t>(nd.ld);
-            t.inv = invP;
-            trsmTiles64(tt, static_cast<int>(td.size()), nd.ld);
-            td.push_back(t);
-            // eig <- (G_ii L^-T)^T
-            CopyDesc c{};
-            c.in = mP + nd.frontOff;
-            c.ldin = nd.ld;
-            c.out = eP + nd.eigOff;
-            c.ldout = nd.n;
-            c.r = c.c = static_cast<int32_t>(nd.n);
-            copyTiles(copyT, static_cast<int>(cp.size()), nd.n, nd.n);
-            cp.push_back(c);
-            // eig <- eig L^-T  => C = L^-1 M^ L^-T
-            TrsmDesc t2{};
-            t2.L = kP + nd.frontOff;
-            t2.ldl = nd.ld;
-            t2.X = eP + nd.eigOff;
-            t2.ldx = nd.n;
-            t2.n = t2.r = static_cast<int32_t>(nd.n);
-            t2.inv = invP;
-            trsmTiles64(ct, static_cast<int>(cd.size()), nd.n);
-            cd.push_back(t2);
+            // W = G L^-T over all n + s rows of the M front (G L_ii^-T: the
+            // reference's Y solves, K^-1 M columns, in transposed form)
+            GemmDesc w = gemm(nd.ld, nd.n, nd.n, kTransB | kTriKUpTo, mP + nd.frontOff, nd.ld, linvP, nd.n,
+                              gP + nd.frontOff, nd.ld, 1.0, 0.0);
+            gemmTiles(wT, static_cast<int>(wg.size()), nd.ld, nd.n);
+            wg.push_back(w);
+            // C = L^-1 G_ii^T L^-T = W_ii^T L^-T
+            GemmDesc c = gemm(nd.n, nd.n, nd.n, kTransA | kTransB | kTriKUpTo, gP + nd.frontOff, nd.ld, linvP,
+                              nd.n, eP + nd.eigOff, nd.n, 1.0, 0.0);
+            gemmTiles(cT, static_cast<int>(cg.size()), nd.n, nd.n);
+            cg.push_back(c);
             if (s > 0) {
-                // R = Q - L_Si C / 2  (in place in the M front's lower block)
+                // R = Q - L_Si C / 2  (in place in W's lower block)
                 GemmDesc g = gemm(s, nd.n, nd.n, kAccumulate, kP + nd.frontOff + nd.n, nd.ld,
-                                  eP + nd.eigOff, nd.n, mP + nd.frontOff + nd.n, nd.ld, -0.5, 1.0);
+                                  eP + nd.eigOff, nd.n, gP + nd.frontOff + nd.n, nd.ld, -0.5, 1.0);
                 gemmTiles(rt, static_cast<int>(rg.size()), s, nd.n);
                 rg.push_back(g);
                 FrontUpdDesc u{};
                 u.s = static_cast<int32_t>(s);
                 u.n = static_cast<int32_t>(nd.n);
                 u.A = kP + nd.frontOff + nd.n;
-                u.B = mP + nd.frontOff + nd.n;
+                u.B = gP + nd.frontOff + nd.n;
                 u.ld = nd.ld;
                 u.pmin = dPmin + nd.mapCol;
                 u.colOff = dColOff + nd.mapCol;
@@ -560,15 +556,37 @@ void Engine::buildStatic() {
         L.invDesc = sblob_.add(idd);
         L.invTiles = sblob_.add(it);
         L.nInvTiles = static_cast<int>(it.size());
-        L.trsmDesc = sblob_.add(td);
-        L.trsmTiles = sblob_.add(tt);
-        L.nTrsmTiles = static_cast<int>(tt.size());
-        L.tDesc = sblob_.add(cp);
-        L.tTiles = sblob_.add(copyT);
-        L.nTTiles = static_cast<int>(copyT.size());
-        L.cDesc = sblob_.add(cd);
-        L.cTiles = sblob_.add(ct);
-        L.nCTiles = static_cast<int>(ct.size());
+        // L_ii^-1 by doubling: with the diagonal blocks of size b complete,
+        // each pair of neighbouring blocks (A = [a0, a1), B = [a1, b1)) gets
+        //   L^-1[B, A] = -L^-1[B, B] (L[B, A] L^-1[A, A])
+        // (two batched GEMMs per step, T in the scratch copy of the layout)
+        L.inv.clear();
+        for (int64_t b = 64; b < maxN; b *= 2) {
+            std::vector<GemmDesc> d1, d2;
+            std::vector<TileRef> t1, t2;
+            for (int i : byLevel_[static_cast<size_t>(l)]) {
+                const Node& nd = nodes_[static_cast<size_t>(i)];
+                const int64_t n = nd.n, ld = nd.ld;
+                const double* Lf = kP + nd.frontOff;
+                double* li = liP + nd.eigOff;
+                double* ls = lsP + nd.eigOff;
+                for (int64_t a0 = 0; a0 + b < n; a0 += 2 * b) {
+                    const int64_t a1 = a0 + b, b1 = std::min(n, a0 + 2 * b);
+                    GemmDesc g1 = gemm(b1 - a1, a1 - a0, a1 - a0, kTriKFrom, Lf + a1 + a0 * ld, ld,
+                                       li + a0 + a0 * n, n, ls + a1 + a0 * n, n, 1.0, 0.0);
+                    gemmTiles(t1, static_cast<int>(d1.size()), b1 - a1, a1 - a0);
+                    d1.push_back(g1);
+                    GemmDesc g2 = gemm(b1 - a1, a1 - a0, b1 - a1, kTriAUpTo, li + a1 + a1 * n, n,
+                                       ls + a1 + a0 * n, n, li + a1 + a0 * n, n, -1.0, 0.0);
+                    gemmTiles(t2, static_cast<int>(d2.size()), b1 - a1, a1 - a0);
+                    d2.push_back(g2);
+                }
+            }
+            L.inv.push_back(addBatch(d1, t1));
+            L.inv.push_back(addBatch(d2, t2));
+        }
+        L.w = addBatch(wg, wT);
+        L.c = addBatch(cg, cT);
         L.rDesc = sblob_.add(rg);
         L.rTiles = sblob_.add(rt);
         L.nRTiles = static_cast<int>(rt.size());
@@ -584,10 +602,11 @@ void Engine::buildStatic() {
         const double nn = static_cast<double>(nd.n), s = static_cast<double>(nd.S.size());
         elimCatF_[0] += nn * nn * nn / 3.0 + s * nn * nn;               // Cholesky
         elimCatB_[0] += 8.0 * 2.0 * (nn + s) * nn;
-        elimCatF_[1] += (nn + s) * nn * nn + nn * nn * nn;               // TRSMs (G, C)
-        elimCatB_[1] += 8.0 * (2.0 * (nn + s) * nn + 2.0 * nn * nn + nn * nn);
-        elimCatF_[2] += 2.0 * s * nn * nn;                               // R GEMM
-        elimCatB_[2] += 8.0 * (2.0 * s * nn + nn * nn + s * nn);
+        elimCatF_[1] += nn * 64.0 * 64.0 / 3.0;                          // 64 x 64 diagonal inverses
+        elimCatB_[1] += 8.0 * 2.0 * nn * 64.0;
+        // L^-1 (n^3 / 3), W = G L^-T ((n + s) n^2), C = W_ii^T L^-T (n^3), R (2 s n^2)
+        elimCatF_[2] += nn * nn * nn / 3.0 + (nn + s) * nn * nn + nn * nn * nn + 2.0 * s * nn * nn;
+        elimCatB_[2] += 8.0 * (2.0 * nn * nn + 2.0 * (nn + s) * nn + 3.0 * nn * nn + 2.0 * s * nn + nn * nn + s * nn);
         elimCatF_[3] += 3.0 * s * s * nn;                                // extend-add
         elimCatB_[3] += 8.0 * (2.0 * s * nn + 2.0 * s * s);
         elimCatB_[8] += 8.0 * (2.0 * (nn + s) * nn + 2.0 * nn * nn);     // assembly, transposes
@@ -596,8 +615,9 @@ void Engine::buildStatic() {
     for (const Node& nd : nodes_) {
         const double nn = static_cast<double>(nd.n), s = static_cast<double>(nd.S.size());
         fe += nn * nn * nn / 3.0 + s * nn * nn;          // partial Cholesky
-        fe += (nn + s) * nn * nn;                        // G <- G L^-T
-        fe += nn * nn * nn;                              // C = L^-1 (.)
+        fe += nn * nn * nn / 3.0;                        // L_ii^-1
+        fe += (nn + s) * nn * nn;                        // W = G L^-T
+        fe += nn * nn * nn;                              // C = W_ii^T L^-T
         fe += 2.0 * s * nn * nn;                         // R
         fe += 3.0 * s * s * nn;                          // UK (s^2 n) + UM (2 s^2 n), lower half x2
         be += 8.0 * (2.0 * (nn + s) * nn + nn * nn) * 2.0 + 8.0 * s * s;   // fronts r/w + updates
@@ -620,12 +640,12 @@ void Engine::eliminate(cudaStream_t s) {
         }
         LAUNCH(launchInvDiag(sblob_.dev<TrsmDesc>(L.invDesc), sblob_.dev<TileRef>(L.invTiles),
                              L.nInvTiles, s));
-        LAUNCH(launchTrsmRows64(sblob_.dev<TrsmDesc>(L.trsmDesc), sblob_.dev<TileRef>(L.trsmTiles),
-                                L.nTrsmTiles, s));
-        LAUNCH(launchTransposeBatched(sblob_.dev<CopyDesc>(L.tDesc), sblob_.dev<TileRef>(L.tTiles),
-                                      L.nTTiles, s));
-        LAUNCH(launchTrsmRows64(sblob_.dev<TrsmDesc>(L.cDesc), sblob_.dev<TileRef>(L.cTiles),
-                                L.nCTiles, s));
+        LAUNCH(launchPlaceDiagInv(sblob_.dev<TrsmDesc>(L.invDesc), sblob_.dev<TileRef>(L.invTiles),
+                                  L.nInvTiles, s));
+        for (const GemmBatch& g : L.inv)
+            LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(g.desc), sblob_.dev<TileRef>(g.tiles), g.nTiles, s));
+        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.w.desc), sblob_.dev<TileRef>(L.w.tiles), L.w.nTiles, s));
+        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.c.desc), sblob_.dev<TileRef>(L.c.tiles), L.c.nTiles, s));
         LAUNCH(launchSymmetrizeTiles(sblob_.dev<FrontDesc>(L.symDesc), sblob_.dev<TileRef>(L.symTiles),
                                      L.nSymTiles, s));
         LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.rDesc), sblob_.dev<TileRef>(L.rTiles),
@@ -798,7 +818,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
 
     // ---- projection tables (all levels) ----
     const double* F = kPool_.as<double>();
-    const double* G = mPool_.as<double>();
+    const double* G = gPool_.as<double>();
     // panels
     panelOff_.assign(static_cast<size_t>(N), -1);
     int64_t panelTot = 0;
@@ -866,8 +886,8 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
         }
     }
     struct LevelTabs {
-        size_t cpD, cpT, trD, trT, g1D, g1T, g2D, g2T, midD, midT, i1D, i1T, i2D, i2T;
-        int ncpT, ntrT, ng1T, ng2T, nmidT, ni1T, ni2T;
+        size_t pjD, pjT, g1D, g1T, g2D, g2T, midD, midT, i1D, i1T, i2D, i2T;
+        int npjT, ng1T, ng2T, nmidT, ni1T, ni2T;
     };
     std::vector<LevelTabs> tabs(static_cast<size_t>(maxLevel_) + 1);
     Blob idx;
@@ -885,10 +905,8 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     double fc = 0, bc = 0;
     const double fcEig = 0.0;
     for (int l = 0; l <= maxLevel_; ++l) {
-        std::vector<CopyDesc> cp;
-        std::vector<TrsmDesc> tr;
-        std::vector<GemmDesc> g1, g2, mid, i1, i2;
-        std::vector<TileRef> cpT, trT, g1T, g2T, midT, i1T, i2T;
+        std::vector<GemmDesc> pj, g1, g2, mid, i1, i2;
+        std::vector<TileRef> pjT, g1T, g2T, midT, i1T, i2T;
         for (int i : byLevel_[static_cast<size_t>(l)]) {
             const Node& nd = nodes_[static_cast<size_t>(i)];
             const int64_t ni = nd.n, si = static_cast<int64_t>(nd.S.size());
@@ -897,30 +915,23 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
             double* wti = wt + wtOff[static_cast<size_t>(i)];
             const double* Yi = Y + yOff_[static_cast<size_t>(i)];
             if (Ki > 0 && ni > 0) {
+                // wt (Ki x ni) = [panel rows of node i, each descendant's
+                // columns]^T L_ii^-T: the descendants' M-bar columns solved
+                // with K^_ii, in transposed form
                 int64_t colPos = 0;
+                const double* linvI = linvPool_.as<double>() + nd.eigOff;
                 for (int kk : descK[static_cast<size_t>(i)]) {
                     const Node& nk = nodes_[static_cast<size_t>(kk)];
-                    CopyDesc c{};
-                    c.in = panel + panelOff_[static_cast<size_t>(kk)] + nd.pathPrefix;
-                    c.ldin = nk.pathPrefix;
-                    c.out = wti + colPos;
-                    c.ldout = Ki;
-                    c.r = static_cast<int32_t>(ni);
-                    c.c = P.k[static_cast<size_t>(kk)];
-                    copyTiles(cpT, static_cast<int>(cp.size()), ni, c.c);
-                    cp.push_back(c);
-                    colPos += c.c;
+                    const int ck = P.k[static_cast<size_t>(kk)];
+                    if (ck > 0) {
+                        GemmDesc g = gemm(ck, ni, ni, kTransA | kTransB | kTriKUpTo,
+                                          panel + panelOff_[static_cast<size_t>(kk)] + nd.pathPrefix,
+                                          nk.pathPrefix, linvI, ni, wti + colPos, Ki, 1.0, 0.0);
+                        gemmTiles(pjT, static_cast<int>(pj.size()), ck, ni);
+                        pj.push_back(g);
+                    }
+                    colPos += ck;
                 }
-                TrsmDesc t{};
-                t.L = F + nd.frontOff;
-                t.ldl = nd.ld;
-                t.X = wti;
-                t.ldx = Ki;
-                t.n = static_cast<int32_t>(ni);
-                t.r = static_cast<int32_t>(Ki);
-                t.inv = invPool_.as<double>() + nd.invOff;
-                trsmTiles64(trT, static_cast<int>(tr.size()), Ki);
-                tr.push_back(t);
                 fc += static_cast<double>(Ki) * ni * ni;
                 if (ki > 0) {
                     GemmDesc a = gemm(ki, Ki, ni, kTransA | kTransB | kScatter, Yi, ni, wti, Ki, cred, p, 1.0, 0.0);
@@ -963,8 +974,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
             bc += 8.0 * (static_cast<double>(Ki) * ni * 3 + si * (Ki + ki) * 2);
         }
         LevelTabs& T = tabs[static_cast<size_t>(l)];
-        T.cpD = b.add(cp); T.cpT = b.add(cpT); T.ncpT = static_cast<int>(cpT.size());
-        T.trD = b.add(tr); T.trT = b.add(trT); T.ntrT = static_cast<int>(trT.size());
+        T.pjD = b.add(pj); T.pjT = b.add(pjT); T.npjT = static_cast<int>(pjT.size());
         T.g1D = b.add(g1); T.g1T = b.add(g1T); T.ng1T = static_cast<int>(g1T.size());
         T.g2D = b.add(g2); T.g2T = b.add(g2T); T.ng2T = static_cast<int>(g2T.size());
         T.midD = b.add(mid); T.midT = b.add(midT); T.nmidT = static_cast<int>(midT.size());
@@ -987,8 +997,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     LAUNCH(launchSetDiagonal(cred, wDev, p, s));
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelTabs& T = tabs[static_cast<size_t>(l)];
-        LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(T.cpD), b.dev<TileRef>(T.cpT), T.ncpT, s));
-        LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.trD), b.dev<TileRef>(T.trT), T.ntrT, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.pjD), b.dev<TileRef>(T.pjT), T.npjT, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.ng1T, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.ng2T, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.midD), b.dev<TileRef>(T.midT), T.nmidT, s));
@@ -1088,6 +1097,9 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
     for (int j = 0; j < m; ++j) st[static_cast<size_t>(j)] = std::sqrt(P.theta[static_cast<size_t>(j)]);
     cudaCheck(cudaMemcpyAsync(sqrtTheta_.as<double>(), st.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s), "sqrt theta");
     double* zt = ztPool_.as<double>();
+    // u_i = (y v_i D_theta)^T - z_S L_Si, then z_i = u_i L_ii^-1 (transposed
+    // layout, m x n_i blocks); u lives in a second buffer of the same layout
+    double* ut = static_cast<double*>(zTmp_.ensure(sizeof(double) * static_cast<size_t>(m * n_)));
     const double* F = kPool_.as<double>();
     const double* Y = yPool_.as<double>();
     const double* V = redY_.as<double>();
@@ -1096,8 +1108,7 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
     std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
     double fb = 0;
     for (int l = maxLevel_; l >= 0; --l) {
-        std::vector<GemmDesc> g1, g2;
-        std::vector<TrsmDesc> tr;
+        std::vector<GemmDesc> g1, g2, tr;
         std::vector<TileRef> g1T, g2T, tT;
         for (int i : byLevel_[static_cast<size_t>(l)]) {
             const Node& nd = nodes_[static_cast<size_t>(i)];
@@ -1105,27 +1116,20 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
             const int ki = P.k[static_cast<size_t>(i)];
             if (ni == 0) continue;
             double* zi = zt + nd.off * m;
+            double* ui = ut + nd.off * m;
             GemmDesc a = gemm(m, ni, ki, kTransA | kTransB | kRowScale, V + P.projOff[static_cast<size_t>(i)], P.p,
-                              Y + yOff_[static_cast<size_t>(i)], std::max<int64_t>(ni, 1), zi, m, 1.0, 0.0);
+                              Y + yOff_[static_cast<size_t>(i)], std::max<int64_t>(ni, 1), ui, m, 1.0, 0.0);
             a.rowScale = sqrtTheta_.as<double>();
             gemmTiles(g1T, static_cast<int>(g1.size()), m, ni);
             g1.push_back(a);
             if (si > 0) {
-                GemmDesc c = gemm(m, ni, si, kGatherA | kAccumulate, zt, m, F + nd.frontOff + ni, nd.ld, zi, m, -1.0, 1.0);
+                GemmDesc c = gemm(m, ni, si, kGatherA | kAccumulate, zt, m, F + nd.frontOff + ni, nd.ld, ui, m, -1.0, 1.0);
                 c.aMap = sIdxDev_ + nd.mapCol;
                 gemmTiles(g2T, static_cast<int>(g2.size()), m, ni);
                 g2.push_back(c);
             }
-            TrsmDesc t{};
-            t.L = F + nd.frontOff;
-            t.ldl = nd.ld;
-            t.X = zi;
-            t.ldx = m;
-            t.n = static_cast<int32_t>(ni);
-            t.r = m;
-            t.backward = 1;
-            t.inv = invPool_.as<double>() + nd.invOff;
-            trsmTiles64(tT, static_cast<int>(tr.size()), m);
+            GemmDesc t = gemm(m, ni, ni, kTriKFrom, ui, m, linvPool_.as<double>() + nd.eigOff, ni, zi, m, 1.0, 0.0);
+            gemmTiles(tT, static_cast<int>(tr.size()), m, ni);
             tr.push_back(t);
             fb += 2.0 * m * ni * (ki + si) + static_cast<double>(m) * ni * ni;
         }
@@ -1140,7 +1144,7 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
         const Tabs& T = tabs[static_cast<size_t>(l)];
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.n1, s));
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
-        LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
+        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
     }
     catF_[2] += fb;
     catB_[2] += 8.0 * 3.0 * m * static_cast<double>(n_);
@@ -1488,18 +1492,6 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const d
     cudaCheck(cudaStreamSynchronize(s), "sensitivities");
 }
 
-// device arrays of the nodes' eig-pool offsets and sizes (post-order)
-const int64_t* Engine::eigOffsDev() {
-    std::vector<int64_t> v;
-    for (int i : order_) v.push_back(nodes_[static_cast<size_t>(i)].eigOff);
-    for (int i : order_) v.push_back(nodes_[static_cast<size_t>(i)].n);
-    int64_t* d = static_cast<int64_t*>(nodeOffDev_.ensure(sizeof(int64_t) * v.size()));
-    cudaCheck(cudaMemcpyAsync(d, v.data(), sizeof(int64_t) * v.size(), cudaMemcpyHostToDevice, stream_), "offsets");
-    cudaCheck(cudaStreamSynchronize(stream_), "offsets");
-    return d;
-}
-
-const int64_t* Engine::nodeSizesDev() { return nodeOffDev_.as<int64_t>() + order_.size(); }
 
 void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
     norms_.ensure(sizeof(double) * static_cast<size_t>(m));

@@ -131,6 +131,8 @@ private:
 
     // static device data
     DevBuf kPool_, mPool_, eigPool_, dPool_, ePool_, tauPool_, invPool_;
+    DevBuf gPool_;                                 // G L^-T of every front (R in its lower block)
+    DevBuf linvPool_, linvScratch_;                // L_ii^-1 per node (eig layout), doubling scratch
     DevBuf kVal_, mVal_, kDst_, mDst_;             // CSR values and their front destinations
     DevBuf mRp_, mCi_, invDev_, permDev_;          // original M CSR pattern, maps
     DevBuf mGrp_;                                  // row groups with one M pattern
@@ -140,17 +142,18 @@ private:
     DevBuf status_;
     Blob sblob_;
     // offsets into sblob_ for level tables
+    struct GemmBatch {                          // one batched GEMM launch
+        size_t desc = 0, tiles = 0;
+        int nTiles = 0;
+    };
     struct LevelPlan {
         size_t frontK = 0, frontM = 0;             // FrontDesc tables
         int nFront = 0, maxBlocks = 0, maxRowTiles = 0;
         size_t invDesc = 0, invTiles = 0;           // 64x64 diagonal-block inverses
         int nInvTiles = 0;
-        size_t trsmDesc = 0, trsmTiles = 0;
-        int nTrsmTiles = 0;
-        size_t tDesc = 0, tTiles = 0;              // transpose G_ii -> eig matrix
-        int nTTiles = 0;
-        size_t cDesc = 0, cTiles = 0;              // TRSM on eig matrix
-        int nCTiles = 0;
+        std::vector<GemmBatch> inv;                // L^-1 doubling: (T, L^-1 block) per step
+        GemmBatch w;                               // W = G L^-T (all rows of the front)
+        GemmBatch c;                               // C = W_ii^T L^-T
         size_t symDesc = 0, symTiles = 0;          // symmetrize eig matrices
         int nSymTiles = 0;
         size_t rDesc = 0, rTiles = 0;              // R = Q - L C / 2
@@ -168,7 +171,7 @@ private:
     // per-pass device buffers
     DevBuf yPool_, wPool_, kOutDev_, iiWork_, panelPool_, wtPool_, credPool_;
     DevBuf redY_, redW_, redWork_, redD_, redE_, redTau_, redK_, redP_;
-    DevBuf ztPool_, zOut_, norms_, sqrtTheta_, passBlob_, tlBlob_, redBlob_, idxBlob_, tlLargeBlob_;
+    DevBuf ztPool_, zTmp_, zOut_, norms_, sqrtTheta_, passBlob_, tlBlob_, redBlob_, idxBlob_, tlLargeBlob_;
     const int32_t* sIdxDev_ = nullptr;              // S_i lists (device, static)
     const int32_t* rowSDev_ = nullptr;             // panel rows of S_i (device, static)
     std::vector<int64_t> panelOff_;                // per node (doubles), -1 none
@@ -177,9 +180,7 @@ private:
     // refinement and the device dense eigensolver
     DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
-    DevBuf refT_, refU_, refUBlob_, nodeOffDev_, refMQ_;
-    const int64_t* eigOffsDev();
-    const int64_t* nodeSizesDev();
+    DevBuf refT_, refMQ_;
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;

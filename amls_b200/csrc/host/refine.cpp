@@ -8,7 +8,7 @@
 // x_i = L_ii^-T (x_i - L_Si^T x_S).  The refinement is the subspace
 // iteration of AMLS-SIMb (papers/Improving_eigenpairs...md:288-420) on
 // nq = nev + extra vectors with T = K^-1 M (the diagonal blocks applied as
-// block-triangular GEMMs with U_i = L_ii^-T, computed once per refinement),
+// block-triangular GEMMs with the elimination's L_ii^-1),
 // accelerated by a Chebyshev
 // filter: each outer iteration forms Y_c = C_c(2 T / a - I) Q, the unwanted
 // part of T's spectrum being [0, a] with a = 1 / (largest Ritz value), then
@@ -140,34 +140,11 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     double* Vc = static_cast<double*>(refV_.ensure(sizeof(double) * nq * nq));
     double* wd = static_cast<double*>(refW_.ensure(sizeof(double) * nq));
     double* Tm = static_cast<double*>(refT_.ensure(sizeof(double) * sz));
-    double* U = static_cast<double*>(refU_.ensure(sizeof(double) * std::max<int64_t>(eigTotal_, 1)));
     const double* F = kPool_.as<double>();
 
-    // U_i = L_ii^-T (upper triangular, n_i x n_i at eigOff) for every node:
-    // identity, then one row-panel TRSM  U <- U L^-T.  K^-1 is then applied
-    // with block-triangular GEMMs, which keep all SMs busy on the large
-    // separators where a row-panel TRSM has only a few row tiles.
-    {
-        Blob ub;
-        std::vector<TrsmDesc> ud;
-        std::vector<TileRef> uT;
-        for (int i : order_) {
-            const Node& nd = nodes_[static_cast<size_t>(i)];
-            if (nd.n == 0) continue;
-            TrsmDesc t{F + nd.frontOff, nd.ld, U + nd.eigOff, nd.n, static_cast<int32_t>(nd.n),
-                       static_cast<int32_t>(nd.n), 0, 0, invPool_.as<double>() + nd.invOff};
-            for (int r0 = 0; r0 < nd.n; r0 += kTrsmRows64) uT.push_back({static_cast<int32_t>(ud.size()), r0, 0, 0});
-            ud.push_back(t);
-        }
-        const size_t oD = ub.add(ud), oT = ub.add(uT);
-        ub.upload(refUBlob_, s);
-        const int64_t* dOffs = eigOffsDev();
-        const int64_t* dSizes = nodeSizesDev();
-        LAUNCH(launchIdentityBlocks(U, dOffs, dSizes, static_cast<int>(order_.size()), s));
-        LAUNCH(launchTrsmRows64(ub.dev<TrsmDesc>(oD), ub.dev<TileRef>(oT), static_cast<int>(uT.size()), s));
-        cudaCheck(cudaStreamSynchronize(s), "U = L^-T");
-        for (const Node& nd : nodes_) catF_[1] += static_cast<double>(nd.n) * nd.n * nd.n;
-    }
+    // L_ii^-1 (lower triangular, n_i x n_i at eigOff) of every node comes from
+    // the elimination; K^-1 is applied with block-triangular GEMMs on it.
+    const double* Linv = linvPool_.as<double>();
 
     // ---- tables: K^-1 sweeps, Rayleigh-Ritz products, subspace update ----
     Blob b;
@@ -200,16 +177,16 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             if (ni == 0) continue;
             double* Xi = X + nd.off * nq;
             double* Ti = Tm + nd.off * nq;
-            const double* Ui = U + nd.eigOff;
-            // forward: T_i = X_i U_i  (= (L_ii^-1 x_i)^T)
+            const double* Li = Linv + nd.eigOff;
+            // forward: T_i = X_i L_ii^-T  (= (L_ii^-1 x_i)^T)
             GemmDesc tf{};
             tf.M = nq;
             tf.N = static_cast<int32_t>(ni);
             tf.K = static_cast<int32_t>(ni);
-            tf.flags = kTriKUpTo;
+            tf.flags = kTransB | kTriKUpTo;
             tf.A = Xi;
             tf.lda = nq;
-            tf.B = Ui;
+            tf.B = Li;
             tf.ldb = ni;
             tf.C = Ti;
             tf.ldc = nq;
@@ -218,15 +195,15 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 for (int it = 0; it < cdiv2(nq, kTB); ++it)
                     ftT.push_back({static_cast<int32_t>(ft.size()), it * kTB, jt * kTB, 0});
             ft.push_back(tf);
-            // backward: X_i = T_i U_i^T  (= (L_ii^-T t_i)^T)
+            // backward: X_i = T_i L_ii^-1  (= (L_ii^-T t_i)^T)
             GemmDesc tb{};
             tb.M = nq;
             tb.N = static_cast<int32_t>(ni);
             tb.K = static_cast<int32_t>(ni);
-            tb.flags = kTransB | kTriKFrom;
+            tb.flags = kTriKFrom;
             tb.A = Ti;
             tb.lda = nq;
-            tb.B = Ui;
+            tb.B = Li;
             tb.ldb = ni;
             tb.C = Xi;
             tb.ldc = nq;

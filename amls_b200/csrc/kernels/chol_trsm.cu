@@ -278,6 +278,28 @@ cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* tiles, int nTiles, c
     return cudaGetLastError();
 }
 
+// X[J*64 + r, J*64 + c] = inv[J][r + 64 c] for r, c < the block's size: the
+// diagonal blocks of L^-1 (X n x n, ld ldx), the start of its doubling
+// construction.  One CTA per (descriptor, block).
+__global__ void __launch_bounds__(256) placeDiagInvKernel(const TrsmDesc* __restrict__ descs,
+                                                          const TileRef* __restrict__ tiles) {
+    const TileRef t = tiles[blockIdx.x];
+    const TrsmDesc D = descs[t.desc];
+    const int J = t.m0;
+    const int j0 = J * 64, nb = min(64, D.n - j0);
+    const double* in = D.inv + (int64_t)J * 4096;
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+        const int r = e % 64, c = e / 64;
+        if (r < nb && c < nb) D.X[(j0 + r) + (int64_t)(j0 + c) * D.ldx] = in[r + 64 * c];
+    }
+}
+
+cudaError_t launchPlaceDiagInv(const TrsmDesc* d, const TileRef* tiles, int nTiles, cudaStream_t s) {
+    if (nTiles <= 0) return cudaSuccess;
+    placeDiagInvKernel<<<nTiles, 256, 0, s>>>(d, tiles);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------------
 // row-panel TRSM with 64-row tiles and register tiling:
 //   forward:  X <- X L^-T    backward: X <- X L^-1     (X: r x n)

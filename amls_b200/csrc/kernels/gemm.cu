@@ -91,11 +91,13 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
     // split-K range; triangular B restricts k to <= the tile's last column
-    // (kTriKUpTo) or >= its first column (kTriKFrom)
+    // (kTriKUpTo) or >= its first column (kTriKFrom), triangular A to <= the
+    // tile's last row (kTriAUpTo)
     int kBeg = D.kChunk > 0 ? t.pad * D.kChunk : 0;
     int kEnd = D.kChunk > 0 ? min(D.K, kBeg + D.kChunk) : D.K;
     if (D.flags & kTriKUpTo) kEnd = min(kEnd, n0 + kBN);
     if (D.flags & kTriKFrom) kBeg = max(kBeg, n0);
+    if (D.flags & kTriAUpTo) kEnd = min(kEnd, m0 + kBM);
     const int nSlices = kEnd > kBeg ? (kEnd - kBeg + kKs - 1) / kKs : 0;
 #pragma unroll
     for (int st = 0; st < kStages - 1; ++st) {

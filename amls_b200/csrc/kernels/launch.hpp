@@ -28,6 +28,7 @@ enum GemmFlags : int32_t {
     kAccumulate = 128,  // dense: C = alpha*AB + beta*C ; scatter: *dst += alpha*AB
     kTriKUpTo = 256,    // op(B) upper triangular: column j uses k <= j only
     kTriKFrom = 512,    // op(B) lower triangular: column j uses k >= j only
+    kTriAUpTo = 1024,   // op(A) lower triangular: row i uses k <= i only
 };
 
 struct GemmDesc {
@@ -113,6 +114,9 @@ constexpr int kTrsmRows64 = 64;
 cudaError_t launchTrsmRows64(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
 // inv + 4096*J = (L_JJ)^-1 for the 64x64 diagonal blocks J (TileRef.m0 = J).
 cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
+// X (n x n, ld ldx) diagonal 64 x 64 blocks <- inv blocks (TileRef.m0 = J);
+// the rest of X is left as it is (the caller zeroes it).
+cudaError_t launchPlaceDiagInv(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
 
 // ------------------------------------------------------- eigensolver ----
 // Symmetric tridiagonalisation (Householder), in place.  A (n x n, full
@@ -219,9 +223,6 @@ cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, cons
 // out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
 cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
                          double c, const double* z, double* out, cudaStream_t s);
-// Block b (size[b] x size[b] at pool + off[b], ld size[b]) set to the identity.
-cudaError_t launchIdentityBlocks(double* pool, const int64_t* off, const int64_t* size, int nBlocks,
-                                 cudaStream_t s);
 // out[i] = 1 / in[i]   (reciprocals, for eigenvalue maps)
 cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s);
 

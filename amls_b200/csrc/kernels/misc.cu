@@ -440,23 +440,4 @@ cudaError_t launchSymmetrizeTiles(const FrontDesc* d, const TileRef* tiles, int 
     return cudaGetLastError();
 }
 
-// Identity blocks: block b (n = size[b], at pool + off[b], ld n) = I.
-__global__ void identityBlocksKernel(double* __restrict__ pool, const int64_t* __restrict__ off,
-                                     const int64_t* __restrict__ size) {
-    const int b = blockIdx.y;
-    const int64_t n = size[b];
-    double* A = pool + off[b];
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * n;
-         e += (int64_t)gridDim.x * blockDim.x)
-        A[e] = (e % n == e / n) ? 1.0 : 0.0;
-}
-
-cudaError_t launchIdentityBlocks(double* pool, const int64_t* off, const int64_t* size, int nBlocks,
-                                 cudaStream_t s) {
-    if (nBlocks <= 0) return cudaSuccess;
-    dim3 grid(64, nBlocks);
-    identityBlocksKernel<<<grid, 256, 0, s>>>(pool, off, size);
-    return cudaGetLastError();
-}
-
 }  // namespace amls_b200
