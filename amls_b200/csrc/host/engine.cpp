@@ -457,33 +457,17 @@ void Engine::buildStatic() {
     double* eP = eigPool_.as<double>();
     double* liP = linvPool_.as<double>();
     double* lsP = linvScratch_.as<double>();
-    auto addBatch = [&](const std::vector<GemmDesc>& d, const std::vector<TileRef>& t) {
-        GemmBatch g;
-        g.desc = sblob_.add(d);
-        g.tiles = sblob_.add(t);
-        g.nTiles = static_cast<int>(t.size());
-        return g;
-    };
     for (int l = 0; l <= maxLevel_; ++l) {
         LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
-        std::vector<FrontDesc> fk, fm, fsym;
-        std::vector<TrsmDesc> idd;
-        std::vector<TileRef> rt, ut, it, symT, wT, cT;
+        std::vector<FrontDesc> fsym;
+        std::vector<CholItem> ci;
+        std::vector<TileRef> rt, ut, symT, wT, cT;
         std::vector<GemmDesc> rg, wg, cg;
         std::vector<FrontUpdDesc> ud;
         int64_t maxN = 0, maxRows = 0;
         for (int i : byLevel_[static_cast<size_t>(l)]) {
             const Node& nd = nodes_[static_cast<size_t>(i)];
             const int64_t s = static_cast<int64_t>(nd.S.size());
-            FrontDesc f{};
-            f.F = kP + nd.frontOff;
-            f.ld = nd.ld;
-            f.n = static_cast<int32_t>(nd.n);
-            f.rows = static_cast<int32_t>(nd.ld);
-            f.node = i;
-            fk.push_back(f);
-            f.F = mP + nd.frontOff;
-            fm.push_back(f);
             FrontDesc fe{};
             fe.F = eP + nd.eigOff;
             fe.ld = nd.n;
@@ -495,19 +479,9 @@ void Engine::buildStatic() {
             fsym.push_back(fe);
             maxN = std::max(maxN, nd.n);
             maxRows = std::max(maxRows, nd.ld);
-            double* invP = invPool_.as<double>() + nd.invOff;
             double* linvP = liP + nd.eigOff;
-            // inverses of the 64x64 diagonal blocks of L_ii, placed on the
-            // diagonal of L_ii^-1 (the doubling below completes it)
-            TrsmDesc iv{};
-            iv.L = kP + nd.frontOff;
-            iv.ldl = nd.ld;
-            iv.X = linvP;
-            iv.ldx = nd.n;
-            iv.n = static_cast<int32_t>(nd.n);
-            iv.inv = invP;
-            for (int J = 0; J < cdiv(nd.n, 64); ++J) it.push_back({static_cast<int32_t>(idd.size()), J, 0, 0});
-            idd.push_back(iv);
+            ci.push_back(CholItem{kP + nd.frontOff, nd.ld, nd.n, invPool_.as<double>() + nd.invOff, linvP,
+                                  lsP + nd.eigOff, i});
             // W = G L^-T over all n + s rows of the M front (G L_ii^-T: the
             // reference's Y solves, K^-1 M columns, in transposed form)
             GemmDesc w = gemm(nd.ld, nd.n, nd.n, kTransB | kTriKUpTo, mP + nd.frontOff, nd.ld, linvP, nd.n,
@@ -545,48 +519,12 @@ void Engine::buildStatic() {
                 ud.push_back(u);
             }
         }
-        L.nFront = static_cast<int>(fk.size());
-        L.maxBlocks = cdiv(maxN, kCholBlock);
-        L.maxRowTiles = cdiv(maxRows, kTrsmRows);
-        L.frontK = sblob_.add(fk);
-        L.frontM = sblob_.add(fm);
+        L.chol = buildCholPlan(sblob_, ci);
         L.symDesc = sblob_.add(fsym);
         L.symTiles = sblob_.add(symT);
         L.nSymTiles = static_cast<int>(symT.size());
-        L.invDesc = sblob_.add(idd);
-        L.invTiles = sblob_.add(it);
-        L.nInvTiles = static_cast<int>(it.size());
-        // L_ii^-1 by doubling: with the diagonal blocks of size b complete,
-        // each pair of neighbouring blocks (A = [a0, a1), B = [a1, b1)) gets
-        //   L^-1[B, A] = -L^-1[B, B] (L[B, A] L^-1[A, A])
-        // (two batched GEMMs per step, T in the scratch copy of the layout)
-        L.inv.clear();
-        for (int64_t b = 64; b < maxN; b *= 2) {
-            std::vector<GemmDesc> d1, d2;
-            std::vector<TileRef> t1, t2;
-            for (int i : byLevel_[static_cast<size_t>(l)]) {
-                const Node& nd = nodes_[static_cast<size_t>(i)];
-                const int64_t n = nd.n, ld = nd.ld;
-                const double* Lf = kP + nd.frontOff;
-                double* li = liP + nd.eigOff;
-                double* ls = lsP + nd.eigOff;
-                for (int64_t a0 = 0; a0 + b < n; a0 += 2 * b) {
-                    const int64_t a1 = a0 + b, b1 = std::min(n, a0 + 2 * b);
-                    GemmDesc g1 = gemm(b1 - a1, a1 - a0, a1 - a0, kTriKFrom, Lf + a1 + a0 * ld, ld,
-                                       li + a0 + a0 * n, n, ls + a1 + a0 * n, n, 1.0, 0.0);
-                    gemmTiles(t1, static_cast<int>(d1.size()), b1 - a1, a1 - a0);
-                    d1.push_back(g1);
-                    GemmDesc g2 = gemm(b1 - a1, a1 - a0, b1 - a1, kTriAUpTo, li + a1 + a1 * n, n,
-                                       ls + a1 + a0 * n, n, li + a1 + a0 * n, n, -1.0, 0.0);
-                    gemmTiles(t2, static_cast<int>(d2.size()), b1 - a1, a1 - a0);
-                    d2.push_back(g2);
-                }
-            }
-            L.inv.push_back(addBatch(d1, t1));
-            L.inv.push_back(addBatch(d2, t2));
-        }
-        L.w = addBatch(wg, wT);
-        L.c = addBatch(cg, cT);
+        L.w = addBatch(sblob_, wg, wT);
+        L.c = addBatch(sblob_, cg, cT);
         L.rDesc = sblob_.add(rg);
         L.rTiles = sblob_.add(rt);
         L.nRTiles = static_cast<int>(rt.size());
@@ -630,20 +568,9 @@ void Engine::buildStatic() {
 // elimination
 // ---------------------------------------------------------------------------
 void Engine::eliminate(cudaStream_t s) {
-    int* st = status_.as<int>();
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
-        const FrontDesc* fk = sblob_.dev<FrontDesc>(L.frontK);
-        for (int jb = 0; jb < L.maxBlocks; ++jb) {
-            LAUNCH(launchCholDiag(fk, L.nFront, jb, st, s));
-            LAUNCH(launchCholPanel(fk, L.nFront, jb, L.maxRowTiles, s));
-        }
-        LAUNCH(launchInvDiag(sblob_.dev<TrsmDesc>(L.invDesc), sblob_.dev<TileRef>(L.invTiles),
-                             L.nInvTiles, s));
-        LAUNCH(launchPlaceDiagInv(sblob_.dev<TrsmDesc>(L.invDesc), sblob_.dev<TileRef>(L.invTiles),
-                                  L.nInvTiles, s));
-        for (const GemmBatch& g : L.inv)
-            LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(g.desc), sblob_.dev<TileRef>(g.tiles), g.nTiles, s));
+        runCholPlan(sblob_, L.chol, s);
         LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.w.desc), sblob_.dev<TileRef>(L.w.tiles), L.w.nTiles, s));
         LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.c.desc), sblob_.dev<TileRef>(L.c.tiles), L.c.nTiles, s));
         LAUNCH(launchSymmetrizeTiles(sblob_.dev<FrontDesc>(L.symDesc), sblob_.dev<TileRef>(L.symTiles),

@@ -146,12 +146,26 @@ private:
         size_t desc = 0, tiles = 0;
         int nTiles = 0;
     };
+    static GemmBatch addBatch(Blob& b, const std::vector<GemmDesc>& d, const std::vector<TileRef>& t);
+    // Batched right-looking partial Cholesky with the diagonal-block inverses
+    // and L^-1 (cholesky.cpp).  linv must be zero above the diagonal.
+    struct CholItem {
+        double* F;             // (ld x n) front, factored in place
+        int64_t ld, n;
+        double* inv;           // ceil(n / 64) x 4096 diagonal-block inverses
+        double* linv;          // n x n, ld n: L^-1
+        double* scratch;       // n x n, ld n
+        int node;              // reported with a non-positive pivot
+    };
+    struct CholPlan {
+        size_t fronts = 0, invd = 0, invTiles = 0;
+        int nFront = 0, nInvTiles = 0, nChol = 0;
+        std::vector<GemmBatch> panel, trail, dbl;
+    };
+    static CholPlan buildCholPlan(Blob& b, const std::vector<CholItem>& items);
+    void runCholPlan(const Blob& b, const CholPlan& P, cudaStream_t s);
     struct LevelPlan {
-        size_t frontK = 0, frontM = 0;             // FrontDesc tables
-        int nFront = 0, maxBlocks = 0, maxRowTiles = 0;
-        size_t invDesc = 0, invTiles = 0;           // 64x64 diagonal-block inverses
-        int nInvTiles = 0;
-        std::vector<GemmBatch> inv;                // L^-1 doubling: (T, L^-1 block) per step
+        CholPlan chol;                             // partial Cholesky and L_ii^-1 of the fronts
         GemmBatch w;                               // W = G L^-T (all rows of the front)
         GemmBatch c;                               // C = W_ii^T L^-T
         size_t symDesc = 0, symTiles = 0;          // symmetrize eig matrices
@@ -178,7 +192,7 @@ private:
     std::vector<int64_t> yOff_;                    // per node (doubles into yPool_)
 
     // refinement and the device dense eigensolver
-    DevBuf dgE_, dgY_, dgYt_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
+    DevBuf dgE_, dgY_, dgT_, dgLinv_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
     DevBuf refT_, refMQ_;
     int refineIters_ = 0, refineNq_ = 0;

@@ -41,30 +41,51 @@ int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 // smallest `want` eigenpairs of (K, M), n x n column-major on the device;
 // K and M are overwritten.  w[want] ascending, V (n x want, ld ldv).
+// M = L L^T (blocked Cholesky with L^-1), C = L^-1 K L^-T by two triangular
+// GEMMs, the symmetric tridiagonal eigensolver on C, V = L^-T Y.
 void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, double* V,
                             int64_t ldv, cudaStream_t s) {
     const int64_t nn = n;
     double* E = static_cast<double*>(dgE_.ensure(sizeof(double) * nn * nn));
+    double* T = static_cast<double*>(dgT_.ensure(sizeof(double) * nn * nn));
+    double* Linv = static_cast<double*>(dgLinv_.ensure(sizeof(double) * nn * nn));
     double* Y = static_cast<double*>(dgY_.ensure(sizeof(double) * nn * want));
-    double* Yt = static_cast<double*>(dgYt_.ensure(sizeof(double) * nn * want));
     double* d = static_cast<double*>(dgD_.ensure(sizeof(double) * 3 * nn));
     double* work = static_cast<double*>(dgWork_.ensure(sizeof(double) * 6 * nn * want));
     int* kOut = static_cast<int*>(dgK_.ensure(sizeof(int) * 4));
     double* inv = static_cast<double*>(dgInv_.ensure(sizeof(double) * (size_t)((n + 63) / 64) * 4096));
-    std::vector<TileRef> rowT, rowK, sq, yk, ky, invT;
-    for (int r = 0; r < n; r += kTrsmRows64) rowT.push_back({0, r, 0, 0});
-    for (int r = 0; r < want; r += kTrsmRows64) rowK.push_back({0, r, 0, 0});
-    for (int J = 0; J < (n + 63) / 64; ++J) invT.push_back({0, J, 0, 0});
-    for (int j = 0; j < n; j += 32)
-        for (int i = 0; i < n; i += 32) sq.push_back({0, i, j, 0});
-    for (int j = 0; j < want; j += 32)
-        for (int i = 0; i < n; i += 32) yk.push_back({0, i, j, 0});
-    for (int j = 0; j < n; j += 32)
-        for (int i = 0; i < want; i += 32) ky.push_back({0, i, j, 0});
-    FrontDesc f{M, nn, n, n, -2, 0}, fe{E, nn, n, n, -2, 0};
-    TrsmDesc t1{M, nn, K, nn, n, n, 0, 0, inv}, t2{M, nn, E, nn, n, n, 0, 0, inv},
-        t3{M, nn, Yt, want, n, want, 0, 1, inv};
-    CopyDesc c1{K, nn, E, nn, n, n}, c2{Y, nn, Yt, want, n, want}, c3{Yt, want, V, ldv, want, n};
+    cudaCheck(cudaMemsetAsync(Linv, 0, sizeof(double) * nn * nn, s), "zero");
+    Blob b;
+    const CholPlan P = buildCholPlan(b, {CholItem{M, nn, nn, inv, Linv, T, -2}});
+    std::vector<GemmDesc> g1(1), g2(1), g3(1);
+    std::vector<TileRef> t1, t2, t3;
+    auto set = [](GemmDesc& g, int64_t Mr, int64_t N, int64_t Kd, int flags, const double* A, int64_t lda,
+                  const double* B, int64_t ldb, double* C, int64_t ldc) {
+        g = GemmDesc{};
+        g.M = static_cast<int32_t>(Mr);
+        g.N = static_cast<int32_t>(N);
+        g.K = static_cast<int32_t>(Kd);
+        g.flags = flags;
+        g.A = A;
+        g.lda = lda;
+        g.B = B;
+        g.ldb = ldb;
+        g.C = C;
+        g.ldc = ldc;
+        g.alpha = 1.0;
+    };
+    auto tiles = [](std::vector<TileRef>& t, int64_t Mr, int64_t N) {
+        for (int j = 0; j < cdiv2(N, kT); ++j)
+            for (int i = 0; i < cdiv2(Mr, kT); ++i) t.push_back({0, i * kT, j * kT, 0});
+    };
+    set(g1[0], n, n, n, kTransB | kTriKUpTo, K, nn, Linv, nn, T, nn);              // T = K L^-T
+    tiles(t1, n, n);
+    set(g2[0], n, n, n, kTransA | kTransB | kTriKUpTo, T, nn, Linv, nn, E, nn);    // C = T^T L^-T
+    tiles(t2, n, n);
+    set(g3[0], n, want, n, kTransA, Linv, nn, Y, nn, V, ldv);                       // V = L^-T Y
+    tiles(t3, n, want);
+    const GemmBatch b1 = addBatch(b, g1, t1), b2 = addBatch(b, g2, t2), b3 = addBatch(b, g3, t3);
+    FrontDesc fe{E, nn, n, n, -2, 0};
     EigDesc ed{};
     ed.A = E;
     ed.lda = nn;
@@ -79,11 +100,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     ed.kcap = want;
     ed.kOut = kOut;
     ed.work = work;
-    Blob b;
-    const size_t oF = b.add(&f, 1), oFe = b.add(&fe, 1), oT1 = b.add(&t1, 1), oT2 = b.add(&t2, 1),
-                 oT3 = b.add(&t3, 1), oC1 = b.add(&c1, 1), oC2 = b.add(&c2, 1), oC3 = b.add(&c3, 1),
-                 oE = b.add(&ed, 1), oRow = b.add(rowT), oK = b.add(rowK), oSq = b.add(sq),
-                 oYk = b.add(yk), oKy = b.add(ky), oInvT = b.add(invT);
+    const size_t oFe = b.add(&fe, 1), oE = b.add(&ed, 1);
     std::vector<int> gOf, gFirst{0}, gSize;
     std::vector<int64_t> pOff{0};
     int nCta = 0;
@@ -94,15 +111,9 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     }
     const size_t oGo = b.add(gOf), oGf = b.add(gFirst), oGs = b.add(gSize), oPo = b.add(pOff);
     b.upload(dgBlob_, s);
-    const FrontDesc* dF = b.dev<FrontDesc>(oF);
-    for (int jb = 0; jb * kCholBlock < n; ++jb) {
-        LAUNCH(launchCholDiag(dF, 1, jb, status_.as<int>(), s));
-        LAUNCH(launchCholPanel(dF, 1, jb, cdiv2(n, kTrsmRows), s));
-    }
-    LAUNCH(launchInvDiag(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oInvT), static_cast<int>(invT.size()), s));
-    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT1), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
-    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC1), b.dev<TileRef>(oSq), static_cast<int>(sq.size()), s));
-    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT2), b.dev<TileRef>(oRow), static_cast<int>(rowT.size()), s));
+    runCholPlan(b, P, s);
+    LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b1.desc), b.dev<TileRef>(b1.tiles), b1.nTiles, s));
+    LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b2.desc), b.dev<TileRef>(b2.tiles), b2.nTiles, s));
     LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
     const EigDesc* dE = b.dev<EigDesc>(oE);
     if (n <= 384) LAUNCH(launchTridiagSmall(dE, 1, s));
@@ -114,16 +125,14 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     LAUNCH(launchBisectWarp(dE, 1, 2, want, 0.0, want, s));
     LAUNCH(launchInverseIter(dE, 1, want, nullptr, s));
     LAUNCH(launchBackTransformSmem(dE, 1, want, n, s));
-    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC2), b.dev<TileRef>(oYk), static_cast<int>(yk.size()), s));
-    LAUNCH(launchTrsmRows64(b.dev<TrsmDesc>(oT3), b.dev<TileRef>(oK), static_cast<int>(rowK.size()), s));
-    LAUNCH(launchTransposeBatched(b.dev<CopyDesc>(oC3), b.dev<TileRef>(oKy), static_cast<int>(ky.size()), s));
+    LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b3.desc), b.dev<TileRef>(b3.tiles), b3.nTiles, s));
     // the tables live in dgBlob_ until the stream passes this point
     cudaCheck(cudaStreamSynchronize(s), "dense eigensolve");
     const double nd = n;
     catF_[4] += 4.0 / 3.0 * nd * nd * nd;
     catB_[4] += 8.0 / 3.0 * nd * nd * nd;
     catF_[0] += nd * nd * nd / 3.0;
-    catF_[1] += 2.0 * nd * nd * nd + nd * nd * want;
+    catF_[2] += nd * nd * nd / 3.0 + 2.0 * nd * nd * nd + 2.0 * nd * nd * want;
 }
 
 // Q (nq x n, transposed, permuted order) holds the AMLS Ritz vectors on entry

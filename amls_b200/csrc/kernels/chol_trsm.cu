@@ -238,6 +238,88 @@ cudaError_t launchTrsmRows(const TrsmDesc* d, const TileRef* dTiles, int nTiles,
 
 
 // ------------------------------------------------------------------------
+// right-looking blocked partial Cholesky, 64-wide column blocks: per block J
+// this kernel factors the (already updated) diagonal block in place and
+// writes its inverse; the panel solve (in place, times inv^T) and the
+// trailing SYRK update are batched GEMMs issued by the host.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) cholDiag64Kernel(const FrontDesc* __restrict__ fronts,
+                                                       const TrsmDesc* __restrict__ invd, int J,
+                                                       int* status) {
+    __shared__ double D[64][65];
+    __shared__ int bad;
+    const FrontDesc F = fronts[blockIdx.x];
+    const int j0 = J * 64;
+    if (j0 >= F.n) return;
+    const int nb = min(64, F.n - j0);
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 64 * 64; e += NT) {
+        const int r = e % 64, c = e / 64;
+        D[r][c] = (r < nb && c < nb) ? F.F[(j0 + r) + (int64_t)(j0 + c) * F.ld] : (r == c ? 1.0 : 0.0);
+    }
+    __shared__ double piv[64];
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    // right-looking on the unscaled block, one barrier per column: with
+    // d_k = D[k][k] (a non-positive or NaN pivot counts as 1, as in the
+    // left-looking kernel), D[r][c] -= D[r][k] D[c][k] / d_k for k < c <= r;
+    // thread (r = tid % 64, columns c = tid / 64 + 4 j)
+    const int tr = tid & 63, tc = tid >> 6;
+    for (int k = 0; k < nb; ++k) {
+        double dk = D[k][k];
+        if (!(dk > 0.0) || !isfinite(dk)) {
+            if (tid == 0) bad = 1;
+            dk = 1.0;
+        }
+        if (tid == 0) piv[k] = sqrt(dk);
+        const double rinv = 1.0 / dk;
+        if (tr < nb) {
+            const double lr = D[tr][k] * rinv;
+            for (int c = k + 1 + tc; c <= tr; c += 4) D[tr][c] -= lr * D[c][k];
+        }
+        __syncthreads();
+    }
+    if (bad && tid == 0) setStatus(status, kDevNotSpd, F.node);
+    // scale: L[r][c] = D[r][c] / piv[c] (r > c), L[c][c] = piv[c]
+    for (int e = tid; e < nb * nb; e += NT) {
+        const int r = e % nb, c = e / nb;
+        if (r > c) D[r][c] /= piv[c];
+        else if (r == c) D[r][c] = piv[c];
+    }
+    __syncthreads();
+    for (int e = tid; e < nb * nb; e += NT) {
+        const int r = e % nb, c = e / nb;
+        F.F[(j0 + r) + (int64_t)(j0 + c) * F.ld] = (r >= c) ? D[r][c] : 0.0;
+    }
+    // inverse of the (identity-padded) block: thread c solves L x = e_c
+    if (tid < 64) {
+        const int c = tid;
+        double* out = invd[blockIdx.x].inv + (int64_t)J * 4096;
+        double x[64];
+#pragma unroll
+        for (int r = 0; r < 64; ++r) x[r] = 0.0;
+#pragma unroll
+        for (int r = 0; r < 64; ++r) {
+            if (r >= c) {
+                double v = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+                for (int q = 0; q < r; ++q) v -= D[r][q] * x[q];
+                x[r] = v / D[r][r];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 64; ++r) out[r + 64 * c] = (r < c) ? 0.0 : x[r];
+    }
+}
+
+cudaError_t launchCholDiag64(const FrontDesc* fronts, const TrsmDesc* invd, int nFront, int J,
+                             int* status, cudaStream_t s) {
+    if (nFront <= 0) return cudaSuccess;
+    cholDiag64Kernel<<<nFront, NT, 0, s>>>(fronts, invd, J, status);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
 // inverses of the 64x64 diagonal blocks of a factored L (for trsmRows64)
 // ------------------------------------------------------------------------
 // inv[J] (64 x 64, column-major, lower) = L_JJ^-1 for J = 0 .. ceil(n/64)-1;

@@ -114,6 +114,11 @@ constexpr int kTrsmRows64 = 64;
 cudaError_t launchTrsmRows64(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
 // inv + 4096*J = (L_JJ)^-1 for the 64x64 diagonal blocks J (TileRef.m0 = J).
 cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
+// Right-looking variant, 64-wide blocks: factor the diagonal block J of each
+// front in place (fronts[i]) and write its inverse to invd[i].inv + 4096 J
+// (identity-padded, as launchInvDiag); panel and trailing update are GEMMs.
+cudaError_t launchCholDiag64(const FrontDesc* fronts, const TrsmDesc* invd, int nFront, int J,
+                             int* status, cudaStream_t s);
 // X (n x n, ld ldx) diagonal 64 x 64 blocks <- inv blocks (TileRef.m0 = J);
 // the rest of X is left as it is (the caller zeroes it).
 cudaError_t launchPlaceDiagInv(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
