@@ -19,7 +19,7 @@ namespace amls_b200 {
 
 namespace {
 
-constexpr int kSmallEig = 384;     // tridiagonalise n <= this with one CTA per matrix
+constexpr int kSmallEig = kTridiagSmallMax;   // tridiagonalise n <= this with one CTA per matrix
 constexpr int kT = kGemmTile;      // 64
 
 int cdiv(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }

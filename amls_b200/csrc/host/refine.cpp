@@ -104,7 +104,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     std::vector<int> gOf, gFirst{0}, gSize;
     std::vector<int64_t> pOff{0};
     int nCta = 0;
-    if (n > 384) {
+    if (n > kTridiagSmallMax) {
         nCta = tridiagLargeMaxCtas(n);
         gOf.assign(static_cast<size_t>(nCta), 0);
         gSize.push_back(nCta);
@@ -116,7 +116,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b2.desc), b.dev<TileRef>(b2.tiles), b2.nTiles, s));
     LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
     const EigDesc* dE = b.dev<EigDesc>(oE);
-    if (n <= 384) LAUNCH(launchTridiagSmall(dE, 1, s));
+    if (n <= kTridiagSmallMax) LAUNCH(launchTridiagSmall(dE, 1, s));
     else {
         dgP_.ensure(sizeof(double) * kTridiagPBufs * nn);
         LAUNCH(launchTridiagLargeGroups(dE, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,

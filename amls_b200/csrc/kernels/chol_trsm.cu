@@ -246,7 +246,10 @@ cudaError_t launchTrsmRows(const TrsmDesc* d, const TileRef* dTiles, int nTiles,
 __global__ void __launch_bounds__(NT) cholDiag64Kernel(const FrontDesc* __restrict__ fronts,
                                                        const TrsmDesc* __restrict__ invd, int J,
                                                        int* status) {
-    __shared__ double D[64][65];
+    extern __shared__ double cdSmem[];
+    double (*D)[65] = reinterpret_cast<double (*)[65]>(cdSmem);            // block, then L
+    double (*X)[65] = reinterpret_cast<double (*)[65]>(cdSmem + 64 * 65);  // L^-1
+    __shared__ double piv[64];
     __shared__ int bad;
     const FrontDesc F = fronts[blockIdx.x];
     const int j0 = J * 64;
@@ -256,8 +259,8 @@ __global__ void __launch_bounds__(NT) cholDiag64Kernel(const FrontDesc* __restri
     for (int e = tid; e < 64 * 64; e += NT) {
         const int r = e % 64, c = e / 64;
         D[r][c] = (r < nb && c < nb) ? F.F[(j0 + r) + (int64_t)(j0 + c) * F.ld] : (r == c ? 1.0 : 0.0);
+        X[r][c] = (r == c) ? 1.0 : 0.0;
     }
-    __shared__ double piv[64];
     if (tid == 0) bad = 0;
     __syncthreads();
     // right-looking on the unscaled block, one barrier per column: with
@@ -274,8 +277,23 @@ __global__ void __launch_bounds__(NT) cholDiag64Kernel(const FrontDesc* __restri
         if (tid == 0) piv[k] = sqrt(dk);
         const double rinv = 1.0 / dk;
         if (tr < nb) {
+            // operands staged in registers first: the stores cannot then
+            // serialise the loads of the next columns
             const double lr = D[tr][k] * rinv;
-            for (int c = k + 1 + tc; c <= tr; c += 4) D[tr][c] -= lr * D[c][k];
+            double a[16], b[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int c = k + 1 + tc + 4 * j;
+                if (c <= tr) {
+                    a[j] = D[c][k];
+                    b[j] = D[tr][c];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int c = k + 1 + tc + 4 * j;
+                if (c <= tr) D[tr][c] = b[j] - lr * a[j];
+            }
         }
         __syncthreads();
     }
@@ -291,31 +309,47 @@ __global__ void __launch_bounds__(NT) cholDiag64Kernel(const FrontDesc* __restri
         const int r = e % nb, c = e / nb;
         F.F[(j0 + r) + (int64_t)(j0 + c) * F.ld] = (r >= c) ? D[r][c] : 0.0;
     }
-    // inverse of the (identity-padded) block: thread c solves L x = e_c
-    if (tid < 64) {
-        const int c = tid;
-        double* out = invd[blockIdx.x].inv + (int64_t)J * 4096;
-        double x[64];
+    // X = L^-1 of the identity-padded block, right-looking on unscaled rows:
+    // X[r][c] -= L[r][k] X[k][c] / L[k][k] for r > k, c <= k; rows scaled last
+    for (int k = 0; k < nb; ++k) {
+        const double rinv = 1.0 / D[k][k];
+        if (tr > k && tr < nb) {
+            const double lr = D[tr][k] * rinv;
+            double a[16], b[16];
 #pragma unroll
-        for (int r = 0; r < 64; ++r) x[r] = 0.0;
+            for (int j = 0; j < 16; ++j) {
+                const int c = tc + 4 * j;
+                if (c <= k) {
+                    a[j] = X[k][c];
+                    b[j] = X[tr][c];
+                }
+            }
 #pragma unroll
-        for (int r = 0; r < 64; ++r) {
-            if (r >= c) {
-                double v = (r == c) ? 1.0 : 0.0;
-#pragma unroll
-                for (int q = 0; q < r; ++q) v -= D[r][q] * x[q];
-                x[r] = v / D[r][r];
+            for (int j = 0; j < 16; ++j) {
+                const int c = tc + 4 * j;
+                if (c <= k) X[tr][c] = b[j] - lr * a[j];
             }
         }
-#pragma unroll
-        for (int r = 0; r < 64; ++r) out[r + 64 * c] = (r < c) ? 0.0 : x[r];
+        __syncthreads();
+    }
+    double* out = invd[blockIdx.x].inv + (int64_t)J * 4096;
+    for (int e = tid; e < 64 * 64; e += NT) {
+        const int r = e % 64, c = e / 64;
+        out[r + 64 * c] = (r < nb && c <= r) ? X[r][c] / D[r][r] : (r == c ? 1.0 : 0.0);
     }
 }
 
 cudaError_t launchCholDiag64(const FrontDesc* fronts, const TrsmDesc* invd, int nFront, int J,
                              int* status, cudaStream_t s) {
     if (nFront <= 0) return cudaSuccess;
-    cholDiag64Kernel<<<nFront, NT, 0, s>>>(fronts, invd, J, status);
+    constexpr size_t smem = sizeof(double) * 2 * 64 * 65;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(cholDiag64Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    cholDiag64Kernel<<<nFront, NT, smem, s>>>(fronts, invd, J, status);
     return cudaGetLastError();
 }
 

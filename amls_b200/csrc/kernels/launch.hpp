@@ -142,6 +142,8 @@ struct EigDesc {
     int32_t* kOut;      // number selected (device)
     double* work;       // per-matrix scratch (>= 8n doubles)
 };
+// One CTA per matrix, n <= kTridiagSmallMax.
+constexpr int kTridiagSmallMax = 384;
 cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s);
 // Cooperative multi-CTA tridiagonalisation of a batch of large matrices: the
 // grid is split into CTA groups, group g (CTAs groupFirst[g] ..

@@ -57,71 +57,140 @@ __device__ __forceinline__ HouseholderScalars makeReflector(double alpha, double
 // ------------------------------------------------------------------------
 // tridiagonalisation, one CTA per matrix
 // ------------------------------------------------------------------------
+// The one-CTA form of the fused step of tridiagLargeKernel: per column one
+// read-modify-write pass over the trailing matrix, in which each warp
+// applies step k's rank-2 update to a whole column and dots it with the next
+// reflector (p_{k+1}[j] directly, no atomics), and __syncthreads for the
+// barrier.  n <= kTridiagSmallMax.
 __global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDesc* __restrict__ descs) {
-    extern __shared__ double sm[];
+    __shared__ double v0[kTridiagSmallMax], v1[kTridiagSmallMax], sw[kTridiagSmallMax];
+    __shared__ double p0[kTridiagSmallMax], p1[kTridiagSmallMax];
     __shared__ double red[32];
     const EigDesc D = descs[blockIdx.x];
     const int n = D.n;
     double* A = D.A;
     const int64_t lda = D.lda;
-    double* v = sm;        // n
-    double* p = sm + n;    // n
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    for (int k = 0; k + 2 < n; ++k) {
-        const int m = n - k - 1;
-        double* col = A + (k + 1) + (int64_t)k * lda;
-        double part = 0.0;
-        for (int i = 1 + tid; i < m; i += blockDim.x) part += col[i] * col[i];
-        const double xnorm2 = blockSum(part, red);
-        const double alpha = col[0];
-        const HouseholderScalars h = makeReflector(alpha, xnorm2);
-        for (int i = tid; i < m; i += blockDim.x) v[i] = (i == 0) ? 1.0 : col[i] * h.scale;
-        __syncthreads();
+    const int bd = blockDim.x;
+    double *vcur = v0, *vnext = v1, *p = p0, *pn = p1;
+    if (n <= 2) {
         if (tid == 0) {
-            D.d[k] = A[k + (int64_t)k * lda];
-            D.e[k] = h.beta;
-            D.tau[k] = h.tau;
+            if (n >= 1) D.d[0] = A[0];
+            if (n == 2) {
+                D.e[0] = A[1];
+                D.tau[0] = 0.0;
+                D.d[1] = A[1 + lda];
+            }
         }
-        for (int i = tid; i < m; i += blockDim.x) col[i] = v[i];
-        if (h.tau != 0.0) {
-            double* A22 = A + (k + 1) + (int64_t)(k + 1) * lda;
-            // p = tau * A22 v  (warp per column)
-            for (int j = wid; j < m; j += nw) {
-                const double* cj = A22 + (int64_t)j * lda;
-                double s = 0.0;
-                for (int i = lane; i < m; i += 32) s += cj[i] * v[i];
-                s = warpSum<32>(s);
-                if (lane == 0) p[j] = h.tau * s;
-            }
-            __syncthreads();
-            double pv = 0.0;
-            for (int i = tid; i < m; i += blockDim.x) pv += p[i] * v[i];
-            pv = blockSum(pv, red);
-            const double a2 = -0.5 * h.tau * pv;
-            for (int i = tid; i < m; i += blockDim.x) p[i] += a2 * v[i];   // p := w
-            __syncthreads();
-            for (int j = wid; j < m; j += nw) {
-                double* cj = A22 + (int64_t)j * lda;
-                const double vj = v[j], wj = p[j];
-                for (int i = lane; i < m; i += 32) cj[i] -= v[i] * wj + p[i] * vj;
-            }
+        return;
+    }
+    // reflector 0 and p_0 = tau_0 A22 v_0
+    HouseholderScalars h;
+    {
+        const int m = n - 1;
+        const double* col = A + 1;
+        double part = 0.0;
+        for (int i = 1 + tid; i < m; i += bd) part += col[i] * col[i];
+        h = makeReflector(col[0], blockSum(part, red));
+        for (int i = tid; i < m; i += bd) vcur[i] = (i == 0) ? 1.0 : col[i] * h.scale;
+        __syncthreads();
+        const double* A22 = A + 1 + lda;
+        for (int j = wid; j < m; j += nw) {
+            const double* cj = A22 + (int64_t)j * lda;
+            double sum = 0.0;
+            for (int i = lane; i < m; i += 32) sum += cj[i] * vcur[i];
+            sum = warpSum<32>(sum);
+            if (lane == 0) p[j] = h.tau * sum;
         }
         __syncthreads();
     }
-    if (tid == 0) {
-        if (n >= 2) {
-            D.d[n - 2] = A[(n - 2) + (int64_t)(n - 2) * lda];
-            D.e[n - 2] = A[(n - 1) + (int64_t)(n - 2) * lda];
-            D.tau[n - 2] = 0.0;
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1, m1 = m - 1;
+        double* B = A + (k + 1) + (int64_t)(k + 1) * lda;
+        double pv = 0.0;
+        for (int i = tid; i < m; i += bd) pv += p[i] * vcur[i];
+        pv = blockSum(pv, red);
+        const double a2 = -0.5 * h.tau * pv;
+        for (int i = tid; i < m; i += bd) sw[i] = p[i] + a2 * vcur[i];
+        __syncthreads();
+        const double w0 = sw[0];
+        const double b00 = B[0] - (w0 + w0);
+        const double alpha = B[1] - (vcur[1] * w0 + sw[1]);
+        HouseholderScalars hn{0.0, 0.0, 0.0};
+        if (m1 >= 2) {
+            double part = 0.0;
+            for (int i = 2 + tid; i < m; i += bd) {
+                const double b = B[i] - (vcur[i] * w0 + sw[i]);
+                vnext[i - 1] = b;
+                part += b * b;
+            }
+            hn = makeReflector(alpha, blockSum(part, red));
+            for (int i = 1 + tid; i < m1; i += bd) vnext[i] *= hn.scale;
+            if (tid == 0) vnext[0] = 1.0;
+            __syncthreads();
         }
-        if (n >= 1) D.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda];
+        {
+            double* col = A + (k + 1) + (int64_t)k * lda;
+            for (int i = tid; i < m; i += bd) col[i] = vcur[i];
+            if (tid == 0) {
+                if (k == 0) D.d[0] = A[0];
+                D.e[k] = h.beta;
+                D.tau[k] = h.tau;
+                D.d[k + 1] = b00;
+                if (m1 < 2) {
+                    D.e[k + 1] = alpha;
+                    D.tau[k + 1] = 0.0;
+                    D.d[k + 2] = B[1 + lda] - 2.0 * vcur[1] * sw[1];
+                }
+            }
+        }
+        if (m1 >= 2) {
+            double* C = B + 1 + lda;
+            const double* vp = vcur + 1;
+            const double* wp = sw + 1;
+            const bool upd = h.tau != 0.0;
+            for (int j = wid; j < m1; j += nw) {
+                double* cj = C + (int64_t)j * lda;
+                const double vj = vp[j], wj = wp[j];
+                double sum = 0.0;
+                for (int i0 = 0; i0 < m1; i0 += 256) {
+                    double cv[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const int i = i0 + lane + 32 * t;
+                        cv[t] = i < m1 ? cj[i] : 0.0;
+                    }
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const int i = i0 + lane + 32 * t;
+                        if (i < m1) {
+                            double c = cv[t];
+                            if (upd) {
+                                c -= vp[i] * wj + wp[i] * vj;
+                                cj[i] = c;
+                            }
+                            sum += c * vnext[i];
+                        }
+                    }
+                }
+                sum = warpSum<32>(sum);
+                if (lane == 0) pn[j] = hn.tau * sum;
+            }
+        }
+        h = hn;
+        double* t = vcur;
+        vcur = vnext;
+        vnext = t;
+        t = p;
+        p = pn;
+        pn = t;
+        __syncthreads();
     }
 }
 
 cudaError_t launchTridiagSmall(const EigDesc* d, int nDesc, cudaStream_t s) {
-    // callers guarantee n <= 2048 for this path (2 * 2048 doubles of smem)
     if (nDesc <= 0) return cudaSuccess;
-    tridiagSmallKernel<<<nDesc, kSmallThreads, 2 * 2048 * sizeof(double), s>>>(d);
+    tridiagSmallKernel<<<nDesc, kSmallThreads, 0, s>>>(d);
     return cudaGetLastError();
 }
 
@@ -260,16 +329,24 @@ __global__ void __launch_bounds__(kTridiagLargeThreads) tridiagLargeKernel(Large
                     double* cj = C + (int64_t)j * lda;
                     const double vj = vp[j], wj = wp[j];
                     double sum = 0.0;
-                    if (upd) {
-#pragma unroll 4
-                        for (int i = s0 + lane; i < s1; i += 32) {
-                            const double c = cj[i] - (vp[i] * wj + wp[i] * vj);
-                            cj[i] = c;
+                    // SEG / 32 = 8 loads per lane issued together
+                    double cv[SEG / 32];
+#pragma unroll
+                    for (int t = 0; t < SEG / 32; ++t) {
+                        const int i = s0 + lane + 32 * t;
+                        cv[t] = i < s1 ? cj[i] : 0.0;
+                    }
+#pragma unroll
+                    for (int t = 0; t < SEG / 32; ++t) {
+                        const int i = s0 + lane + 32 * t;
+                        if (i < s1) {
+                            double c = cv[t];
+                            if (upd) {
+                                c -= vp[i] * wj + wp[i] * vj;
+                                cj[i] = c;
+                            }
                             sum += c * vnext[i];
                         }
-                    } else {
-#pragma unroll 4
-                        for (int i = s0 + lane; i < s1; i += 32) sum += cj[i] * vnext[i];
                     }
                     sum = warpSum<32>(sum);
                     if (lane == 0 && hn.tau != 0.0) atomicAdd(pn + j, hn.tau * sum);
