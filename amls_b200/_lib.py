@@ -50,6 +50,7 @@ class Options(C.Structure):
         ("denseProjectedMax", C.c_int64), ("shift", C.c_double), ("numThreads", C.c_int32),
         ("recoverVectors", C.c_int32), ("verbosity", C.c_int32), ("refine", C.c_int32),
         ("refineMaxIter", C.c_int32), ("refineExtra", C.c_int32), ("refineTol", C.c_double),
+        ("precision", C.c_int32),
     ]
 
 

@@ -36,6 +36,7 @@ extern "C" int amls_options_default(amls_options* opt) {
     opt->refineMaxIter = 60;
     opt->refineExtra = -1;
     opt->refineTol = 1e-9;
+    opt->precision = AMLS_PRECISION_FP64;
     return AMLS_OK;
 }
 

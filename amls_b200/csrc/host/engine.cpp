@@ -25,9 +25,9 @@ constexpr int kT = kGemmTile;      // 64
 int cdiv(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 // tiles of a GEMM descriptor (M x N)
-void gemmTiles(std::vector<TileRef>& t, int desc, int64_t M, int64_t N) {
-    for (int j = 0; j < cdiv(N, kT); ++j)
-        for (int i = 0; i < cdiv(M, kT); ++i) t.push_back({desc, i * kT, j * kT, 0});
+void gemmTiles(std::vector<TileRef>& t, int desc, int64_t M, int64_t N, int tile = kT) {
+    for (int j = 0; j < cdiv(N, tile); ++j)
+        for (int i = 0; i < cdiv(M, tile); ++i) t.push_back({desc, i * tile, j * tile, 0});
 }
 
 void trsmTiles(std::vector<TileRef>& t, int desc, int64_t rows) {
@@ -185,6 +185,8 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
         if (kp[r + 1] < kp[r] || mp[r + 1] < mp[r])
             throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "CSR row pointers not monotone");
     }
+    if (opt.precision != AMLS_PRECISION_FP64 && opt.precision != AMLS_PRECISION_MIXED)
+        throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "precision must be AMLS_PRECISION_FP64 or AMLS_PRECISION_MIXED");
     opt_ = opt;
     n_ = n;
     nnzK_ = kp[n];
@@ -486,18 +488,18 @@ void Engine::buildStatic() {
             // reference's Y solves, K^-1 M columns, in transposed form)
             GemmDesc w = gemm(nd.ld, nd.n, nd.n, kTransB | kTriKUpTo, mP + nd.frontOff, nd.ld, linvP, nd.n,
                               gP + nd.frontOff, nd.ld, 1.0, 0.0);
-            gemmTiles(wT, static_cast<int>(wg.size()), nd.ld, nd.n);
+            gemmTiles(wT, static_cast<int>(wg.size()), nd.ld, nd.n, mTile());
             wg.push_back(w);
             // C = L^-1 G_ii^T L^-T = W_ii^T L^-T
             GemmDesc c = gemm(nd.n, nd.n, nd.n, kTransA | kTransB | kTriKUpTo, gP + nd.frontOff, nd.ld, linvP,
                               nd.n, eP + nd.eigOff, nd.n, 1.0, 0.0);
-            gemmTiles(cT, static_cast<int>(cg.size()), nd.n, nd.n);
+            gemmTiles(cT, static_cast<int>(cg.size()), nd.n, nd.n, mTile());
             cg.push_back(c);
             if (s > 0) {
                 // R = Q - L_Si C / 2  (in place in W's lower block)
                 GemmDesc g = gemm(s, nd.n, nd.n, kAccumulate, kP + nd.frontOff + nd.n, nd.ld,
                                   eP + nd.eigOff, nd.n, gP + nd.frontOff + nd.n, nd.ld, -0.5, 1.0);
-                gemmTiles(rt, static_cast<int>(rg.size()), s, nd.n);
+                gemmTiles(rt, static_cast<int>(rg.size()), s, nd.n, mTile());
                 rg.push_back(g);
                 FrontUpdDesc u{};
                 u.s = static_cast<int32_t>(s);
@@ -571,15 +573,22 @@ void Engine::eliminate(cudaStream_t s) {
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
         runCholPlan(sblob_, L.chol, s);
-        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.w.desc), sblob_.dev<TileRef>(L.w.tiles), L.w.nTiles, s));
-        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.c.desc), sblob_.dev<TileRef>(L.c.tiles), L.c.nTiles, s));
+        LAUNCH(launchGemmM(sblob_.dev<GemmDesc>(L.w.desc), sblob_.dev<TileRef>(L.w.tiles), L.w.nTiles, s));
+        LAUNCH(launchGemmM(sblob_.dev<GemmDesc>(L.c.desc), sblob_.dev<TileRef>(L.c.tiles), L.c.nTiles, s));
         LAUNCH(launchSymmetrizeTiles(sblob_.dev<FrontDesc>(L.symDesc), sblob_.dev<TileRef>(L.symTiles),
                                      L.nSymTiles, s));
-        LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(L.rDesc), sblob_.dev<TileRef>(L.rTiles),
+        LAUNCH(launchGemmM(sblob_.dev<GemmDesc>(L.rDesc), sblob_.dev<TileRef>(L.rTiles),
                                  L.nRTiles, s));
         LAUNCH(launchFrontUpdate(sblob_.dev<FrontUpdDesc>(L.uDesc), sblob_.dev<TileRef>(L.uTiles),
                                  L.nUTiles, kPool_.as<double>(), mPool_.as<double>(), s));
     }
+}
+
+// the M-side products of the AMLS approximation: FP64 DMMA or, with
+// AMLS_PRECISION_MIXED, the split-BF16 tcgen05 kernel (tables built with
+// mTile()-sized tiles)
+cudaError_t Engine::launchGemmM(const GemmDesc* d, const TileRef* t, int n, cudaStream_t s) {
+    return mixed() ? launchGemmBatchedMixed(d, t, n, status_.as<int>(), s) : launchGemmBatched(d, t, n, s);
 }
 
 void Engine::checkStatus(const char* phase) {
@@ -592,6 +601,9 @@ void Engine::checkStatus(const char* phase) {
                                               " (input outside the SPD range; shift K)");
     if (h[0] == kDevIterCap)
         throw AmlsError(AMLS_ERR_ITERATION, std::string(phase) + ": iteration cap at " + std::to_string(h[1]));
+    if (h[0] == kDevTimeout)
+        throw AmlsError(AMLS_ERR_TIMEOUT, std::string(phase) + ": tensor-core wait timed out in tile " +
+                                              std::to_string(h[1]));
 }
 
 // ---------------------------------------------------------------------------
@@ -854,7 +866,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                         GemmDesc g = gemm(ck, ni, ni, kTransA | kTransB | kTriKUpTo,
                                           panel + panelOff_[static_cast<size_t>(kk)] + nd.pathPrefix,
                                           nk.pathPrefix, linvI, ni, wti + colPos, Ki, 1.0, 0.0);
-                        gemmTiles(pjT, static_cast<int>(pj.size()), ck, ni);
+                        gemmTiles(pjT, static_cast<int>(pj.size()), ck, ni, mTile());
                         pj.push_back(g);
                     }
                     colPos += ck;
@@ -864,12 +876,12 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                     GemmDesc a = gemm(ki, Ki, ni, kTransA | kTransB | kScatter, Yi, ni, wti, Ki, cred, p, 1.0, 0.0);
                     a.rowIdx = dNR + oNodeRow[static_cast<size_t>(i)];
                     a.colOff = dDC + oDescCol[static_cast<size_t>(i)];
-                    gemmTiles(g1T, static_cast<int>(g1.size()), ki, Ki);
+                    gemmTiles(g1T, static_cast<int>(g1.size()), ki, Ki, mTile());
                     g1.push_back(a);
                     GemmDesc a2 = gemm(Ki, ki, ni, kScatter, wti, Ki, Yi, ni, cred, p, 1.0, 0.0);
                     a2.rowIdx = dDR + oDescRow[static_cast<size_t>(i)];
                     a2.colOff = dNC + oNodeCol[static_cast<size_t>(i)];
-                    gemmTiles(g2T, static_cast<int>(g2.size()), Ki, ki);
+                    gemmTiles(g2T, static_cast<int>(g2.size()), Ki, ki, mTile());
                     g2.push_back(a2);
                     fc += 4.0 * ki * Ki * ni;
                 }
@@ -878,7 +890,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                                       wti, Ki, panel, 0, -1.0, 0.0);
                     m.rowIdx = rowSDev_ + nd.rowS;
                     m.colOff = dPC + oPanelCol[static_cast<size_t>(i)];
-                    gemmTiles(midT, static_cast<int>(mid.size()), si, Ki);
+                    gemmTiles(midT, static_cast<int>(mid.size()), si, Ki, mTile());
                     mid.push_back(m);
                     fc += 2.0 * si * Ki * ni;
                 }
@@ -887,14 +899,14 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                 GemmDesc a = gemm(si, ki, ni, kScatter, G + nd.frontOff + ni, nd.ld, Yi, ni, panel, 0, 1.0, 0.0);
                 a.rowIdx = rowSDev_ + nd.rowS;
                 a.colOff = dIC + oInitCol[static_cast<size_t>(i)];
-                gemmTiles(i1T, static_cast<int>(i1.size()), si, ki);
+                gemmTiles(i1T, static_cast<int>(i1.size()), si, ki, mTile());
                 i1.push_back(a);
                 GemmDesc a2 = gemm(si, ki, ni, kScatter | kAccumulate | kColScale, F + nd.frontOff + ni, nd.ld, Yi,
                                    ni, panel, 0, -0.5, 0.0);
                 a2.rowIdx = rowSDev_ + nd.rowS;
                 a2.colOff = dIC + oInitCol[static_cast<size_t>(i)];
                 a2.colScale = wDev + P.projOff[static_cast<size_t>(i)];
-                gemmTiles(i2T, static_cast<int>(i2.size()), si, ki);
+                gemmTiles(i2T, static_cast<int>(i2.size()), si, ki, mTile());
                 i2.push_back(a2);
                 fc += 4.0 * si * ki * ni;
             }
@@ -924,12 +936,12 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     LAUNCH(launchSetDiagonal(cred, wDev, p, s));
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelTabs& T = tabs[static_cast<size_t>(l)];
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.pjD), b.dev<TileRef>(T.pjT), T.npjT, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.ng1T, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.ng2T, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.midD), b.dev<TileRef>(T.midT), T.nmidT, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i1D), b.dev<TileRef>(T.i1T), T.ni1T, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.i2D), b.dev<TileRef>(T.i2T), T.ni2T, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.pjD), b.dev<TileRef>(T.pjT), T.npjT, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.ng1T, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.ng2T, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.midD), b.dev<TileRef>(T.midT), T.nmidT, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.i1D), b.dev<TileRef>(T.i1T), T.ni1T, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.i2D), b.dev<TileRef>(T.i2T), T.ni2T, s));
     }
     // ledger (local eig: bisection + inverse iteration + back-transform;
     // tridiagonalisation counted once per solve)
@@ -1047,16 +1059,16 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
             GemmDesc a = gemm(m, ni, ki, kTransA | kTransB | kRowScale, V + P.projOff[static_cast<size_t>(i)], P.p,
                               Y + yOff_[static_cast<size_t>(i)], std::max<int64_t>(ni, 1), ui, m, 1.0, 0.0);
             a.rowScale = sqrtTheta_.as<double>();
-            gemmTiles(g1T, static_cast<int>(g1.size()), m, ni);
+            gemmTiles(g1T, static_cast<int>(g1.size()), m, ni, mTile());
             g1.push_back(a);
             if (si > 0) {
                 GemmDesc c = gemm(m, ni, si, kGatherA | kAccumulate, zt, m, F + nd.frontOff + ni, nd.ld, ui, m, -1.0, 1.0);
                 c.aMap = sIdxDev_ + nd.mapCol;
-                gemmTiles(g2T, static_cast<int>(g2.size()), m, ni);
+                gemmTiles(g2T, static_cast<int>(g2.size()), m, ni, mTile());
                 g2.push_back(c);
             }
             GemmDesc t = gemm(m, ni, ni, kTriKFrom, ui, m, linvPool_.as<double>() + nd.eigOff, ni, zi, m, 1.0, 0.0);
-            gemmTiles(tT, static_cast<int>(tr.size()), m, ni);
+            gemmTiles(tT, static_cast<int>(tr.size()), m, ni, mTile());
             tr.push_back(t);
             fb += 2.0 * m * ni * (ki + si) + static_cast<double>(m) * ni * ni;
         }
@@ -1069,9 +1081,9 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
     b.upload(passBlob_, s);
     for (int l = maxLevel_; l >= 0; --l) {
         const Tabs& T = tabs[static_cast<size_t>(l)];
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.n1, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.g1D), b.dev<TileRef>(T.g1T), T.n1, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.g2D), b.dev<TileRef>(T.g2T), T.n2, s));
+        LAUNCH(launchGemmM(b.dev<GemmDesc>(T.tD), b.dev<TileRef>(T.tT), T.nt, s));
     }
     catF_[2] += fb;
     catB_[2] += 8.0 * 3.0 * m * static_cast<double>(n_);

@@ -105,6 +105,9 @@ private:
                         cudaStream_t s);
     int refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s);
     void checkStatus(const char* phase);
+    bool mixed() const { return opt_.precision == AMLS_PRECISION_MIXED; }
+    int mTile() const { return mixed() ? kGemmTileMixed : kGemmTile; }
+    cudaError_t launchGemmM(const GemmDesc* d, const TileRef* t, int n, cudaStream_t s);
     // generic selected-eigenpair driver over prepared EigDesc tables
     void selectEigen(std::vector<EigDesc>& descs, int mode, int want, double thr, bool tridiag,
                      cudaStream_t s);

@@ -13,6 +13,7 @@ enum DevStatus : int {
     kDevOk = 0,
     kDevNotSpd = 1,      // non-positive or NaN pivot
     kDevIterCap = 2,     // iteration cap reached
+    kDevTimeout = 3,     // a bounded wait on the tensor cores ran out
 };
 
 // ---------------------------------------------------------------- GEMM --
@@ -59,6 +60,12 @@ constexpr int kGemmTile = 64;
 
 cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
                               cudaStream_t s);
+// Mixed precision (gemm_mixed.cu): the same descriptors on tcgen05 with the
+// operands split into BF16 pairs (3 products, FP32 accumulation, relative
+// error ~2^-16), 128 x 128 tiles (TileRef m0/n0 multiples of 128).
+constexpr int kGemmTileMixed = 128;
+cudaError_t launchGemmBatchedMixed(const GemmDesc* dDescs, const TileRef* dTiles, int nTiles,
+                                   int* status, cudaStream_t s);
 
 // Extend-add update of one eliminated front (multifrontal form of the
 // reference's Schur + congruence updates):

@@ -37,6 +37,9 @@ class AmlsOptions:
     refineMaxIter: int = 60
     refineExtra: int = -1
     refineTol: float = 1e-9
+    # "fp64" or "mixed" (M-side AMLS products on the BF16 tensor cores, split
+    # operands; not in the reference)
+    precision: str = "fp64"
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -56,6 +59,9 @@ class AmlsOptions:
         o.refineMaxIter = int(self.refineMaxIter)
         o.refineExtra = int(self.refineExtra)
         o.refineTol = float(self.refineTol)
+        if self.precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {self.precision!r}")
+        o.precision = 0 if self.precision == "fp64" else 1
         return o
 
 

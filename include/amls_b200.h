@@ -65,7 +65,20 @@ typedef struct amls_options {
     int32_t refineExtra;        /* extra subspace vectors beyond nev; -1 = nev/2 + 16 */
     double refineTol;           /* 1e-9: target relative eigenvalue error, estimated
                                    from the geometric contraction of the Ritz values */
+    /* Arithmetic of the M-side products of the AMLS approximation (no
+     * counterpart in the reference, which is FP64 throughout):
+     * AMLS_PRECISION_FP64 (0): every product in FP64 on the FP64 tensor
+     * cores; AMLS_PRECISION_MIXED (1): the M congruence (G L^-T, C, R), the
+     * projection and the back-transform products on the BF16 tensor cores
+     * with each FP64 operand split into two BF16 parts (three products, FP32
+     * accumulation, relative error ~2^-16).  The factorisation of K, its
+     * Schur updates, the eigensolvers and the refinement stay FP64, so the
+     * refined eigenpairs reach the same accuracy. */
+    int32_t precision;          /* 0    */
 } amls_options;
+
+#define AMLS_PRECISION_FP64 0
+#define AMLS_PRECISION_MIXED 1
 
 /* slots of the timing array filled by amls_solve (seconds) */
 #define AMLS_T_PARTITION 0     /* METIS + permutation + symbolic analysis (host) */

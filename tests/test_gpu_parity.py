@@ -203,3 +203,57 @@ def test_c5_refined_matches_exact(solver):
     sol = solver.solve(p.K, p.M, AmlsOptions(nev=500, nLevels=8, leafSize=500, refine=3,
                                              recoverVectors=False))
     assert rel_err(sol.theta, g[:500]) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["hex8_8", "hex27_4"])
+def test_mixed_precision_amls_close_to_fp64(solver, case):
+    """Mixed precision (M-side AMLS products on the BF16 tensor cores with
+    split operands, relative error ~2^-16 per product): the AMLS Ritz values
+    move by far less than the AMLS truncation error itself."""
+    if case == "hex8_8":
+        p = cases.hex_pencil(8, 8, 8, 1, seed=5)
+        o = dict(nev=40, nLevels=4, leafSize=200)
+    else:
+        p = cases.hex_pencil(4, 4, 4, 2, seed=6)
+        o = dict(nev=30, nLevels=4, leafSize=200)
+    wr, _ = R.LapackDense.solve_all(p.K.toarray(), p.M.toarray())
+    f64 = solver.solve(p.K, p.M, AmlsOptions(**o))
+    mix = solver.solve(p.K, p.M, AmlsOptions(precision="mixed", **o))
+    assert f64.p == mix.p
+    trunc = rel_err(f64.theta, wr[:o["nev"]])
+    assert rel_err(mix.theta, f64.theta) < 1e-3 * max(trunc, 1e-6) + 1e-4
+
+
+@pytest.mark.parametrize("case", ["hex8_8", "hex27_4"])
+def test_mixed_precision_refined_reaches_exact(solver, case):
+    """Mixed precision followed by the FP64 refinement: eigenvalues within
+    1e-8 relative of dense LAPACK dsygvd, M-normalised vectors."""
+    if case == "hex8_8":
+        p = cases.hex_pencil(8, 8, 8, 1, seed=5)
+        o = dict(nev=40, nLevels=4, leafSize=200)
+    else:
+        p = cases.hex_pencil(4, 4, 4, 2, seed=6)
+        o = dict(nev=30, nLevels=4, leafSize=200)
+    wr, _ = R.LapackDense.solve_all(p.K.toarray(), p.M.toarray())
+    sol = solver.solve(p.K, p.M, AmlsOptions(precision="mixed", refine=3, **o))
+    assert rel_err(sol.theta, wr[:o["nev"]]) < 1e-8
+    assert residuals(p.K, p.M, sol.theta, sol.Z).max() < 1e-6
+    mn = np.einsum("ij,ij->j", sol.Z, p.M @ sol.Z)
+    assert np.allclose(mn, 1.0, atol=1e-12)
+
+
+def test_c5_mixed_refined_matches_exact(solver):
+    """Full-size workload, mixed precision + FP64 refinement: all 500
+    eigenvalues within 1e-8 relative of the exact golden."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c5_exact.npz"))["theta"]
+    p = cases.config_pencil("C5", seed=0)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=500, nLevels=8, leafSize=500, refine=3,
+                                             precision="mixed", recoverVectors=False))
+    assert rel_err(sol.theta, g[:500]) < 1e-8
+
+
+def test_invalid_precision(solver):
+    p = cases.hex_pencil(3, 3, 3, 1, seed=1)
+    with pytest.raises(ValueError):
+        solver.solve(p.K, p.M, AmlsOptions(nev=5, nLevels=2, precision="fp16"))
