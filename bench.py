@@ -24,6 +24,7 @@ oracle/workmodel.py.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -49,10 +50,13 @@ REFINE = 3          # K^-1 M applications per Rayleigh-Ritz step (Chebyshev degr
 REFINE_TOL = 1e-9   # target relative eigenvalue error
 
 
-def workload(name, refine=True):
+def workload(name, refine=True, precision="mixed"):
     c = CONFIGS[name]
+    prec = ("mixed: M-side AMLS products (congruence G L^-T, C, R; projection; back-transform) "
+            "on tcgen05 with BF16 split operands, everything else FP64 (DMMA tensor cores)"
+            if precision == "mixed" else "fp64 (DMMA tensor cores)")
     return dict(workload=c["workload"], nev=c["nev"], nLevels=c["nLevels"], leafSize=500, eta=2.0,
-                seed=0, precision="fp64",
+                seed=0, precision=prec,
                 refinement=(f"FP64 Chebyshev-filtered subspace iteration with the elimination's "
                             f"K factor, {REFINE} K^-1M applications per Rayleigh-Ritz, target "
                             f"{REFINE_TOL:g}") if refine else "none",
@@ -139,7 +143,8 @@ def run_ours(args, rank, world, dist):
     p = cases.config_pencil(args.config, seed=0)
     n, nev = p.n, cfg["nev"]
     opt = AmlsOptions(nev=nev, nLevels=cfg["nLevels"], leafSize=500, thresholdFactor=2.0,
-                      verbosity=0, refine=0 if args.no_refine else REFINE, refineTol=REFINE_TOL)
+                      verbosity=0, refine=0 if args.no_refine else REFINE, refineTol=REFINE_TOL,
+                      precision=args.precision)
     s = AmlsSolver(dev)
     s.analyze(p.K, p.M, opt)
     kv = torch.from_numpy(np.ascontiguousarray(p.K.data)).cuda()
@@ -191,13 +196,41 @@ def run_ours(args, rank, world, dist):
         accuracy["median_rel_err_vs_exact"] = float(np.median(np.abs(th - ex) / ex))
         accuracy["exact_reference"] = ("shift-invert Lanczos (scipy ARPACK, sigma 0, tol 1e-13), "
                                        "tests/golden/c5_exact.npz")
+    # the other precision arm, same protocol (the metric compares the two)
+    other = None
+    if not args.no_compare:
+        oprec = "fp64" if args.precision == "mixed" else "mixed"
+        s3 = AmlsSolver(dev)
+        s3.analyze(p.K, p.M, dataclasses.replace(opt, precision=oprec))
+
+        def step3():
+            return s3.solve_values(kv.data_ptr(), mv.data_ptr(), True, theta.data_ptr(),
+                                   Z.data_ptr(), True)
+        for _ in range(args.warmup):
+            step3()
+        t3 = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t3.append(step3()["device"])
+        o_step = float(np.mean(t3))
+        if dist:
+            tt = torch.tensor([o_step], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            o_step = float(tt.item())
+        other = {"precision": oprec, "s": o_step}
+        if args.config == "C5" and os.path.exists(gold):
+            th3 = theta.cpu().numpy()
+            other["max_rel_err_vs_exact"] = float(np.max(np.abs(th3 - ex) / ex))
+        other["speedup_of_" + args.precision] = o_step / t_step
+        s3.close()
     # the AMLS solve alone, for context (not at the metric's accuracy)
     s.set_profiling(False)
     amls_only = None
     if not args.no_refine:
         s2 = AmlsSolver(dev)
         s2.analyze(p.K, p.M, AmlsOptions(nev=nev, nLevels=cfg["nLevels"], leafSize=500,
-                                         thresholdFactor=2.0, verbosity=0))
+                                         thresholdFactor=2.0, verbosity=0, precision=args.precision))
         tt = []
         for k in range(2):
             r2 = s2.solve_values(kv.data_ptr(), mv.data_ptr(), True, theta.data_ptr(),
@@ -254,9 +287,10 @@ def run_ours(args, rank, world, dist):
     line = {
         "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+bf16x3" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded hex-elasticity pencil)",
-        "config": dict(workload(args.config, not args.no_refine),
+        "config": dict(workload(args.config, not args.no_refine, args.precision),
                        parallelism="replicas" if world > 1 else "single GPU",
                        p_final=info["p"], p_passA=info["p_passA"], tree_nodes=info["tree_nodes"]),
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": int(h2d),
@@ -270,6 +304,7 @@ def run_ours(args, rank, world, dist):
         "accuracy": accuracy,
         "amls_only_s": amls_only,
         "refine_iters": info.get("refine_iters"),
+        "other_precision": other,
         "sensitivities": sens,
     }
     if rank == 0 and world == 1 and not args.no_cpu and args.config == "C5":
@@ -303,7 +338,8 @@ def dominant_roofline(cat, ms, launches, work, info, pk, src, s):
     tensor_bound = cat in ("gemm", "front_update", "cholesky", "trsm")
     if tensor_bound:
         peak = fp64_gemm_peak()
-        psrc = "measured in this run: cuBLAS DGEMM 8192^3 (FP64 has no tcgen05 kind)"
+        psrc = ("measured in this run: cuBLAS DGEMM 8192^3 (the FP64 products run on the DMMA "
+                "tensor path; FP64 has no tcgen05 kind)")
         ach = flops / t / 1e12 if t > 0 else 0.0
         return {"bound": "tensor", "kernel": cat, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                 "frac": ach / peak, "traffic": None, "peak_source": psrc,
@@ -405,6 +441,9 @@ def main():
                     help="workload (C5 is the benchmark; smaller ones for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="arm timed as `value` (the other one is timed beside it)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the other precision arm")
     ap.add_argument("--no-refine", action="store_true",
                     help="time the AMLS solve alone (not at the metric's accuracy)")
     args = ap.parse_args()
