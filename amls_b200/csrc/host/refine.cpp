@@ -112,6 +112,14 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     const size_t oGo = b.add(gOf), oGf = b.add(gFirst), oGs = b.add(gSize), oPo = b.add(pOff);
     b.upload(dgBlob_, s);
     runCholPlan(b, P, s);
+    {
+        // a breakdown of the Cholesky of M (status kDevNotSpd) ends the call:
+        // the caller reads the status word
+        int st[2] = {0, 0};
+        cudaCheck(cudaMemcpyAsync(st, status_.as<int>(), sizeof(st), cudaMemcpyDeviceToHost, s), "status");
+        cudaCheck(cudaStreamSynchronize(s), "dense eigensolve");
+        if (st[0] == kDevNotSpd) return;
+    }
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b1.desc), b.dev<TileRef>(b1.tiles), b1.nTiles, s));
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b2.desc), b.dev<TileRef>(b2.tiles), b2.nTiles, s));
     LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
@@ -341,7 +349,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         catF_[2] += fsolve;
     };
     // Chebyshev recurrence buffers (degree = refine - 1)
-    const int cheb = std::max(0, opt_.refine - 1);
+    int cheb = std::max(0, opt_.refine - 1);
     double* Y1 = cheb >= 1 ? static_cast<double*>(refY1_.ensure(sizeof(double) * sz)) : nullptr;
     double* Y2 = cheb >= 2 ? static_cast<double*>(refY2_.ensure(sizeof(double) * sz)) : nullptr;
     std::vector<double> prev(theta.begin(), theta.end());
@@ -379,8 +387,23 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
         denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
         std::vector<double> th(static_cast<size_t>(nq));
+        int st[2] = {0, 0};
         cudaCheck(cudaMemcpyAsync(th.data(), wd, sizeof(double) * nq, cudaMemcpyDeviceToHost, s), "theta");
+        cudaCheck(cudaMemcpyAsync(st, status_.as<int>(), sizeof(st), cudaMemcpyDeviceToHost, s), "status");
         cudaCheck(cudaStreamSynchronize(s), "refine");
+        if (st[0] == kDevNotSpd && cheb > 0) {
+            // The filter amplifies low modes by up to C_c(2 theta_max / theta_1 - 1):
+            // a trace of them in a high column can take the column over, and
+            // the filtered block loses rank (Cholesky of Mc breaks down).  Q
+            // is unchanged until the update below, so redo the iteration
+            // with a lower degree, and keep that degree from now on.
+            --cheb;
+            cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
+            if (opt_.verbosity > 1)
+                std::fprintf(stderr, "[amls_b200] refine: filtered block lost rank, degree now %d\n", cheb);
+            --it;
+            continue;
+        }
         catF_[2] += 2.0 * 2.0 * dn * dq * dq;
         catB_[2] += 8.0 * (3.0 * dn * dq);
         // error estimate per wanted value: change * r / (1 - r), r the observed

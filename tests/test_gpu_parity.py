@@ -205,6 +205,18 @@ def test_c5_refined_matches_exact(solver):
     assert rel_err(sol.theta, g[:500]) < 1e-8
 
 
+def test_c5_refined_high_filter_degree(solver):
+    """A degree-4 Chebyshev filter (refine = 5) makes the filtered block of
+    the full-size workload lose rank; the refinement lowers the degree and
+    still reaches the exact eigenvalues."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c5_exact.npz"))["theta"]
+    p = cases.config_pencil("C5", seed=0)
+    sol = solver.solve(p.K, p.M, AmlsOptions(nev=500, nLevels=8, leafSize=500, refine=5,
+                                             recoverVectors=False))
+    assert rel_err(sol.theta, g[:500]) < 1e-8
+
+
 @pytest.mark.parametrize("case", ["hex8_8", "hex27_4"])
 def test_mixed_precision_amls_close_to_fp64(solver, case):
     """Mixed precision (M-side AMLS products on the BF16 tensor cores with
