@@ -928,7 +928,11 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     for (const Node& nd : nodes_) maxNodeN = std::max<int>(maxNodeN, static_cast<int>(nd.n));
     LAUNCH(launchBisectWarp(dd, N, mode == 0 ? 0 : 1, want, thr, maxK, s));
     LAUNCH(launchInverseIter(dd, N, maxK, nullptr, s));
-    LAUNCH(launchBackTransformSmem(dd, N, maxK, maxNodeN, s));
+    LAUNCH(launchBackTransformSmem(dd, N, maxK, std::min(maxNodeN, kTridiagSmallMax), s));
+    {
+        std::vector<int> kv(P.k.begin(), P.k.end());
+        backTransformBig(descs, kv, s);
+    }
 
     // ---- projection ----
     LAUNCH(launchZero(panel, panelTot, s));
@@ -1008,7 +1012,8 @@ int Engine::reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors) {
     LAUNCH(launchBisectWarp(dd, 1, 0, want, 0.0, want, s));
     if (vectors) {
         LAUNCH(launchInverseIter(dd, 1, want, nullptr, s));
-        LAUNCH(launchBackTransformSmem(dd, 1, want, static_cast<int>(p), s));
+        if (p <= kSmallEig) LAUNCH(launchBackTransformSmem(dd, 1, want, static_cast<int>(p), s));
+        else backTransformBig({e}, {want}, s);
     }
     std::vector<double> nu(static_cast<size_t>(want));
     cudaCheck(cudaMemcpyAsync(nu.data(), redW_.as<double>(), sizeof(double) * want, cudaMemcpyDeviceToHost, s), "theta");

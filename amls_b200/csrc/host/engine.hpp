@@ -103,6 +103,9 @@ private:
     void finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s);
     void denseGenEigDev(double* K, double* M, int n, int want, double* w, double* V, int64_t ldv,
                         cudaStream_t s);
+    // Y <- Q Y for the matrices of `descs` with n > kTridiagSmallMax (k[i]
+    // vectors each) by compact-WY blocks (eig_wy.cpp)
+    void backTransformBig(const std::vector<EigDesc>& descs, const std::vector<int>& k, cudaStream_t s);
     int refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s);
     void checkStatus(const char* phase);
     bool mixed() const { return opt_.precision == AMLS_PRECISION_MIXED; }
@@ -198,6 +201,7 @@ private:
     DevBuf dgE_, dgY_, dgT_, dgLinv_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
     DevBuf refT_, refMQ_;
+    DevBuf wyS_, wyW_, wyBlob_;                    // blocked back-transform
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;

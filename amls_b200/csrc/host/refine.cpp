@@ -132,7 +132,8 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     }
     LAUNCH(launchBisectWarp(dE, 1, 2, want, 0.0, want, s));
     LAUNCH(launchInverseIter(dE, 1, want, nullptr, s));
-    LAUNCH(launchBackTransformSmem(dE, 1, want, n, s));
+    if (n <= kTridiagSmallMax) LAUNCH(launchBackTransformSmem(dE, 1, want, n, s));
+    else backTransformBig({ed}, {want}, s);
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b3.desc), b.dev<TileRef>(b3.tiles), b3.nTiles, s));
     // the tables live in dgBlob_ until the stream passes this point
     cudaCheck(cudaStreamSynchronize(s), "dense eigensolve");

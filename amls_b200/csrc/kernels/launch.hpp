@@ -175,8 +175,20 @@ cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int* status
                               cudaStream_t s);
 // Y <- Q Y with Q = H_0 ... H_{n-3} (back-transform of tridiagonal vectors).
 cudaError_t launchBackTransform(const EigDesc* d, int nDesc, int maxK, cudaStream_t s);
-// Same with columns and reflectors staged in shared memory (maxN = largest n).
+// Same with columns and reflectors staged in shared memory; matrices with
+// n > maxN are skipped (they go through the blocked form below).
 cudaError_t launchBackTransformSmem(const EigDesc* d, int nDesc, int maxK, int maxN, cudaStream_t s);
+// Blocked back-transform pieces (matrices with n > kTridiagSmallMax): zero
+// the upper triangle (diagonal included) of each A so its reflector columns
+// form a unit lower trapezoidal V; T factors of 64-reflector blocks.
+struct WyBlock {
+    const double* tau;     // first tau of the block
+    const double* S;       // V^T V, 64 x 64 (ld 64)
+    double* T;             // out: 64 x 64 upper triangular (ld 64)
+    int32_t nb, pad;       // reflectors in the block (<= 64)
+};
+cudaError_t launchZeroUpper(const EigDesc* d, int nDesc, cudaStream_t s);
+cudaError_t launchWyT(const WyBlock* blocks, int nBlocks, cudaStream_t s);
 // Bisection with one warp per eigenvalue (32-point multisection per round).
 cudaError_t launchBisectWarp(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
                              cudaStream_t s);

@@ -740,10 +740,11 @@ __global__ void __launch_bounds__(256) backTransformSmemKernel(const EigDesc* __
     extern __shared__ double sb[];
     const int b = blockIdx.y;
     const EigDesc D = descs[b];
+    const int n = D.n;
+    if (n > maxN) return;             // larger matrices go through the blocked form
     const int k = *D.kOut;
     const int c0 = blockIdx.x * cols;
     if (c0 >= k) return;
-    const int n = D.n;
     const int nc = min(cols, k - c0);
     double* sv = sb;                  // maxN
     double* sy = sb + maxN;           // cols x maxN
@@ -787,6 +788,54 @@ cudaError_t launchBackTransformSmem(const EigDesc* d, int nDesc, int maxK, int m
     if (e != cudaSuccess) return e;
     dim3 grid((maxK + cols - 1) / cols, nDesc);
     backTransformSmemKernel<<<grid, 256, smem, s>>>(d, cols, maxN);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// blocked (compact WY) back-transform, for the matrices above the one-CTA
+// size: Q = H_0 ... H_{n-3} = B_0 ... B_last with B_j = I - V_j T_j V_j^T
+// over 64 reflectors; the host applies the blocks with GEMMs.
+// ------------------------------------------------------------------------
+// zero A[i, j] for i <= j: the reflector columns become unit lower
+// trapezoidal (v_k[0] = 1 at row k + 1) with zeros above
+__global__ void zeroUpperKernel(const EigDesc* __restrict__ descs) {
+    const EigDesc D = descs[blockIdx.y];
+    for (int j = blockIdx.x; j < D.n; j += gridDim.x)
+        for (int i = threadIdx.x; i <= j; i += blockDim.x) D.A[i + (int64_t)j * D.lda] = 0.0;
+}
+
+cudaError_t launchZeroUpper(const EigDesc* d, int nDesc, cudaStream_t s) {
+    if (nDesc <= 0) return cudaSuccess;
+    zeroUpperKernel<<<dim3(64, nDesc), 256, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+// T (upper triangular, ld 64) of one block from S = V^T V (ld 64) and tau
+// (LAPACK dlarft, forward, columnwise): T[i][i] = tau_i,
+// T[0:i, i] = -tau_i T[0:i, 0:i] S[0:i, i].
+__global__ void __launch_bounds__(64) wyTKernel(const WyBlock* __restrict__ blocks) {
+    const WyBlock B = blocks[blockIdx.x];
+    __shared__ double z[64];
+    const int r = threadIdx.x, nb = B.nb;
+    for (int e = r; e < 64 * 64; e += 64) B.T[e] = 0.0;
+    __syncthreads();
+    for (int i = 0; i < nb; ++i) {
+        const double ti = B.tau[i];
+        if (r < i) z[r] = -ti * B.S[r + 64 * i];
+        __syncthreads();
+        if (r < i) {
+            double acc = 0.0;
+            for (int q = r; q < i; ++q) acc += B.T[r + 64 * q] * z[q];
+            B.T[r + 64 * i] = acc;
+        }
+        if (r == i) B.T[i + 64 * i] = ti;
+        __syncthreads();
+    }
+}
+
+cudaError_t launchWyT(const WyBlock* blocks, int nBlocks, cudaStream_t s) {
+    if (nBlocks <= 0) return cudaSuccess;
+    wyTKernel<<<nBlocks, 64, 0, s>>>(blocks);
     return cudaGetLastError();
 }
 
