@@ -520,14 +520,16 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
         if (tid == 0) D.Y[0 + (int64_t)j * D.ldy] = 1.0;
         return;
     }
-    // scratch: a, b(super), c(sub), dd(2nd super), y, piv  (6n doubles)
+    // scratch: a, b(super), c(sub), dd(2nd super), 1/a (guarded), piv  (6n doubles)
     double* W = D.work + (int64_t)j * 6 * n;
     double* a = W;
     double* bs = W + n;
     double* c = W + 2 * n;
     double* dd = W + 3 * n;
+    double* ainv = W + 4 * n;
     double* piv = W + 5 * n;
     const double eps = DBL_EPSILON;
+    const double tol = fmax(eps * tnorm, DBL_MIN);
     double prevLam = 0.0;
     for (int jj = j; jj < jend; ++jj) {
         double lam = D.w[jj];
@@ -539,39 +541,57 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
         }
         prevLam = lam;
         double* x = D.Y + (int64_t)jj * D.ldy;
-        // LU with partial pivoting of T - lam I (dlagtf), on one thread
+        // LU with partial pivoting of T - lam I (dlagtf), on one thread.  The
+        // recurrence carries the current pivot row (ak, bk) in registers and
+        // only writes the factors, so the chain is arithmetic, not memory;
+        // no interchange when |c|/scale2 <= |a|/scale1 (compared without
+        // divisions; a zero row a = b = 0 always interchanges).
+        // ainv holds the guarded reciprocals of the U diagonal.
         if (tid == 0) {
-            for (int i = 0; i < n; ++i) a[i] = D.d[i] - lam;
-            for (int i = 0; i + 1 < n; ++i) {
-                bs[i] = D.e[i];
-                c[i] = D.e[i];
-            }
+            const double* __restrict__ dg = D.d;
+            const double* __restrict__ eg = D.e;
+            double* __restrict__ aw = a;
+            double* __restrict__ bw = bs;
+            double* __restrict__ cw = c;
+            double* __restrict__ dw = dd;
+            double* __restrict__ pw = piv;
+            double* __restrict__ iw = ainv;
+            double ak = dg[0] - lam, bk = n > 1 ? eg[0] : 0.0;
+#pragma unroll 4
             for (int kk = 0; kk + 1 < n; ++kk) {
-                const double scale1 = fabs(a[kk]) + fabs(bs[kk]);
-                const double piv1 = scale1 == 0.0 ? 0.0 : fabs(a[kk]) / scale1;
-                double scale2 = fabs(c[kk]) + fabs(a[kk + 1]);
-                if (kk + 2 < n) scale2 += fabs(bs[kk + 1]);
-                const double piv2 = (c[kk] == 0.0 || scale2 == 0.0) ? 0.0 : fabs(c[kk]) / scale2;
-                if (c[kk] == 0.0 || piv2 <= piv1) {
-                    piv[kk] = 0.0;
-                    const double mult = (c[kk] == 0.0 || a[kk] == 0.0) ? 0.0 : c[kk] / a[kk];
-                    c[kk] = mult;
-                    a[kk + 1] -= mult * bs[kk];
-                    if (kk + 2 < n) dd[kk] = 0.0;
+                const double ck = eg[kk];
+                const double a1 = dg[kk + 1] - lam;
+                const double b1 = (kk + 2 < n) ? eg[kk + 1] : 0.0;
+                const double scale1 = fabs(ak) + fabs(bk);
+                const double scale2 = fabs(ck) + fabs(a1) + fabs(b1);
+                double ua, ub, na, nb;   // stored U row kk, carried row kk + 1
+                if (ck == 0.0 || scale2 == 0.0 || (scale1 > 0.0 && fabs(ck) * scale1 <= fabs(ak) * scale2)) {
+                    const double mult = (ck == 0.0 || ak == 0.0) ? 0.0 : ck / ak;
+                    pw[kk] = 0.0;
+                    cw[kk] = mult;
+                    ua = ak;
+                    ub = bk;
+                    na = a1 - mult * bk;
+                    nb = b1;
+                    dw[kk] = 0.0;
                 } else {
-                    piv[kk] = 1.0;
-                    const double mult = a[kk] / c[kk];
-                    a[kk] = c[kk];
-                    const double temp = a[kk + 1];
-                    a[kk + 1] = bs[kk] - mult * temp;
-                    if (kk + 2 < n) {
-                        dd[kk] = bs[kk + 1];
-                        bs[kk + 1] = -mult * dd[kk];
-                    }
-                    bs[kk] = temp;
-                    c[kk] = mult;
+                    const double mult = ak / ck;
+                    pw[kk] = 1.0;
+                    cw[kk] = mult;
+                    ua = ck;
+                    ub = a1;
+                    na = bk - mult * a1;
+                    dw[kk] = b1;
+                    nb = -mult * b1;
                 }
+                aw[kk] = ua;
+                bw[kk] = ub;
+                iw[kk] = 1.0 / (fabs(ua) < tol ? (ua >= 0.0 ? tol : -tol) : ua);
+                ak = na;
+                bk = nb;
             }
+            aw[n - 1] = ak;
+            iw[n - 1] = 1.0 / (fabs(ak) < tol ? (ak >= 0.0 ? tol : -tol) : ak);
         }
         // deterministic start vector
         for (int i = tid; i < n; i += blockDim.x) {
@@ -582,25 +602,38 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
             x[i] = ((h & 0xffffff) / double(0x1000000)) - 0.5 + 1e-3;
         }
         __syncthreads();
-        const double tol = fmax(eps * tnorm, DBL_MIN);
         for (int it = 0; it < 4; ++it) {
             if (tid == 0) {
-                // apply L^-1 with interchanges, then U^-1 (dlagts, job -1)
+                // apply L^-1 with interchanges, then U^-1 (dlagts, job -1),
+                // carrying the running components in registers
+                const double* __restrict__ cw = c;
+                const double* __restrict__ pw = piv;
+                const double* __restrict__ bw = bs;
+                const double* __restrict__ dw = dd;
+                const double* __restrict__ iw = ainv;
+                double cur = x[0];
+#pragma unroll 8
                 for (int kk = 0; kk + 1 < n; ++kk) {
-                    if (piv[kk] == 0.0) x[kk + 1] -= c[kk] * x[kk];
-                    else {
-                        const double temp = x[kk];
-                        x[kk] = x[kk + 1];
-                        x[kk + 1] = temp - c[kk] * x[kk];
+                    const double nxt = x[kk + 1];
+                    if (pw[kk] == 0.0) {
+                        x[kk] = cur;
+                        cur = nxt - cw[kk] * cur;
+                    } else {
+                        x[kk] = nxt;
+                        cur = cur - cw[kk] * nxt;
                     }
                 }
+                x[n - 1] = cur;
+                double x1 = 0.0, x2 = 0.0;     // x[kk + 1], x[kk + 2]
+#pragma unroll 8
                 for (int kk = n - 1; kk >= 0; --kk) {
-                    double temp = x[kk];
-                    if (kk + 1 < n) temp -= bs[kk] * x[kk + 1];
-                    if (kk + 2 < n) temp -= dd[kk] * x[kk + 2];
-                    double ak = a[kk];
-                    if (fabs(ak) < tol) ak = (ak >= 0.0) ? tol : -tol;
-                    x[kk] = temp / ak;
+                    double t = x[kk];
+                    if (kk + 1 < n) t -= bw[kk] * x1;
+                    if (kk + 2 < n) t -= dw[kk] * x2;
+                    const double v = t * iw[kk];
+                    x[kk] = v;
+                    x2 = x1;
+                    x1 = v;
                 }
             }
             __syncthreads();
