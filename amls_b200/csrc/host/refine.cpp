@@ -410,6 +410,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         // error estimate per wanted value: change * r / (1 - r), r the observed
         // contraction of the change (geometric convergence)
         double est = 0.0;
+        int prefix = 0;                                 // leading wanted values already below tol
+        bool inPrefix = true;
         for (int j = 0; j < nev; ++j) {
             const double ch = std::fabs(th[static_cast<size_t>(j)] - prev[static_cast<size_t>(j)]) /
                               std::fabs(th[static_cast<size_t>(j)]);
@@ -421,11 +423,14 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 e = ch * std::max(rr, 0.05) / (1.0 - rr);
             }
             est = std::max(est, std::max(e, ch * 1e-3));
+            if (inPrefix && std::max(e, ch * 1e-3) <= opt_.refineTol) ++prefix;
+            else inPrefix = false;
             prevChange[static_cast<size_t>(j)] = ch;
         }
         prev = th;
         if (opt_.verbosity > 1)
-            std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e\n", it + 1, est);
+            std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e, converged prefix %d\n",
+                         it + 1, est, prefix);
         const bool last = est <= opt_.refineTol || it + 1 >= std::max(1, opt_.refineMaxIter);
         // Q = Vc^T X, and M Q for the next iteration unless this is the last
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),

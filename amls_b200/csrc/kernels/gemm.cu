@@ -16,7 +16,6 @@ namespace amls_b200 {
 
 namespace {
 constexpr int NT = 256;
-constexpr int TM = 64, TN = 64, TK = 16;   // tiles of the front-update kernel
 
 constexpr int kBM = kGemmTile, kBN = kGemmTile;   // 64 x 64
 constexpr int kKs = 16;                            // K slice
@@ -209,81 +208,133 @@ cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int
 // ------------------------------------------------------------------------
 // front extend-add: UK = A A^T, UM = A B^T + B A^T, scattered (subtracted)
 // ------------------------------------------------------------------------
+// The front update on the FP64 tensor cores: tile (p0, q0) of the s x s
+// update, operands A = L_Si and B = R_i^T rows p (M side) and rows q (N side)
+// through the same cp.async ring as the GEMM (four 64 x 16 slices per stage),
+// three m16n8k16 DMMA products per fragment pair (UK += Ap Aq^T,
+// UM += Ap Bq^T + Bp Aq^T), then the extend-add scatter (subtract, atomic)
+// into the ancestors' K and M fronts for p >= pmin[q].
+namespace {
+constexpr int kFuStage = 4 * kKs * kLdA;   // Ap, Bp, Aq, Bq slices
+constexpr size_t kFuSmem = sizeof(double) * kStages * kFuStage;
+
+__device__ __forceinline__ void fuIssueSlice(const FrontUpdDesc& D, int p0, int q0, int k0, double* st) {
+    // 4 operands x 64 rows x 16 k = 4096 elements, 16 per thread
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int idx = threadIdx.x + NT * u;
+        const int op = idx >> 10, e = idx & 1023;
+        const int r = e % 64, k = e / 64;
+        const int gk = k0 + k;
+        const int gr = (op < 2 ? p0 : q0) + r;
+        const bool ok = gr < D.s && gk < D.n;
+        const double* base = (op == 0 || op == 2) ? D.A : D.B;
+        const double* src = ok ? base + gr + (int64_t)gk * D.ld : D.A;
+        cpAsync8(st + op * kKs * kLdA + k * kLdA + r, src, ok);
+    }
+}
+}  // namespace
+
 __global__ void __launch_bounds__(NT) frontUpdateKernel(const FrontUpdDesc* __restrict__ descs,
                                                         const TileRef* __restrict__ tiles,
                                                         double* __restrict__ kPool,
                                                         double* __restrict__ mPool) {
-    __shared__ double Ap[TK][TM + 2], Bp[TK][TM + 2], Aq[TK][TN + 2], Bq[TK][TN + 2];
+    extern __shared__ double fuSmem[];
     const TileRef t = tiles[blockIdx.x];
     const FrontUpdDesc D = descs[t.desc];
     const int p0 = t.m0, q0 = t.n0;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double aK[4][4], aM[4][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+    double aK[2][2][4], aM[2][2][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) aK[i][j] = aM[i][j] = 0.0;
-
-    for (int k0 = 0; k0 < D.n; k0 += TK) {
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int idx = threadIdx.x + NT * u;
-            const int r = idx % TM, k = idx / TM;
-            const int gk = k0 + k;
-            const bool kin = gk < D.n;
-            const int gp = p0 + r, gq = q0 + r;
-            const int64_t cofs = (int64_t)gk * D.ld;
-            Ap[k][r] = (kin && gp < D.s) ? D.A[gp + cofs] : 0.0;
-            Bp[k][r] = (kin && gp < D.s) ? D.B[gp + cofs] : 0.0;
-            Aq[k][r] = (kin && gq < D.s) ? D.A[gq + cofs] : 0.0;
-            Bq[k][r] = (kin && gq < D.s) ? D.B[gq + cofs] : 0.0;
-        }
+            for (int q = 0; q < 4; ++q) aK[i][j][q] = aM[i][j][q] = 0.0;
+    const int nSlices = (D.n + kKs - 1) / kKs;
+#pragma unroll
+    for (int st = 0; st < kStages - 1; ++st) {
+        if (st < nSlices) fuIssueSlice(D, p0, q0, st * kKs, fuSmem + st * kFuStage);
+        cpAsyncCommit();
+    }
+    for (int sl = 0; sl < nSlices; ++sl) {
+        cpAsyncWait<kStages - 2>();
         __syncthreads();
+        const int nx = sl + kStages - 1;
+        if (nx < nSlices) fuIssueSlice(D, p0, q0, nx * kKs, fuSmem + (nx % kStages) * kFuStage);
+        cpAsyncCommit();
+        const double* Ap = fuSmem + (sl % kStages) * kFuStage;
+        const double* Bp = Ap + kKs * kLdA;
+        const double* Aq = Bp + kKs * kLdA;
+        const double* Bq = Aq + kKs * kLdA;
+        double ap[2][8], bp[2][8], aq[2][4], bq[2][4];
 #pragma unroll
-        for (int kk = 0; kk < TK; ++kk) {
-            double ap[4], bp[4], aq[4], bq[4];
+        for (int i = 0; i < 2; ++i) {
+            const int r = wm + 16 * i + g;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                ap[i] = Ap[kk][tx + 16 * i];
-                bp[i] = Bp[kk][tx + 16 * i];
+            for (int q = 0; q < 4; ++q) {
+                ap[i][2 * q] = Ap[(tg + 4 * q) * kLdA + r];
+                ap[i][2 * q + 1] = Ap[(tg + 4 * q) * kLdA + r + 8];
+                bp[i][2 * q] = Bp[(tg + 4 * q) * kLdA + r];
+                bp[i][2 * q + 1] = Bp[(tg + 4 * q) * kLdA + r + 8];
             }
+        }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                aq[j] = Aq[kk][ty + 16 * j];
-                bq[j] = Bq[kk][ty + 16 * j];
+        for (int j = 0; j < 2; ++j) {
+            const int c = wn + 8 * j + g;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                aq[j][q] = Aq[(tg + 4 * q) * kLdA + c];
+                bq[j][q] = Bq[(tg + 4 * q) * kLdA + c];
             }
+        }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    aK[i][j] = fma(ap[i], aq[j], aK[i][j]);
-                    aM[i][j] = fma(ap[i], bq[j], fma(bp[i], aq[j], aM[i][j]));
+            for (int j = 0; j < 2; ++j) {
+                dmma16x8x16(aK[i][j], ap[i], aq[j]);
+                dmma16x8x16(aM[i][j], ap[i], bq[j]);
+                dmma16x8x16(aM[i][j], bp[i], aq[j]);
+            }
+    }
+    cpAsyncWait<0>();
+    // fragment (i, j) element e: row p = p0 + wm + 16 i + g + 8 (e / 2),
+    // column q = q0 + wn + 8 j + 2 tg + (e % 2)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            const int q = q0 + wn + 8 * j + 2 * tg + e2;
+            if (q >= D.s) continue;
+            const int pm = D.pmin[q];
+            const int64_t co = D.colOff[q];
+            const int rb = D.rowBase[q];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int p = p0 + wm + 16 * i + g + 8 * h;
+                    if (p >= D.s || p < pm) continue;
+                    const int64_t o = co + D.rowIdx[rb + p];
+                    atomicAdd(kPool + o, -aK[i][j][2 * h + e2]);
+                    atomicAdd(mPool + o, -aM[i][j][2 * h + e2]);
                 }
         }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int q = q0 + ty + 16 * j;
-        if (q >= D.s) continue;
-        const int pm = D.pmin[q];
-        const int64_t co = D.colOff[q];
-        const int rb = D.rowBase[q];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int p = p0 + tx + 16 * i;
-            if (p >= D.s || p < pm) continue;
-            const int64_t o = co + D.rowIdx[rb + p];
-            atomicAdd(kPool + o, -aK[i][j]);
-            atomicAdd(mPool + o, -aM[i][j]);
-        }
-    }
 }
 
 cudaError_t launchFrontUpdate(const FrontUpdDesc* dDescs, const TileRef* dTiles, int nTiles,
                               double* kPool, double* mPool, cudaStream_t s) {
     if (nTiles <= 0) return cudaSuccess;
-    frontUpdateKernel<<<nTiles, NT, 0, s>>>(dDescs, dTiles, kPool, mPool);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(frontUpdateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kFuSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    frontUpdateKernel<<<nTiles, NT, kFuSmem, s>>>(dDescs, dTiles, kPool, mPool);
     return cudaGetLastError();
 }
 
