@@ -200,7 +200,7 @@ private:
     // refinement and the device dense eigensolver
     DevBuf dgE_, dgY_, dgT_, dgLinv_, dgD_, dgWork_, dgK_, dgBlob_, dgP_, dgInv_;
     DevBuf refR_, refX_, refMX_, refKc_, refMc_, refV_, refW_, refIdx_, refBlob_, refY1_, refY2_;
-    DevBuf refT_, refMQ_;
+    DevBuf refT_, refMQ_, refKQ_;
     DevBuf wyS_, wyW_, wyBlob_;                    // blocked back-transform
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve

@@ -179,11 +179,16 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     idx.upload(refIdx_, s);
     const int32_t* dId = idx.dev<int32_t>(oId);
     const int64_t* dCo = idx.dev<int64_t>(oCo);
+    // All sweep descriptors live in one array (`sweep`, tiles index into it),
+    // so locking converged vectors can re-point them at the active rows with
+    // one upload: M = nq - L, A += L, C += L (every sweep operand A and
+    // output C is a block of the vector rows; B is the factor).
     struct Tabs {
-        size_t ftD, ftT, fgD, fgT, bgD, bgT, btD, btT;
+        size_t ftT, fgT, bgT, btT;
         int nft, nfg, nbg, nbt;
     };
     std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
+    std::vector<GemmDesc> sweep;
     double fsolve = 0;
     for (int l = 0; l <= maxLevel_; ++l) {
         std::vector<GemmDesc> ft, bt;
@@ -270,12 +275,22 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 fsolve += 4.0 * nq * ni * si;
             }
         }
+        auto append = [&](const std::vector<GemmDesc>& d, std::vector<TileRef>& t) {
+            const int base = static_cast<int>(sweep.size());
+            sweep.insert(sweep.end(), d.begin(), d.end());
+            for (TileRef& r : t) r.desc += base;
+        };
+        append(ft, ftT);
+        append(fg, fgT);
+        append(bg, bgT);
+        append(bt, btT);
         Tabs& T = tabs[static_cast<size_t>(l)];
-        T.ftD = b.add(ft); T.ftT = b.add(ftT); T.nft = static_cast<int>(ftT.size());
-        T.fgD = b.add(fg); T.fgT = b.add(fgT); T.nfg = static_cast<int>(fgT.size());
-        T.bgD = b.add(bg); T.bgT = b.add(bgT); T.nbg = static_cast<int>(bgT.size());
-        T.btD = b.add(bt); T.btT = b.add(btT); T.nbt = static_cast<int>(btT.size());
+        T.ftT = b.add(ftT); T.nft = static_cast<int>(ftT.size());
+        T.fgT = b.add(fgT); T.nfg = static_cast<int>(fgT.size());
+        T.bgT = b.add(bgT); T.nbg = static_cast<int>(bgT.size());
+        T.btT = b.add(btT); T.nbt = static_cast<int>(btT.size());
     }
+    const size_t oSweep = b.add(sweep);
     // Rayleigh-Ritz products: Kc = X R^T, Mc = X MX^T (split-K over n), Q = Vc^T X
     const int chunk = 4096;
     std::vector<GemmDesc> rr(2), up(1);
@@ -297,57 +312,79 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             for (int jt = 0; jt < cdiv2(nq, kTB); ++jt)
                 for (int it = 0; it < cdiv2(nq, kTB); ++it) rrT.push_back({q, it * kTB, jt * kTB, kc});
     }
-    // subspace update Q = Vc^T X and, for the next iteration's first K^-1 M
-    // application, M Q = Vc^T (M X) (a GEMM instead of a sparse product)
+    // subspace update Q = Vc^T X and, for the next iteration, M Q = Vc^T (M X)
+    // (the first K^-1 M application's right-hand side, a GEMM instead of a
+    // sparse product) and K Q = Vc^T R on the rows that will be locked (R =
+    // K X holds for every row: X = K^-1 R on the active rows, and the locked
+    // rows carry K Q)
     double* MQ = static_cast<double*>(refMQ_.ensure(sizeof(double) * sz));
-    up.resize(2);
-    for (int q = 0; q < 2; ++q) {
+    double* KQ = static_cast<double*>(refKQ_.ensure(sizeof(double) * sz));
+    up.resize(3);
+    for (int q = 0; q < 3; ++q) {
         GemmDesc& g = up[static_cast<size_t>(q)];
-        g.M = nq;
+        g.M = q == 2 ? 0 : nq;                           // KQ rows: set when locking
         g.N = static_cast<int32_t>(n);
         g.K = nq;
         g.flags = kTransA;
         g.A = Vc;
         g.lda = nq;
-        g.B = q == 0 ? X : MX;
+        g.B = q == 0 ? X : q == 1 ? MX : R;
         g.ldb = nq;
-        g.C = q == 0 ? Q : MQ;
+        g.C = q == 0 ? Q : q == 1 ? MQ : KQ;
         g.ldc = nq;
         g.alpha = 1.0;
     }
-    for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
-        for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({0, it * kTB, jt * kTB, 0});
-    const int nUp1 = static_cast<int>(upT.size());
-    for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
-        for (int it = 0; it < cdiv2(nq, kTB); ++it) upT.push_back({1, it * kTB, jt * kTB, 0});
+    for (int q = 0; q < 3; ++q)
+        for (int jt = 0; jt < cdiv2(n, kTB); ++jt)
+            for (int it = 0; it < cdiv2(q == 2 ? nev : nq, kTB); ++it)
+                upT.push_back({q, it * kTB, jt * kTB, 0});
+    const int nUp1 = cdiv2(n, kTB) * cdiv2(nq, kTB);     // the Q = Vc^T X tiles come first
     FrontDesc sym[2] = {{Kc, nq, nq, nq, -3, 0}, {Mc, nq, nq, nq, -3, 0}};
     const size_t oRR = b.add(rr), oRRT = b.add(rrT), oUP = b.add(up), oUPT = b.add(upT),
                  oSym = b.add(sym, 2);
     b.upload(refBlob_, s);
 
     const double dn = static_cast<double>(n), dq = nq;
+    // Soft locking: the leading `lock` Ritz vectors (a multiple of the tile
+    // height, all with converged values) stay in the Rayleigh-Ritz basis as
+    // they are (X = Q, R = K Q, M X = M Q on those rows) and get no K^-1 M
+    // applications; the sweeps and sparse products run on rows [lock, nq).
+    int lock = 0;
+    auto setLock = [&](int L) {
+        lock = L;
+        std::vector<GemmDesc> act(sweep);
+        for (GemmDesc& g : act) {
+            g.M = nq - L;
+            g.A += L;
+            g.C += L;
+        }
+        cudaCheck(cudaMemcpyAsync(b.dev<GemmDesc>(oSweep), act.data(), sizeof(GemmDesc) * act.size(),
+                                  cudaMemcpyHostToDevice, s), "lock");
+    };
     auto spmm = [&](const double* Y, double* out) {
+        const int m = nq - lock;
         LAUNCH(launchSpmmGroupT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), nGrp_,
-                                mGrp_.as<int64_t>(), invDev_.as<int64_t>(), Y, nq, out, s));
-        catF_[8] += 2.0 * nnzM_ * dq;
-        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * dq;
+                                mGrp_.as<int64_t>(), invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s));
+        catF_[8] += 2.0 * nnzM_ * m;
+        catB_[8] += 12.0 * nnzM_ + 16.0 * dn * m;
     };
     // the K^-1 M application on Y (nq x n): R = M Y (or the given M Y), X = K^-1 R
     auto applyT = [&](const double* Y, const double* MY) {
         if (MY) cudaCheck(cudaMemcpyAsync(R, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         else spmm(Y, R);
         cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+        const GemmDesc* sw = b.dev<GemmDesc>(oSweep);
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.ftD), b.dev<TileRef>(T.ftT), T.nft, s));
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.fgD), b.dev<TileRef>(T.fgT), T.nfg, s));
+            LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.ftT), T.nft, s));
+            LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.fgT), T.nfg, s));
         }
         for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.bgD), b.dev<TileRef>(T.bgT), T.nbg, s));
-            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(T.btD), b.dev<TileRef>(T.btT), T.nbt, s));
+            LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.bgT), T.nbg, s));
+            LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.btT), T.nbt, s));
         }
-        catF_[2] += fsolve;
+        catF_[2] += fsolve * (nq - lock) / dq;
     };
     // Chebyshev recurrence buffers (degree = refine - 1)
     int cheb = std::max(0, opt_.refine - 1);
@@ -382,6 +419,12 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         }
         applyT(Yc, MYc);                                 // X = T Y_c, R = M Y_c = K X
         spmm(X, MX);
+        if (lock > 0) {
+            const size_t pitch = sizeof(double) * static_cast<size_t>(nq), w = sizeof(double) * lock;
+            cudaCheck(cudaMemcpy2DAsync(X, pitch, Q, pitch, w, n, cudaMemcpyDeviceToDevice, s), "lock");
+            cudaCheck(cudaMemcpy2DAsync(R, pitch, KQ, pitch, w, n, cudaMemcpyDeviceToDevice, s), "lock");
+            cudaCheck(cudaMemcpy2DAsync(MX, pitch, MQ, pitch, w, n, cudaMemcpyDeviceToDevice, s), "lock");
+        }
         cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
         cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
@@ -432,12 +475,26 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             std::fprintf(stderr, "[amls_b200] refine it %d: estimated max rel error %.3e, converged prefix %d\n",
                          it + 1, est, prefix);
         const bool last = est <= opt_.refineTol || it + 1 >= std::max(1, opt_.refineMaxIter);
-        // Q = Vc^T X, and M Q for the next iteration unless this is the last
+        // rows to lock next: the converged prefix rounded down to whole tiles
+        const int nextLock = last ? lock : std::max(lock, std::min(prefix, nq - 1) / kTB * kTB);
+        if (!last && nextLock > 0) {
+            GemmDesc kq = up[2];
+            kq.M = nextLock;
+            cudaCheck(cudaMemcpyAsync(b.dev<GemmDesc>(oUP) + 2, &kq, sizeof(kq), cudaMemcpyHostToDevice, s),
+                      "lock");
+        }
+        // Q = Vc^T X, and M Q (and K Q on the rows to lock) for the next
+        // iteration unless this is the last
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
                                     last ? nUp1 : static_cast<int>(upT.size()), s));
-        catF_[2] += (last ? 1.0 : 2.0) * 2.0 * dn * dq * dq;
+        catF_[2] += (last ? 1.0 : 2.0 + static_cast<double>(nextLock) / dq) * 2.0 * dn * dq * dq;
         catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;
         haveMQ = !last;
+        if (nextLock != lock) {
+            if (opt_.verbosity > 1)
+                std::fprintf(stderr, "[amls_b200] refine: %d vectors locked\n", nextLock);
+            setLock(nextLock);
+        }
         if (est <= opt_.refineTol) {
             ++it;
             break;

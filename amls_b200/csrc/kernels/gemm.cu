@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restri
     extern __shared__ double gemmSmem[];
     const TileRef t = tiles[blockIdx.x];
     const GemmDesc D = descs[t.desc];
+    if (t.m0 >= D.M || t.n0 >= D.N) return;          // tile outside a shrunk descriptor
     const bool ta = D.flags & kTransA, tb = D.flags & kTransB, ga = D.flags & kGatherA;
     if (ga) {
         if (tb) gemmTile<false, true, true>(D, t, gemmSmem);

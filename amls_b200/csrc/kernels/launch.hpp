@@ -234,11 +234,12 @@ cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, i
                         const int64_t* perm, const int64_t* inv, const double* Qt, int m,
                         double* Rt, cudaStream_t s);
 // The same over groups of consecutive original rows with one shared column
-// pattern (grp: ngrp + 1 row starts, groups of at most kSpmmGroup rows).
+// pattern (grp: ngrp + 1 row starts, groups of at most kSpmmGroup rows),
+// on m rows of Qt and Rt whose columns are ld apart (m <= ld).
 constexpr int kSpmmGroup = 4;
 cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
                              const int64_t* grp, const int64_t* inv, const double* Qt, int m,
-                             double* Rt, cudaStream_t s);
+                             int64_t ld, double* Rt, cudaStream_t s);
 // Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
 // (n x nmodes, original order): see sensitivity.cu.  weight[k] NaN marks a
 // non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.

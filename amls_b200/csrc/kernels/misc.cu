@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict
                                                        const int64_t* __restrict__ grp,
                                                        const int64_t* __restrict__ inv,
                                                        const double* __restrict__ Qt, int m,
-                                                       double* __restrict__ Rt) {
+                                                       int64_t ld, double* __restrict__ Rt) {
     constexpr int kStage = 256;
     __shared__ double sv[kSpmmGroup][kStage];
     __shared__ int64_t sc[kStage];
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict
                 const int c = (int)((cnt - eb) < kStage ? (cnt - eb) : kStage);
                 __syncthreads();
                 for (int t = threadIdx.x; t < c; t += blockDim.x) {
-                    sc[t] = inv[ci[rp[o0] + eb + t]] * (int64_t)m;
+                    sc[t] = inv[ci[rp[o0] + eb + t]] * ld;
                     for (int r = 0; r < G; ++r) sv[r][t] = v[rp[o0 + r] + eb + t];
                 }
                 __syncthreads();
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict
 #pragma unroll
             for (int r = 0; r < kSpmmGroup; ++r)
                 if (r < G) {
-                    double* out = Rt + inv[o0 + r] * (int64_t)m;
+                    double* out = Rt + inv[o0 + r] * ld;
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
                         const int j = j0 + threadIdx.x + 256 * u;
@@ -375,18 +375,18 @@ __global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict
 
 cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
                              const int64_t* grp, const int64_t* inv, const double* Qt, int m,
-                             double* Rt, cudaStream_t s) {
+                             int64_t ld, double* Rt, cudaStream_t s) {
     if (ngrp <= 0 || m <= 0) return cudaSuccess;
     const int grid = gridFor(ngrp * 256, 256);
     const int u = (m + 255) / 256;
     if (u <= 1)
-        spmmGroupKernel<1><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+        spmmGroupKernel<1><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
     else if (u == 2)
-        spmmGroupKernel<2><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+        spmmGroupKernel<2><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
     else if (u == 3)
-        spmmGroupKernel<3><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+        spmmGroupKernel<3><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
     else
-        spmmGroupKernel<4><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, Rt);
+        spmmGroupKernel<4><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
     return cudaGetLastError();
 }
 
