@@ -9,6 +9,7 @@
 #include <cstring>
 #include <exception>
 #include <functional>
+#include <iterator>
 #include <mutex>
 #include <thread>
 #include <cstdio>
@@ -343,24 +344,71 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     permDev_.ensure(sizeof(int64_t) * static_cast<size_t>(n));
     kDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzK_, 1)));
     mDst_.ensure(sizeof(int64_t) * static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
-    // groups of consecutive rows with identical M column patterns (the DOFs
-    // of one mesh node), at most kSpmmGroup rows each, for the grouped SpMM
+    // super-rows for the products with M: node groups (consecutive rows with
+    // identical column patterns, the DOFs of one mesh node) merged greedily
+    // with their successors while the rows fit kSpmmSuperRows and each added
+    // group brings at most 80 % new columns; a dense block per super-row over
+    // the union pattern, filled from the CSR values at each numeric solve
+    // through supDst (CSR entry -> block position)
     {
-        std::vector<int64_t> grp;
-        int64_t r = 0;
-        while (r < n) {
-            grp.push_back(r);
+        std::vector<SpmmSuper> sup;
+        std::vector<int32_t> ucols;
+        std::vector<int64_t> dst(static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+        std::vector<int32_t> uni, tmp, pat;
+        int64_t valOff = 0;
+        auto groupEnd = [&](int64_t r) {
             const int64_t len = mp[r + 1] - mp[r];
             int64_t e = r + 1;
-            while (e < n && e - r < kSpmmGroup && mp[e + 1] - mp[e] == len &&
-                   std::equal(mc + mp[r], mc + mp[r + 1], mc + mp[e]))
+            while (e < n && e - r < kSpmmSuperRows && mp[e + 1] - mp[e] == len && std::equal(mc + mp[r], mc + mp[r + 1], mc + mp[e]))
                 ++e;
+            return e;
+        };
+        auto sortedPattern = [&](int64_t r, std::vector<int32_t>& out) {
+            out.assign(mc + mp[r], mc + mp[r + 1]);
+            std::sort(out.begin(), out.end());
+            out.erase(std::unique(out.begin(), out.end()), out.end());
+        };
+        int64_t r = 0;
+        while (r < n) {
+            int64_t e = groupEnd(r);
+            sortedPattern(r, uni);
+            while (e < n) {
+                const int64_t e2 = groupEnd(e);
+                if (e2 - r > kSpmmSuperRows) break;
+                sortedPattern(e, pat);
+                tmp.clear();
+                std::set_union(uni.begin(), uni.end(), pat.begin(), pat.end(), std::back_inserter(tmp));
+                if (static_cast<double>(tmp.size() - uni.size()) > 0.8 * static_cast<double>(pat.size())) break;
+                uni.swap(tmp);
+                e = e2;
+            }
+            SpmmSuper S{};
+            S.row0 = r;
+            S.rows = static_cast<int32_t>(e - r);
+            S.colOff = static_cast<int64_t>(ucols.size());
+            S.len = static_cast<int32_t>(uni.size());
+            S.valOff = valOff;
+            for (int64_t d = r; d < e; ++d)
+                for (int64_t q = mp[d]; q < mp[d + 1]; ++q) {
+                    const int64_t t = std::lower_bound(uni.begin(), uni.end(), mc[q]) - uni.begin();
+                    dst[static_cast<size_t>(q)] = valOff + t * kSpmmSuperRows + (d - r);
+                }
+            ucols.insert(ucols.end(), uni.begin(), uni.end());
+            valOff += static_cast<int64_t>(uni.size()) * kSpmmSuperRows;
+            sup.push_back(S);
             r = e;
         }
-        grp.push_back(n);
-        nGrp_ = static_cast<int64_t>(grp.size()) - 1;
-        mGrp_.ensure(sizeof(int64_t) * grp.size());
-        cudaCheck(cudaMemcpyAsync(mGrp_.as<int64_t>(), grp.data(), sizeof(int64_t) * grp.size(),
+        nSup_ = static_cast<int64_t>(sup.size());
+        supValTotal_ = valOff;
+        supDesc_.ensure(sizeof(SpmmSuper) * std::max<size_t>(sup.size(), 1));
+        supCols_.ensure(sizeof(int32_t) * std::max<size_t>(ucols.size(), 1));
+        supDst_.ensure(sizeof(int64_t) * dst.size());
+        supVal_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(valOff, 1)));
+        cudaCheck(cudaMemcpyAsync(supDesc_.as<SpmmSuper>(), sup.data(), sizeof(SpmmSuper) * sup.size(),
+                                  cudaMemcpyHostToDevice, stream_), "upload");
+        cudaCheck(cudaMemcpyAsync(supCols_.as<int32_t>(), ucols.data(), sizeof(int32_t) * ucols.size(),
+                                  cudaMemcpyHostToDevice, stream_), "upload");
+        cudaCheck(cudaMemcpyAsync(supDst_.as<int64_t>(), dst.data(), sizeof(int64_t) * nnzM_,
                                   cudaMemcpyHostToDevice, stream_), "upload");
         cudaCheck(cudaStreamSynchronize(stream_), "upload");
     }
@@ -1141,6 +1189,8 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     if (opt_.shift != 0.0)
         LAUNCH(launchScatterAdd(mVal_.as<double>(), mDst_.as<int64_t>(), nnzM_, opt_.shift, kPool_.as<double>(), s));
     LAUNCH(launchScatterAdd(mVal_.as<double>(), mDst_.as<int64_t>(), nnzM_, 1.0, mPool_.as<double>(), s));
+    LAUNCH(launchZero(supVal_.as<double>(), supValTotal_, s));
+    LAUNCH(launchScatterAdd(mVal_.as<double>(), supDst_.as<int64_t>(), nnzM_, 1.0, supVal_.as<double>(), s));
     eliminate(s);
     checkStatus("elimination");
     const auto t2 = Clock::now();
@@ -1443,8 +1493,8 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const d
 void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
     norms_.ensure(sizeof(double) * static_cast<size_t>(m));
     zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
-    LAUNCH(launchMNorm(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), n_, invDev_.as<int64_t>(), zt, ldz,
-                       m, norms_.as<double>(), s));
+    LAUNCH(launchMNormSuper(supDesc_.as<SpmmSuper>(), nSup_, supCols_.as<int32_t>(), supVal_.as<double>(),
+                            invDev_.as<int64_t>(), zt, m, ldz, norms_.as<double>(), s));
     LAUNCH(launchUnpermute(zt, ldz, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
     cudaCheck(cudaStreamSynchronize(s), "finalize");
 }

@@ -141,8 +141,8 @@ private:
     DevBuf linvPool_, linvScratch_;                // L_ii^-1 per node (eig layout), doubling scratch
     DevBuf kVal_, mVal_, kDst_, mDst_;             // CSR values and their front destinations
     DevBuf mRp_, mCi_, invDev_, permDev_;          // original M CSR pattern, maps
-    DevBuf mGrp_;                                  // row groups with one M pattern
-    int64_t nGrp_ = 0;
+    DevBuf supDesc_, supCols_, supDst_, supVal_;   // super-rows of M (SpMM, M-norms)
+    int64_t nSup_ = 0, supValTotal_ = 0;
     DevBuf staticInts_;                            // extend-add and panel maps
     DevBuf staticBlob_;                            // level launch tables
     DevBuf status_;

@@ -363,8 +363,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
     };
     auto spmm = [&](const double* Y, double* out) {
         const int m = nq - lock;
-        LAUNCH(launchSpmmGroupT(mRp_.as<int64_t>(), mCi_.as<int32_t>(), mVal_.as<double>(), nGrp_,
-                                mGrp_.as<int64_t>(), invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s));
+        LAUNCH(launchSpmmSuperT(supDesc_.as<SpmmSuper>(), nSup_, supCols_.as<int32_t>(), supVal_.as<double>(),
+                                invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s));
         catF_[8] += 2.0 * nnzM_ * m;
         catB_[8] += 12.0 * nnzM_ + 16.0 * dn * m;
     };

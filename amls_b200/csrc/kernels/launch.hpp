@@ -221,25 +221,27 @@ cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int 
 cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* out,
                              const int64_t* dstOff, const int32_t* len, int nSeg,
                              cudaStream_t s);
-// M-norms of the columns of X under the original M (CSR rp/ci/v), with X
-// held transposed in permuted order: x[o, j] = zt[j + inv[o]*ldz], j < m.
-cudaError_t launchMNorm(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* inv, const double* zt, int64_t ldz, int m, double* norms,
-                        cudaStream_t s);
 // Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]), j < m.
 cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
                             const double* norms, double* Z, cudaStream_t s);
-// Rt[:, d] = (P M P^T Q)[d, :]^T in the transposed layout (see misc.cu).
-cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* perm, const int64_t* inv, const double* Qt, int m,
-                        double* Rt, cudaStream_t s);
-// The same over groups of consecutive original rows with one shared column
-// pattern (grp: ngrp + 1 row starts, groups of at most kSpmmGroup rows),
-// on m rows of Qt and Rt whose columns are ld apart (m <= ld).
-constexpr int kSpmmGroup = 4;
-cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
-                             const int64_t* grp, const int64_t* inv, const double* Qt, int m,
-                             int64_t ld, double* Rt, cudaStream_t s);
+// Products with M in the transposed layout over super-rows (see misc.cu):
+// rows row0 .. row0 + rows - 1 (original order, rows <= kSpmmSuperRows) with
+// the union column pattern ucols[colOff .. colOff + len) and the dense block
+// vals[valOff + t * kSpmmSuperRows + r].
+constexpr int kSpmmSuperRows = 12;
+struct SpmmSuper {
+    int64_t row0, colOff, valOff;
+    int32_t rows, len;
+};
+// Rt[j + inv[o]*ld] = sum_c M[o, c] Qt[j + inv[c]*ld] for j < m <= ld.
+cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
+                             const int64_t* inv, const double* Qt, int m, int64_t ld, double* Rt,
+                             cudaStream_t s);
+// M-norms of the columns of X held transposed in permuted order:
+// norms[j] = x_j^T M x_j with x[o, j] = zt[j + inv[o]*ld], j < m <= ld.
+cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
+                             const int64_t* inv, const double* zt, int m, int64_t ld, double* norms,
+                             cudaStream_t s);
 // Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
 // (n x nmodes, original order): see sensitivity.cu.  weight[k] NaN marks a
 // non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.

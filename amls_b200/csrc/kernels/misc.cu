@@ -148,67 +148,6 @@ cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* ou
     return cudaGetLastError();
 }
 
-// norms[j] = sum_d x[d,j] * sum_{c in row d} M[d,c] x[c,j] over the original
-// M (CSR), with x[o, j] = zt[j + inv[o]*m] (zt in permuted order)
-// one warp per row d at a time; each thread keeps partial sums for columns
-// j = lane + 32*t (t < 16, m <= 512 per pass), flushed by atomics per CTA.
-__global__ void __launch_bounds__(256) mnormKernel(const int64_t* __restrict__ rp,
-                                                   const int32_t* __restrict__ ci,
-                                                   const double* __restrict__ v, int64_t n,
-                                                   const int64_t* __restrict__ inv,
-                                                   const double* __restrict__ zt, int64_t ldz,
-                                                   int m, int j0, double* __restrict__ norms) {
-    constexpr int T = 16;
-    __shared__ double part[8][T * 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double acc[T];
-#pragma unroll
-    for (int t = 0; t < T; ++t) acc[t] = 0.0;
-    const int64_t gw = blockIdx.x * 8 + wid, GW = (int64_t)gridDim.x * 8;
-    for (int64_t d = gw; d < n; d += GW) {
-        double row[T];
-#pragma unroll
-        for (int t = 0; t < T; ++t) row[t] = 0.0;
-        for (int64_t e = rp[d]; e < rp[d + 1]; ++e) {
-            const double a = v[e];
-            const double* zc = zt + inv[ci[e]] * ldz;
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const int j = j0 + lane + 32 * t;
-                if (j < m) row[t] = fma(a, zc[j], row[t]);
-            }
-        }
-        const double* zd = zt + inv[d] * ldz;
-#pragma unroll
-        for (int t = 0; t < T; ++t) {
-            const int j = j0 + lane + 32 * t;
-            if (j < m) acc[t] = fma(zd[j], row[t], acc[t]);
-        }
-    }
-#pragma unroll
-    for (int t = 0; t < T; ++t) part[wid][lane + 32 * t] = acc[t];
-    __syncthreads();
-    for (int q = threadIdx.x; q < T * 32; q += blockDim.x) {
-        double s = 0.0;
-        for (int w = 0; w < 8; ++w) s += part[w][q];
-        const int j = j0 + q;
-        if (j < m) atomicAdd(norms + j, s);
-    }
-}
-
-cudaError_t launchMNorm(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* inv, const double* zt, int64_t ldz, int m, double* norms,
-                        cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * (size_t)m, s);
-    if (e != cudaSuccess) return e;
-    for (int j0 = 0; j0 < m; j0 += 512) {
-        mnormKernel<<<gridFor(n * 32, 256), 256, 0, s>>>(rp, ci, v, n, inv, zt, ldz, m, j0, norms);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
-
 // Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]); 32 x 32 tiles (d, j).
 __global__ void unpermuteKernel(const double* __restrict__ zt, int64_t ldz, int m, int64_t n,
                                 const int64_t* __restrict__ perm, const double* __restrict__ norms,
@@ -252,141 +191,152 @@ cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t 
     return cudaGetLastError();
 }
 
-// SpMM in the transposed layout: for every permuted row d (original row
-// o = perm[d]) Rt[:, d] = sum_e M[o, c_e] * Qt[:, inv[c_e]], with Qt and Rt
-// m x n column-major (ld = m): one CTA per row at a time, the row's
-// (value, column) pairs staged in shared memory, threads over the m
-// contiguous entries of each referenced column.
-__global__ void __launch_bounds__(128) spmmTKernel(const int64_t* __restrict__ rp,
-                                                   const int32_t* __restrict__ ci,
-                                                   const double* __restrict__ v, int64_t n,
-                                                   const int64_t* __restrict__ perm,
-                                                   const int64_t* __restrict__ inv,
-                                                   const double* __restrict__ Qt, int m,
-                                                   double* __restrict__ Rt) {
-    constexpr int kStage = 512;
-    __shared__ double sv[kStage];
-    __shared__ int64_t sc[kStage];
-    for (int64_t d = blockIdx.x; d < n; d += gridDim.x) {
-        const int64_t o = perm[d];
-        const int64_t e0 = rp[o], e1 = rp[o + 1];
-        for (int j0 = 0; j0 < m; j0 += 4 * 128) {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int64_t eb = e0; eb < e1; eb += kStage) {
-                const int cnt = (int)((e1 - eb) < kStage ? (e1 - eb) : kStage);
-                __syncthreads();
-                for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-                    sv[t] = v[eb + t];
-                    sc[t] = inv[ci[eb + t]] * (int64_t)m;
-                }
-                __syncthreads();
-                for (int t = 0; t < cnt; ++t) {
-                    const double a = sv[t];
-                    const double* q = Qt + sc[t];
+// Sparse products with M in the transposed layout, over super-rows: up to
+// kSpmmSuperRows consecutive original rows (the DOFs of a few neighbouring
+// mesh nodes) whose column patterns mostly overlap, stored as one dense
+// block over the union of their patterns (vals[t * kSpmmSuperRows + r] for
+// union column t, row r; zeros where a row has no entry).  Every gathered
+// column of Qt (m contiguous doubles: Qt[j + inv[c] * ld]) then feeds all
+// rows of the super-row from registers, so the gathers, which bound the
+// product (a column is referenced once per neighbouring node), drop by the
+// pattern overlap.  One CTA of kSpmmThreads per super-row at a time; thread
+// t owns columns j0 + t + kSpmmThreads u (u < U).
+namespace {
+constexpr int kSpmmThreads = 128;
+constexpr int kSpmmStage = 128;
+
+template <int U, bool DOT>
+__device__ __forceinline__ void superRow(const SpmmSuper& S, const int32_t* __restrict__ ucols,
+                                         const double* __restrict__ vals, const int64_t* __restrict__ inv,
+                                         const double* __restrict__ Qt, int m, int64_t ld, int j0,
+                                         double* __restrict__ Rt, double (&dot)[U], double* sv, int64_t* sc) {
+    constexpr int R = kSpmmSuperRows;
+    double acc[R][U];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int j = j0 + threadIdx.x + 128 * u;
-                        if (j < m) acc[u] = fma(a, q[j], acc[u]);
-                    }
-                }
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc[r][u] = 0.0;
+    const int32_t* cols = ucols + S.colOff;
+    const double* blk = vals + S.valOff;
+    for (int eb = 0; eb < S.len; eb += kSpmmStage) {
+        const int c = (S.len - eb) < kSpmmStage ? (S.len - eb) : kSpmmStage;
+        __syncthreads();
+        for (int i = threadIdx.x; i < c * R; i += kSpmmThreads) sv[i] = blk[(int64_t)eb * R + i];
+        for (int t = threadIdx.x; t < c; t += kSpmmThreads) sc[t] = inv[cols[eb + t]] * ld;
+        __syncthreads();
+#pragma unroll 4
+        for (int t = 0; t < c; ++t) {
+            const double* q = Qt + sc[t];
+            double x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = j0 + threadIdx.x + kSpmmThreads * u;
+                x[u] = j < m ? q[j] : 0.0;
             }
+            const double2* a2 = reinterpret_cast<const double2*>(sv + t * R);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + threadIdx.x + 128 * u;
-                if (j < m) Rt[j + d * (int64_t)m] = acc[u];
+            for (int r2 = 0; r2 < R / 2; ++r2) {
+                const double2 a = a2[r2];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    acc[2 * r2][u] = fma(a.x, x[u], acc[2 * r2][u]);
+                    acc[2 * r2 + 1][u] = fma(a.y, x[u], acc[2 * r2 + 1][u]);
+                }
             }
         }
     }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (r < S.rows) {
+            const int64_t o = inv[S.row0 + r] * ld;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = j0 + threadIdx.x + kSpmmThreads * u;
+                if (j < m) {
+                    if (DOT) dot[u] = fma(Qt[o + j], acc[r][u], dot[u]);
+                    else Rt[o + j] = acc[r][u];
+                }
+            }
+        }
+}
+}  // namespace
+
+template <int U>
+__global__ void __launch_bounds__(kSpmmThreads) spmmSuperKernel(const SpmmSuper* __restrict__ sup, int64_t nsup,
+                                                                const int32_t* __restrict__ ucols,
+                                                                const double* __restrict__ vals,
+                                                                const int64_t* __restrict__ inv,
+                                                                const double* __restrict__ Qt, int m, int64_t ld,
+                                                                double* __restrict__ Rt) {
+    __shared__ __align__(16) double sv[kSpmmStage * kSpmmSuperRows];
+    __shared__ int64_t sc[kSpmmStage];
+    double dot[U];
+    for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x) {
+        const SpmmSuper S = sup[g];
+        for (int j0 = 0; j0 < m; j0 += kSpmmThreads * U)
+            superRow<U, false>(S, ucols, vals, inv, Qt, m, ld, j0, Rt, dot, sv, sc);
+    }
 }
 
-cudaError_t launchSpmmT(const int64_t* rp, const int32_t* ci, const double* v, int64_t n,
-                        const int64_t* perm, const int64_t* inv, const double* Qt, int m,
-                        double* Rt, cudaStream_t s) {
-    if (n <= 0 || m <= 0) return cudaSuccess;
-    spmmTKernel<<<gridFor(n * 128, 128), 128, 0, s>>>(rp, ci, v, n, perm, inv, Qt, m, Rt);
+// norms[j] += sum over the super-row's rows o of x[o, j] (M x)[o, j]; the
+// j chunk is blockIdx.y, one atomic per thread and column at the end
+template <int U>
+__global__ void __launch_bounds__(kSpmmThreads) mnormSuperKernel(const SpmmSuper* __restrict__ sup, int64_t nsup,
+                                                                 const int32_t* __restrict__ ucols,
+                                                                 const double* __restrict__ vals,
+                                                                 const int64_t* __restrict__ inv,
+                                                                 const double* __restrict__ zt, int m, int64_t ld,
+                                                                 double* __restrict__ norms) {
+    __shared__ __align__(16) double sv[kSpmmStage * kSpmmSuperRows];
+    __shared__ int64_t sc[kSpmmStage];
+    const int j0 = blockIdx.y * kSpmmThreads * U;
+    double dot[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) dot[u] = 0.0;
+    for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x)
+        superRow<U, true>(sup[g], ucols, vals, inv, zt, m, ld, j0, nullptr, dot, sv, sc);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int j = j0 + threadIdx.x + kSpmmThreads * u;
+        if (j < m) atomicAdd(norms + j, dot[u]);
+    }
+}
+
+namespace {
+// columns per thread: the smallest of 2, 4, 6, 8 covering m (8 beyond 1024)
+int spmmU(int m) {
+    const int u = (m + kSpmmThreads - 1) / kSpmmThreads;
+    return u <= 2 ? 2 : u <= 4 ? 4 : u <= 6 ? 6 : 8;
+}
+}  // namespace
+
+cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
+                             const int64_t* inv, const double* Qt, int m, int64_t ld, double* Rt,
+                             cudaStream_t s) {
+    if (nsup <= 0 || m <= 0) return cudaSuccess;
+    const int grid = gridFor(nsup * kSpmmThreads, kSpmmThreads);
+    switch (spmmU(m)) {
+        case 2: spmmSuperKernel<2><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
+        case 4: spmmSuperKernel<4><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
+        case 6: spmmSuperKernel<6><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
+        default: spmmSuperKernel<8><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
+    }
     return cudaGetLastError();
 }
 
-// The same product over row groups: consecutive original rows grp[g] ..
-// grp[g+1]-1 (at most kSpmmGroup) share one column pattern, as the DOFs of
-// one mesh node do, so every gathered column of Qt (m doubles from L2) feeds
-// all rows of the group.  One CTA per group, thread t owns columns
-// j0 + t + 256 u (u < U).
-template <int U>
-__global__ void __launch_bounds__(256) spmmGroupKernel(const int64_t* __restrict__ rp,
-                                                       const int32_t* __restrict__ ci,
-                                                       const double* __restrict__ v, int64_t ngrp,
-                                                       const int64_t* __restrict__ grp,
-                                                       const int64_t* __restrict__ inv,
-                                                       const double* __restrict__ Qt, int m,
-                                                       int64_t ld, double* __restrict__ Rt) {
-    constexpr int kStage = 256;
-    __shared__ double sv[kSpmmGroup][kStage];
-    __shared__ int64_t sc[kStage];
-    for (int64_t g = blockIdx.x; g < ngrp; g += gridDim.x) {
-        const int64_t o0 = grp[g];
-        const int G = (int)(grp[g + 1] - o0);
-        const int64_t cnt = rp[o0 + 1] - rp[o0];
-        for (int j0 = 0; j0 < m; j0 += 256 * U) {
-            double acc[kSpmmGroup][U];
-#pragma unroll
-            for (int r = 0; r < kSpmmGroup; ++r)
-#pragma unroll
-                for (int u = 0; u < U; ++u) acc[r][u] = 0.0;
-            for (int64_t eb = 0; eb < cnt; eb += kStage) {
-                const int c = (int)((cnt - eb) < kStage ? (cnt - eb) : kStage);
-                __syncthreads();
-                for (int t = threadIdx.x; t < c; t += blockDim.x) {
-                    sc[t] = inv[ci[rp[o0] + eb + t]] * ld;
-                    for (int r = 0; r < G; ++r) sv[r][t] = v[rp[o0 + r] + eb + t];
-                }
-                __syncthreads();
-#pragma unroll 2
-                for (int t = 0; t < c; ++t) {
-                    const double* q = Qt + sc[t];
-                    double x[U];
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int j = j0 + threadIdx.x + 256 * u;
-                        x[u] = j < m ? q[j] : 0.0;
-                    }
-#pragma unroll
-                    for (int r = 0; r < kSpmmGroup; ++r)
-                        if (r < G) {
-                            const double a = sv[r][t];
-#pragma unroll
-                            for (int u = 0; u < U; ++u) acc[r][u] = fma(a, x[u], acc[r][u]);
-                        }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kSpmmGroup; ++r)
-                if (r < G) {
-                    double* out = Rt + inv[o0 + r] * ld;
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int j = j0 + threadIdx.x + 256 * u;
-                        if (j < m) out[j] = acc[r][u];
-                    }
-                }
-        }
+cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
+                             const int64_t* inv, const double* zt, int m, int64_t ld, double* norms,
+                             cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * (size_t)(m > 0 ? m : 0), s);
+    if (e != cudaSuccess || nsup <= 0 || m <= 0) return e;
+    const int u = spmmU(m);
+    const dim3 grid(gridFor(nsup * kSpmmThreads, kSpmmThreads), (m + kSpmmThreads * u - 1) / (kSpmmThreads * u));
+    switch (u) {
+        case 2: mnormSuperKernel<2><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, zt, m, ld, norms); break;
+        case 4: mnormSuperKernel<4><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, zt, m, ld, norms); break;
+        case 6: mnormSuperKernel<6><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, zt, m, ld, norms); break;
+        default: mnormSuperKernel<8><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, zt, m, ld, norms); break;
     }
-}
-
-cudaError_t launchSpmmGroupT(const int64_t* rp, const int32_t* ci, const double* v, int64_t ngrp,
-                             const int64_t* grp, const int64_t* inv, const double* Qt, int m,
-                             int64_t ld, double* Rt, cudaStream_t s) {
-    if (ngrp <= 0 || m <= 0) return cudaSuccess;
-    const int grid = gridFor(ngrp * 256, 256);
-    const int u = (m + 255) / 256;
-    if (u <= 1)
-        spmmGroupKernel<1><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
-    else if (u == 2)
-        spmmGroupKernel<2><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
-    else if (u == 3)
-        spmmGroupKernel<3><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
-    else
-        spmmGroupKernel<4><<<grid, 256, 0, s>>>(rp, ci, v, ngrp, grp, inv, Qt, m, ld, Rt);
     return cudaGetLastError();
 }
 
