@@ -489,12 +489,15 @@ cudaError_t launchBisect(const EigDesc* d, int nDesc, int mode, int want, double
 }
 
 // ------------------------------------------------------------------------
-// inverse iteration (dlagtf / dlagts / dstein), one CTA per cluster
+// inverse iteration (dlagtf / dlagts / dstein), one warp-sized CTA per cluster
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restrict__ descs,
+__global__ void __launch_bounds__(32) inverseIterKernel(const EigDesc* __restrict__ descs,
                                                           int maxK) {
+    constexpr int kIiChunk = 256;
     __shared__ double red[32];
     __shared__ double sh[4];
+    __shared__ double sIn0[kIiChunk + 1], sIn1[kIiChunk + 1], sC[kIiChunk], sPiv[kIiChunk], sDd[kIiChunk],
+        sB[kIiChunk], sInv[kIiChunk], sOut[kIiChunk];
     const int b = blockIdx.y;
     const int j = blockIdx.x;
     const EigDesc D = descs[b];
@@ -506,12 +509,14 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
     // closer than 1e-3 |T|; that makes clusters of hundreds of the reduced
     // problem's eigenvalues and serialises them.  Vectors of eigenvalues
     // separated by g come out of inverse iteration orthogonal to about
-    // eps |T| / g, so grouping only gaps below 1e-6 |T| keeps every pair
-    // orthogonal to ~1e-10 while the clusters stay small and run in
-    // parallel (one CTA each).
+    // eps |T| / g, so grouping only gaps below 1e-8 |T| keeps every pair
+    // orthogonal to ~2e-8 while clusters stay rare and every vector runs
+    // in parallel (one CTA each).  The inverted spectra (1 / lambda) of the
+    // AMLS problems crowd their upper eigenvalues within 1e-6 |T| of each
+    // other, which a wider tolerance would chain into long serial clusters.
     double lo, hi, pivmin, tnorm;
     gershgorin(D.d, D.e, n, lo, hi, pivmin, tnorm);
-    const double ortol = 1e-6 * tnorm;
+    const double ortol = 1e-8 * tnorm;
     // cluster start: j is a start if j == 0 or |w[j] - w[j-1]| > ortol
     if (j > 0 && fabs(D.w[j] - D.w[j - 1]) <= ortol) return;
     int jend = j + 1;
@@ -520,9 +525,8 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
         if (tid == 0) D.Y[0 + (int64_t)j * D.ldy] = 1.0;
         return;
     }
-    // scratch: a, b(super), c(sub), dd(2nd super), 1/a (guarded), piv  (6n doubles)
+    // scratch: (unused), b(super), c(sub), dd(2nd super), 1/a (guarded), piv  (6n doubles)
     double* W = D.work + (int64_t)j * 6 * n;
-    double* a = W;
     double* bs = W + n;
     double* c = W + 2 * n;
     double* dd = W + 3 * n;
@@ -541,57 +545,65 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
         }
         prevLam = lam;
         double* x = D.Y + (int64_t)jj * D.ldy;
-        // LU with partial pivoting of T - lam I (dlagtf), on one thread.  The
-        // recurrence carries the current pivot row (ak, bk) in registers and
-        // only writes the factors, so the chain is arithmetic, not memory;
-        // no interchange when |c|/scale2 <= |a|/scale1 (compared without
-        // divisions; a zero row a = b = 0 always interchanges).
-        // ainv holds the guarded reciprocals of the U diagonal.
-        if (tid == 0) {
-            const double* __restrict__ dg = D.d;
-            const double* __restrict__ eg = D.e;
-            double* __restrict__ aw = a;
-            double* __restrict__ bw = bs;
-            double* __restrict__ cw = c;
-            double* __restrict__ dw = dd;
-            double* __restrict__ pw = piv;
-            double* __restrict__ iw = ainv;
-            double ak = dg[0] - lam, bk = n > 1 ? eg[0] : 0.0;
-#pragma unroll 4
-            for (int kk = 0; kk + 1 < n; ++kk) {
-                const double ck = eg[kk];
-                const double a1 = dg[kk + 1] - lam;
-                const double b1 = (kk + 2 < n) ? eg[kk + 1] : 0.0;
-                const double scale1 = fabs(ak) + fabs(bk);
-                const double scale2 = fabs(ck) + fabs(a1) + fabs(b1);
-                double ua, ub, na, nb;   // stored U row kk, carried row kk + 1
-                if (ck == 0.0 || scale2 == 0.0 || (scale1 > 0.0 && fabs(ck) * scale1 <= fabs(ak) * scale2)) {
-                    const double mult = (ck == 0.0 || ak == 0.0) ? 0.0 : ck / ak;
-                    pw[kk] = 0.0;
-                    cw[kk] = mult;
-                    ua = ak;
-                    ub = bk;
-                    na = a1 - mult * bk;
-                    nb = b1;
-                    dw[kk] = 0.0;
-                } else {
-                    const double mult = ak / ck;
-                    pw[kk] = 1.0;
-                    cw[kk] = mult;
-                    ua = ck;
-                    ub = a1;
-                    na = bk - mult * a1;
-                    dw[kk] = b1;
-                    nb = -mult * b1;
+        // LU with partial pivoting of T - lam I (dlagtf).  The recurrence runs
+        // on one thread and carries the current pivot row (ak, bk) in
+        // registers; its inputs and outputs pass through shared memory in
+        // chunks of kIiChunk that the whole CTA loads and stores, so the
+        // serial chain never waits on global memory.  No interchange when
+        // |c|/scale2 <= |a|/scale1 (compared without divisions; a zero row
+        // a = b = 0 always interchanges).  ainv holds the guarded
+        // reciprocals of the U diagonal.
+        {
+            double ak = 0.0, bk = 0.0;
+            for (int k0 = 0; k0 + 1 < n; k0 += kIiChunk) {
+                const int cnt = min(kIiChunk, n - 1 - k0);     // steps kk = k0 .. k0 + cnt - 1
+                __syncthreads();
+                for (int i = tid; i <= cnt; i += blockDim.x) {
+                    const int kk = k0 + i;                      // e[kk], d[kk + 1] (i < cnt), e[kk + 1]
+                    sIn0[i] = kk < n - 1 ? D.e[kk] : 0.0;
+                    sIn1[i] = (i < cnt) ? D.d[kk + 1] : 0.0;
                 }
-                aw[kk] = ua;
-                bw[kk] = ub;
-                iw[kk] = 1.0 / (fabs(ua) < tol ? (ua >= 0.0 ? tol : -tol) : ua);
-                ak = na;
-                bk = nb;
+                if (k0 == 0 && tid == 0) {
+                    ak = D.d[0] - lam;
+                    bk = D.e[0];
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    // branch-free step: both pivot choices share one division
+                    for (int i = 0; i < cnt; ++i) {
+                        const int kk = k0 + i;
+                        const double ck = sIn0[i];
+                        const double a1 = sIn1[i] - lam;
+                        const double b1 = (kk + 2 < n) ? sIn0[i + 1] : 0.0;
+                        const double scale1 = fabs(ak) + fabs(bk);
+                        const double scale2 = fabs(ck) + fabs(a1) + fabs(b1);
+                        const bool keep = ck == 0.0 || scale2 == 0.0 ||
+                                          (scale1 > 0.0 && fabs(ck) * scale1 <= fabs(ak) * scale2);
+                        // keep: mult = c / a (0 when either is 0); swap: mult = a / c, c != 0
+                        const double q = (keep ? ck : ak) / (keep ? ak : ck);
+                        const double mult = (keep && (ck == 0.0 || ak == 0.0)) ? 0.0 : q;
+                        const double ua = keep ? ak : ck;                       // stored U row kk
+                        sPiv[i] = keep ? 0.0 : 1.0;
+                        sC[i] = mult;
+                        sB[i] = keep ? bk : a1;
+                        sDd[i] = keep ? 0.0 : b1;
+                        sInv[i] = 1.0 / (fabs(ua) < tol ? (ua >= 0.0 ? tol : -tol) : ua);
+                        const double na = keep ? fma(-mult, bk, a1) : fma(-mult, a1, bk);   // carried row kk + 1
+                        const double nb = keep ? b1 : -mult * b1;
+                        ak = na;
+                        bk = nb;
+                    }
+                    if (k0 + cnt == n - 1) ainv[n - 1] = 1.0 / (fabs(ak) < tol ? (ak >= 0.0 ? tol : -tol) : ak);
+                }
+                __syncthreads();
+                for (int i = tid; i < cnt; i += blockDim.x) {
+                    piv[k0 + i] = sPiv[i];
+                    c[k0 + i] = sC[i];
+                    dd[k0 + i] = sDd[i];
+                    bs[k0 + i] = sB[i];
+                    ainv[k0 + i] = sInv[i];
+                }
             }
-            aw[n - 1] = ak;
-            iw[n - 1] = 1.0 / (fabs(ak) < tol ? (ak >= 0.0 ? tol : -tol) : ak);
         }
         // deterministic start vector
         for (int i = tid; i < n; i += blockDim.x) {
@@ -602,39 +614,63 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
             x[i] = ((h & 0xffffff) / double(0x1000000)) - 0.5 + 1e-3;
         }
         __syncthreads();
-        for (int it = 0; it < 4; ++it) {
-            if (tid == 0) {
-                // apply L^-1 with interchanges, then U^-1 (dlagts, job -1),
-                // carrying the running components in registers
-                const double* __restrict__ cw = c;
-                const double* __restrict__ pw = piv;
-                const double* __restrict__ bw = bs;
-                const double* __restrict__ dw = dd;
-                const double* __restrict__ iw = ainv;
-                double cur = x[0];
+        // three solves, as dstein takes once the growth test passes (one
+        // solve reaches it from an eigenvalue accurate to eps |T|, then
+        // EXTRA = 2 more)
+        for (int it = 0; it < 3; ++it) {
+            // apply L^-1 with interchanges, then U^-1 (dlagts, job -1): one
+            // thread carries the running components in registers, the CTA
+            // stages the operands and the results chunk by chunk
+            double cur = 0.0;
+            for (int k0 = 0; k0 + 1 < n; k0 += kIiChunk) {
+                const int cnt = min(kIiChunk, n - 1 - k0);     // kk = k0 .. k0 + cnt - 1 reads x[kk + 1]
+                __syncthreads();
+                for (int i = tid; i < cnt; i += blockDim.x) {
+                    sIn0[i] = x[k0 + i + 1];
+                    sC[i] = c[k0 + i];
+                    sPiv[i] = piv[k0 + i];
+                }
+                if (k0 == 0 && tid == 0) cur = x[0];
+                __syncthreads();
+                if (tid == 0) {
+                    // branch-free, so that the shared-memory loads of later
+                    // steps issue ahead of the dependent chain
 #pragma unroll 8
-                for (int kk = 0; kk + 1 < n; ++kk) {
-                    const double nxt = x[kk + 1];
-                    if (pw[kk] == 0.0) {
-                        x[kk] = cur;
-                        cur = nxt - cw[kk] * cur;
-                    } else {
-                        x[kk] = nxt;
-                        cur = cur - cw[kk] * nxt;
+                    for (int i = 0; i < cnt; ++i) {
+                        const double nxt = sIn0[i], ci = sC[i];
+                        const bool sw = sPiv[i] != 0.0;
+                        sOut[i] = sw ? nxt : cur;
+                        cur = sw ? fma(-ci, nxt, cur) : fma(-ci, cur, nxt);
+                    }
+                    if (k0 + cnt == n - 1) x[n - 1] = cur;
+                }
+                __syncthreads();
+                for (int i = tid; i < cnt; i += blockDim.x) x[k0 + i] = sOut[i];
+            }
+            double x1 = 0.0, x2 = 0.0;     // x[kk + 1], x[kk + 2] of the result
+            for (int k1 = n; k1 > 0; k1 -= kIiChunk) {
+                const int k0 = max(0, k1 - kIiChunk), cnt = k1 - k0;
+                __syncthreads();
+                for (int i = tid; i < cnt; i += blockDim.x) {
+                    const int kk = k0 + i;
+                    sIn0[i] = x[kk];
+                    sB[i] = kk + 1 < n ? bs[kk] : 0.0;       // U's superdiagonals end at n-2, n-3
+                    sDd[i] = kk + 2 < n ? dd[kk] : 0.0;
+                    sInv[i] = ainv[kk];
+                }
+                __syncthreads();
+                if (tid == 0) {
+#pragma unroll 8
+                    for (int i = cnt - 1; i >= 0; --i) {
+                        const double t = fma(-sB[i], x1, fma(-sDd[i], x2, sIn0[i]));
+                        const double v = t * sInv[i];
+                        sOut[i] = v;
+                        x2 = x1;
+                        x1 = v;
                     }
                 }
-                x[n - 1] = cur;
-                double x1 = 0.0, x2 = 0.0;     // x[kk + 1], x[kk + 2]
-#pragma unroll 8
-                for (int kk = n - 1; kk >= 0; --kk) {
-                    double t = x[kk];
-                    if (kk + 1 < n) t -= bw[kk] * x1;
-                    if (kk + 2 < n) t -= dw[kk] * x2;
-                    const double v = t * iw[kk];
-                    x[kk] = v;
-                    x2 = x1;
-                    x1 = v;
-                }
+                __syncthreads();
+                for (int i = tid; i < cnt; i += blockDim.x) x[k0 + i] = sOut[i];
             }
             __syncthreads();
             // reorthogonalise against earlier members of the cluster (MGS)
@@ -682,7 +718,9 @@ __global__ void __launch_bounds__(256) inverseIterKernel(const EigDesc* __restri
 cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int*, cudaStream_t s) {
     if (nDesc <= 0 || maxK <= 0) return cudaSuccess;
     dim3 grid(maxK, nDesc);
-    inverseIterKernel<<<grid, 256, 0, s>>>(d, maxK);
+    // one warp per cluster: the serial recurrences run on one thread, so a
+    // small CTA lets every wanted vector of a large problem run at once
+    inverseIterKernel<<<grid, 32, 0, s>>>(d, maxK);
     return cudaGetLastError();
 }
 
