@@ -38,6 +38,21 @@ __device__ __forceinline__ double blockSum(double v, double* red) {
     return t;
 }
 
+// Block-wide sum with one barrier: every warp reduces the per-warp partials
+// itself (same order in every warp, so all threads get the same bits).
+// `red` holds 64 doubles used alternately (parity flips per call); two calls
+// in a row are safe because the second writes the other half and a third
+// call's barrier follows the first call's reads.
+__device__ __forceinline__ double blockSum1(double v, double* red, int& parity) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    double* r = red + 32 * parity;
+    parity ^= 1;
+    v = warpSum<32>(v);
+    if (lane == 0) r[wid] = v;
+    __syncthreads();
+    return warpSum<32>(lane < nw ? r[lane] : 0.0);
+}
+
 __device__ __forceinline__ double blockMax(double v, double* red) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll

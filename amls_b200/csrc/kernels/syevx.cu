@@ -223,6 +223,8 @@ struct LargeArgs {
 __global__ void __launch_bounds__(kTridiagLargeThreads) tridiagLargeKernel(LargeArgs a) {
     extern __shared__ double sm[];   // vA (maxN), vB (maxN), w (maxN)
     __shared__ double red[32];
+    __shared__ double red2[64];
+    int par = 0;
     constexpr int SEG = 256;
     cg::grid_group grid = cg::this_grid();
     const int g = a.groupOf[blockIdx.x];
@@ -275,31 +277,44 @@ __global__ void __launch_bounds__(kTridiagLargeThreads) tridiagLargeKernel(Large
             const int m1 = m - 1;           // order of the next one, C = B(1:, 1:)
             const double* p = pbase + (int64_t)(k % kTridiagPBufs) * n;
             double* B = A + (k + 1) + (int64_t)(k + 1) * lda;
-            // w = p - tau/2 (p . v) v
+            // p_k and the first column of B are loaded together; then, in the
+            // registers of the thread owning each index, w = p - tau/2 (p . v) v
+            // and the updated first column b0 = B(:,0) - v w0 - w v0 (v0 = 1),
+            // from whose tail the next reflector is built.  Two one-barrier
+            // reductions and one barrier per column inside the CTA.
+            const double pFirst = p[0], pSecond = p[1], bFirst = B[0], bSecond = B[1];
             double pv = 0.0;
-            for (int i = tid; i < m; i += bd) pv += p[i] * vcur[i];
-            pv = blockSum(pv, red);
+            for (int i = tid; i < m; i += bd) {
+                const double pi = p[i];
+                sw[i] = pi;
+                pv += pi * vcur[i];
+                if (i >= 2) vnext[i - 1] = B[i];
+            }
+            pv = blockSum1(pv, red2, par);
             const double a2 = -0.5 * h.tau * pv;
-            for (int i = tid; i < m; i += bd) sw[i] = p[i] + a2 * vcur[i];
-            __syncthreads();
-            // updated first column of B, b0 = B(:,0) - v w0 - w v0 (v0 = 1);
-            // the next reflector is built from b0(1:)
-            const double w0 = sw[0], v0 = vcur[0];
-            const double b00 = B[0] - (v0 * w0 + w0 * v0);
-            const double alpha = B[1] - (vcur[1] * w0 + sw[1] * v0);
-            HouseholderScalars hn{0.0, 0.0, 0.0};
-            if (m1 >= 2) {
-                double part = 0.0;
-                for (int i = 2 + tid; i < m; i += bd) {
-                    const double b = B[i] - (vcur[i] * w0 + sw[i] * v0);
+            const double v0 = vcur[0];
+            const double w0 = pFirst + a2 * v0;
+            double part = 0.0;
+            for (int i = tid; i < m; i += bd) {
+                const double wi = sw[i] + a2 * vcur[i];
+                sw[i] = wi;
+                if (i >= 2) {
+                    const double b = vnext[i - 1] - (vcur[i] * w0 + wi * v0);
                     vnext[i - 1] = b;
                     part += b * b;
                 }
-                hn = makeReflector(alpha, blockSum(part, red));
+            }
+            const double w1 = pSecond + a2 * vcur[1];
+            const double b00 = bFirst - (v0 * w0 + w0 * v0);
+            const double alpha = bSecond - (vcur[1] * w0 + w1 * v0);
+            HouseholderScalars hn{0.0, 0.0, 0.0};
+            if (m1 >= 2) {
+                // the reduction's barrier orders every vnext write before the scaling
+                hn = makeReflector(alpha, blockSum1(part, red2, par));
                 for (int i = 1 + tid; i < m1; i += bd) vnext[i] *= hn.scale;
                 if (tid == 0) vnext[0] = 1.0;
-                __syncthreads();
             }
+            __syncthreads();
             if (rank == 0) {
                 // reflector k into column k; nothing else reads that column now
                 double* col = A + (k + 1) + (int64_t)k * lda;
@@ -312,7 +327,7 @@ __global__ void __launch_bounds__(kTridiagLargeThreads) tridiagLargeKernel(Large
                     if (m1 < 2) {           // last column step: the 2 x 2 tail
                         D.e[k + 1] = alpha;
                         D.tau[k + 1] = 0.0;
-                        D.d[k + 2] = B[1 + lda] - (vcur[1] * sw[1] + sw[1] * vcur[1]);
+                        D.d[k + 2] = B[1 + lda] - (vcur[1] * w1 + w1 * vcur[1]);
                     }
                 }
             }
