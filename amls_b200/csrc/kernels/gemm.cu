@@ -3,8 +3,8 @@
 //
 // B200 has no FP64 tcgen05 kind; its FP64 tensor-core path is the warp-level
 // DMMA (mma.sync .f64), which these kernels use: 64 x 64 output tile per CTA,
-// 8 warps as 2 (M) x 4 (N), warp tile 32 x 16 = 2 x 2 fragments of
-// m16n8k16, operands streamed global -> shared memory with cp.async through a
+// 4 warps as 2 (M) x 2 (N), warp tile 32 x 32 = 2 x 4 fragments of
+// m16n8k16 (the front update: 8 warps of 32 x 16), operands streamed global -> shared memory with cp.async through a
 // three-deep ring of K slices of 16 (one barrier per slice, no register
 // staging).  The operand layout (transposed A / B, gathered A columns) is a
 // template parameter selected per CTA from the descriptor, so the copy loops
@@ -15,7 +15,9 @@
 namespace amls_b200 {
 
 namespace {
-constexpr int NT = 256;
+constexpr int NT = 256;            // front update
+constexpr int kGemmThreads = 128;  // batched GEMM: 4 warps of 32 x 32
+constexpr int kFJ = 4;             // n8 fragments per warp (warp tile 32 x 8 kFJ)
 
 constexpr int kBM = kGemmTile, kBN = kGemmTile;   // 64 x 64
 constexpr int kKs = 16;                            // K slice
@@ -23,7 +25,7 @@ constexpr int kStages = 3;
 constexpr int kLdA = kBM + 4, kLdB = kBN + 4;      // = 4 mod 16 doubles
 constexpr int kStage = kKs * (kLdA + kLdB);        // doubles per stage
 constexpr size_t kGemmSmem = sizeof(double) * kStages * kStage;
-constexpr int kLA = kBM * kKs / NT, kLB = kBN * kKs / NT;
+constexpr int kLA = kBM * kKs / kGemmThreads, kLB = kBN * kKs / kGemmThreads;
 
 __device__ __forceinline__ void dmma16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
     asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
@@ -50,7 +52,7 @@ __device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, in
                                            double* As, double* Bs) {
 #pragma unroll
     for (int u = 0; u < kLA; ++u) {
-        const int idx = threadIdx.x + NT * u;
+        const int idx = threadIdx.x + kGemmThreads * u;
         const int i = TA ? idx / kKs : idx % kBM;
         const int k = TA ? idx % kKs : idx / kBM;
         const int gi = m0 + i, gk = k0 + k;
@@ -65,7 +67,7 @@ __device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, in
     }
 #pragma unroll
     for (int u = 0; u < kLB; ++u) {
-        const int idx = threadIdx.x + NT * u;
+        const int idx = threadIdx.x + kGemmThreads * u;
         const int j = TB ? idx % kBN : idx / kKs;
         const int k = TB ? idx / kBN : idx % kKs;
         const int gj = n0 + j, gk = k0 + k;
@@ -81,12 +83,12 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
     const int m0 = t.m0, n0 = t.n0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, tg = lane & 3;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
-    double acc[2][2][4];
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    double acc[2][kFJ][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < kFJ; ++j)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
     // split-K range; triangular B restricts k to <= the tile's last column
@@ -118,7 +120,7 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
         const double* As = sm + (sl % kStages) * kStage;
         const double* Bs = As + kKs * kLdA;
         // fragments: A element (row g (+8), k tg + 4 q), B element (k tg + 4 q, col g)
-        double a[2][8], b[2][4];
+        double a[2][8], b[kFJ][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int r = wm + 16 * i + g;
@@ -129,7 +131,7 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
             }
         }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < kFJ; ++j) {
             const int c = wn + 8 * j + g;
 #pragma unroll
             for (int q = 0; q < 4; ++q) b[j][q] = Bs[(tg + 4 * q) * kLdB + c];
@@ -137,13 +139,13 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
+            for (int j = 0; j < kFJ; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
     }
     cpAsyncWait<0>();
     // epilogue: fragment (i, j) element q sits at row wm + 16 i + g + 8 (q / 2),
     // column wn + 8 j + 2 tg + (q % 2)
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < kFJ; ++j)
 #pragma unroll
         for (int q2 = 0; q2 < 2; ++q2) {
             const int col = n0 + wn + 8 * j + 2 * tg + q2;
@@ -173,7 +175,7 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
 }
 }  // namespace
 
-__global__ void __launch_bounds__(NT) gemmBatchedKernel(const GemmDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kGemmThreads, 3) gemmBatchedKernel(const GemmDesc* __restrict__ descs,
                                                         const TileRef* __restrict__ tiles) {
     extern __shared__ double gemmSmem[];
     const TileRef t = tiles[blockIdx.x];
@@ -202,7 +204,7 @@ cudaError_t launchGemmBatched(const GemmDesc* dDescs, const TileRef* dTiles, int
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    gemmBatchedKernel<<<nTiles, NT, kGemmSmem, s>>>(dDescs, dTiles);
+    gemmBatchedKernel<<<nTiles, kGemmThreads, kGemmSmem, s>>>(dDescs, dTiles);
     return cudaGetLastError();
 }
 
