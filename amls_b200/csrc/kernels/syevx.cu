@@ -28,7 +28,8 @@ namespace cg = cooperative_groups;
 namespace amls_b200 {
 
 namespace {
-constexpr int kSmallThreads = 512;
+constexpr int kSmallThreads = 768;
+constexpr int kSmallPerLane = (kTridiagSmallMax + 31) / 32;   // column loads per lane
 }
 
 // ------------------------------------------------------------------------
@@ -66,6 +67,7 @@ __global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDes
     __shared__ double v0[kTridiagSmallMax], v1[kTridiagSmallMax], sw[kTridiagSmallMax];
     __shared__ double p0[kTridiagSmallMax], p1[kTridiagSmallMax];
     __shared__ double red[32];
+    __shared__ double red2[64];
     const EigDesc D = descs[blockIdx.x];
     const int n = D.n;
     double* A = D.A;
@@ -104,31 +106,42 @@ __global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDes
         }
         __syncthreads();
     }
+    int par = 0;
     for (int k = 0; k + 2 < n; ++k) {
         const int m = n - k - 1, m1 = m - 1;
         double* B = A + (k + 1) + (int64_t)(k + 1) * lda;
+        // w = p - tau/2 (p . v) v and the updated first column of B in the
+        // registers of the thread owning each index (as tridiagLargeKernel)
+        const double bFirst = B[0], bSecond = B[1];
         double pv = 0.0;
-        for (int i = tid; i < m; i += bd) pv += p[i] * vcur[i];
-        pv = blockSum(pv, red);
+        for (int i = tid; i < m; i += bd) {
+            pv += p[i] * vcur[i];
+            if (i >= 2) vnext[i - 1] = B[i];
+        }
+        pv = blockSum1(pv, red2, par);
         const double a2 = -0.5 * h.tau * pv;
-        for (int i = tid; i < m; i += bd) sw[i] = p[i] + a2 * vcur[i];
-        __syncthreads();
-        const double w0 = sw[0];
-        const double b00 = B[0] - (w0 + w0);
-        const double alpha = B[1] - (vcur[1] * w0 + sw[1]);
-        HouseholderScalars hn{0.0, 0.0, 0.0};
-        if (m1 >= 2) {
-            double part = 0.0;
-            for (int i = 2 + tid; i < m; i += bd) {
-                const double b = B[i] - (vcur[i] * w0 + sw[i]);
+        const double w0 = p[0] + a2 * vcur[0];
+        double part = 0.0;
+        for (int i = tid; i < m; i += bd) {
+            const double wi = p[i] + a2 * vcur[i];
+            sw[i] = wi;
+            if (i >= 2) {
+                const double b = vnext[i - 1] - (vcur[i] * w0 + wi);
                 vnext[i - 1] = b;
                 part += b * b;
             }
-            hn = makeReflector(alpha, blockSum(part, red));
+        }
+        const double w1 = p[1] + a2 * vcur[1];
+        const double b00 = bFirst - (w0 + w0);
+        const double alpha = bSecond - (vcur[1] * w0 + w1);
+        HouseholderScalars hn{0.0, 0.0, 0.0};
+        if (m1 >= 2) {
+            // the reduction's barrier orders every vnext write before the scaling
+            hn = makeReflector(alpha, blockSum1(part, red2, par));
             for (int i = 1 + tid; i < m1; i += bd) vnext[i] *= hn.scale;
             if (tid == 0) vnext[0] = 1.0;
-            __syncthreads();
         }
+        __syncthreads();
         {
             double* col = A + (k + 1) + (int64_t)k * lda;
             for (int i = tid; i < m; i += bd) col[i] = vcur[i];
@@ -140,7 +153,7 @@ __global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDes
                 if (m1 < 2) {
                     D.e[k + 1] = alpha;
                     D.tau[k + 1] = 0.0;
-                    D.d[k + 2] = B[1 + lda] - 2.0 * vcur[1] * sw[1];
+                    D.d[k + 2] = B[1 + lda] - 2.0 * vcur[1] * w1;
                 }
             }
         }
@@ -149,28 +162,28 @@ __global__ void __launch_bounds__(kSmallThreads) tridiagSmallKernel(const EigDes
             const double* vp = vcur + 1;
             const double* wp = sw + 1;
             const bool upd = h.tau != 0.0;
+            // one warp per column; the whole column (m1 <= 383) is loaded in
+            // one batch of kSmallPerLane loads per lane
             for (int j = wid; j < m1; j += nw) {
                 double* cj = C + (int64_t)j * lda;
                 const double vj = vp[j], wj = wp[j];
+                double cv[kSmallPerLane];
+#pragma unroll
+                for (int t = 0; t < kSmallPerLane; ++t) {
+                    const int i = lane + 32 * t;
+                    cv[t] = i < m1 ? cj[i] : 0.0;
+                }
                 double sum = 0.0;
-                for (int i0 = 0; i0 < m1; i0 += 256) {
-                    double cv[8];
 #pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const int i = i0 + lane + 32 * t;
-                        cv[t] = i < m1 ? cj[i] : 0.0;
-                    }
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const int i = i0 + lane + 32 * t;
-                        if (i < m1) {
-                            double c = cv[t];
-                            if (upd) {
-                                c -= vp[i] * wj + wp[i] * vj;
-                                cj[i] = c;
-                            }
-                            sum += c * vnext[i];
+                for (int t = 0; t < kSmallPerLane; ++t) {
+                    const int i = lane + 32 * t;
+                    if (i < m1) {
+                        double c = cv[t];
+                        if (upd) {
+                            c -= vp[i] * wj + wp[i] * vj;
+                            cj[i] = c;
                         }
+                        sum += c * vnext[i];
                     }
                 }
                 sum = warpSum<32>(sum);
