@@ -678,11 +678,22 @@ void Engine::tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, De
         int64_t pTot = 0;
         double wsum = 0;
         for (auto& e : part) wsum += static_cast<double>(e.n) * e.n;
-        int used = 0;
+        std::vector<int> cta(static_cast<size_t>(cnt));
+        int used = 0, big = 0;
         for (int g = 0; g < cnt; ++g) {
             const double share = static_cast<double>(part[static_cast<size_t>(g)].n) * part[static_cast<size_t>(g)].n / wsum;
             int c = std::max(1, static_cast<int>(std::floor(maxCta * share)));
             c = std::max(1, std::min(c, maxCta - used - (cnt - g - 1)));
+            cta[static_cast<size_t>(g)] = c;
+            used += c;
+            if (part[static_cast<size_t>(g)].n > part[static_cast<size_t>(big)].n) big = g;
+        }
+        // the CTAs the rounding leaves over go to the largest matrix, whose
+        // column steps set the length of the launch
+        cta[static_cast<size_t>(big)] += maxCta - used;
+        used = 0;
+        for (int g = 0; g < cnt; ++g) {
+            const int c = cta[static_cast<size_t>(g)];
             groupFirst.push_back(used);
             groupSize.push_back(c);
             for (int q = 0; q < c; ++q) groupOf.push_back(g);

@@ -430,16 +430,43 @@ int tridiagLargeMaxCtas(int maxN) {
 // ------------------------------------------------------------------------
 // bisection (Sturm counts)
 // ------------------------------------------------------------------------
-__device__ __forceinline__ int sturmLess(const double* d, const double* e, int n, double x,
-                                         double pivmin) {
-    int cnt = 0;
-    double q = d[0] - x;
-    if (fabs(q) < pivmin) q = -pivmin;
-    cnt += q < 0.0;
+// Number of eigenvalues of T below x: the sign changes of the Sturm
+// sequence of leading principal minors
+//   p_{-1} = 1, p_0 = d_0 - x, p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2},
+// i.e. the ratios q_i = p_i / p_{i-1} = (d_i - x) - e_{i-1}^2 / q_{i-1} of
+// LAPACK's dstebz counted negative, but without a division on the serial
+// chain (one FMA and a guard per step).  T is scaled by s = 2^-k >= 1/|T|
+// (exact), so |d_i - x| <= 4 and e^2 <= 1 after scaling; a ratio smaller
+// than piv = max(s pivmin, 2^-100) in magnitude is replaced by -piv (dstebz's
+// pivmin rule, moving d_i by at most 2^-100 |T|), which bounds |q| to
+// [2^-100, 2^101] and lets (p_{i-1}, p_i) be rescaled by a power of two
+// only every fourth step.
+__device__ __forceinline__ int sturmLess(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                         double x, double pivmin, double tnorm) {
+    int k = 0;
+    frexp(tnorm > 0.0 ? tnorm : 1.0, &k);
+    const double s = ldexp(1.0, -k), s2 = s * s;
+    const double xs = x * s;
+    const double piv = fmax(pivmin * s, 0x1p-100);
+    double p2 = 1.0;                       // p_{i-2}
+    double p1 = fma(d[0], s, -xs);         // p_{i-1}
+    if (fabs(p1) < piv) p1 = -piv;
+    int cnt = p1 < 0.0;
     for (int i = 1; i < n; ++i) {
-        q = d[i] - x - e[i - 1] * e[i - 1] / q;
-        if (fabs(q) < pivmin) q = -pivmin;
-        cnt += q < 0.0;
+        const double t = fma(d[i], s, -xs);
+        const double c = e[i - 1] * e[i - 1] * s2;
+        double pn = fma(t, p1, -c * p2);
+        if (fabs(pn) < piv * fabs(p1)) pn = -piv * p1;
+        cnt += (pn < 0.0) != (p1 < 0.0);
+        p2 = p1;
+        p1 = pn;
+        if ((i & 3) == 0) {
+            // rescale by 2^-(exponent of p1); |p2 / p1| lies in [2^-101, 2^100]
+            const int ex = (__double2hiint(p1) >> 20) & 0x7ff;
+            const double sc = __hiloint2double((2046 - ex) << 20, 0);
+            p1 *= sc;
+            p2 *= sc;
+        }
     }
     return cnt;
 }
@@ -476,7 +503,7 @@ __global__ void bisectCountKernel(const EigDesc* __restrict__ descs, int nDesc, 
     else {
         double lo, hi, pivmin, tn;
         gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
-        const int less = sturmLess(D.d, D.e, n, thr, pivmin);
+        const int less = sturmLess(D.d, D.e, n, thr, pivmin, tn);
         k = (mode == 1) ? (n - less) : less;
     }
     *D.kOut = min(k, D.kcap);
@@ -499,7 +526,7 @@ __global__ void bisectKernel(const EigDesc* __restrict__ descs, int mode, int ma
             mid >= hi)
             break;
         // count(< mid) >= t  <=>  lambda_t < mid
-        if (sturmLess(D.d, D.e, n, mid, pivmin) >= t) hi = mid;
+        if (sturmLess(D.d, D.e, n, mid, pivmin, tn) >= t) hi = mid;
         else lo = mid;
     }
     D.w[j] = 0.5 * (lo + hi);
@@ -804,7 +831,7 @@ __global__ void __launch_bounds__(256) bisectWarpKernel(const EigDesc* __restric
     for (int it = 0; it < 40; ++it) {
         if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
         const double x = lo + (hi - lo) * (lane + 1) / 33.0;
-        const bool ge = sturmLess(D.d, D.e, n, x, pivmin) >= t;   // lambda_t < x
+        const bool ge = sturmLess(D.d, D.e, n, x, pivmin, tn) >= t;   // lambda_t < x
         const unsigned m = __ballot_sync(0xffffffffu, ge);
         // first lane whose point is above lambda_t
         const int f = m ? __ffs(m) - 1 : 32;
