@@ -94,6 +94,7 @@ Engine::Engine(int device) : device_(device) {
 
 Engine::~Engine() {
     cudaSetDevice(device_);
+    dropGraphs();
     for (cudaEvent_t e : evPool_) cudaEventDestroy(e);
     if (evSolve0_) cudaEventDestroy(evSolve0_);
     if (evSolve1_) cudaEventDestroy(evSolve1_);
@@ -181,6 +182,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
     analyzed_ = false;
     tridiagDone_ = false;
+    dropGraphs();              // the tables (and buffers) they replay are rebuilt
     if (n <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty matrix");
     for (int64_t r = 0; r < n; ++r) {
         if (kp[r + 1] < kp[r] || mp[r + 1] < mp[r])
@@ -617,7 +619,43 @@ void Engine::buildStatic() {
 // ---------------------------------------------------------------------------
 // elimination
 // ---------------------------------------------------------------------------
+// The elimination is a fixed launch schedule over tables built by analyze:
+// captured once into a CUDA graph and replayed by every later numeric solve
+// (the per-launch event instrumentation, when on, runs it eagerly).
 void Engine::eliminate(cudaStream_t s) {
+    if (profiling_) {
+        eliminateLaunches(s);
+        return;
+    }
+    if (!elimExec_) {
+        cudaGraph_t g = nullptr;
+        cudaCheck(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "capture elimination");
+        const int64_t l0 = launches_;
+        try {
+            eliminateLaunches(s);
+        } catch (...) {
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        cudaCheck(cudaStreamEndCapture(s, &g), "capture elimination");
+        elimLaunches_ = launches_ - l0;
+        launches_ = l0;
+        const cudaError_t e = cudaGraphInstantiate(&elimExec_, g, 0);
+        cudaGraphDestroy(g);
+        cudaCheck(e, "instantiate elimination graph");
+    }
+    cudaCheck(cudaGraphLaunch(elimExec_, s), "launch elimination graph");
+    launches_ += elimLaunches_;
+}
+
+void Engine::dropGraphs() {
+    if (elimExec_) cudaGraphExecDestroy(elimExec_);
+    elimExec_ = nullptr;
+    elimLaunches_ = 0;
+}
+
+void Engine::eliminateLaunches(cudaStream_t s) {
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
         runCholPlan(sblob_, L.chol, s);

@@ -93,6 +93,8 @@ private:
 
     void buildStatic();
     void eliminate(cudaStream_t s);
+    void eliminateLaunches(cudaStream_t s);
+    void dropGraphs();
     void tridiagonalizeAll(cudaStream_t s);
     void tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, DevBuf& blob, cudaStream_t s);
     void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
@@ -209,6 +211,8 @@ private:
 
     // kernel profiling
     bool profiling_ = false;
+    cudaGraphExec_t elimExec_ = nullptr;            // captured elimination schedule
+    int64_t elimLaunches_ = 0;                      // kernels in it
     std::vector<cudaEvent_t> evPool_;
     size_t evUsed_ = 0;
     std::vector<int> evCat_;

@@ -269,3 +269,24 @@ def test_invalid_precision(solver):
     p = cases.hex_pencil(3, 3, 3, 1, seed=1)
     with pytest.raises(ValueError):
         solver.solve(p.K, p.M, AmlsOptions(nev=5, nLevels=2, precision="fp16"))
+
+
+def test_elimination_graph_replay_matches_eager(solver):
+    """The numeric solve replays the elimination as a captured CUDA graph
+    (with per-launch instrumentation off); it gives the eager launches'
+    eigenvalues (up to the order of the extend-add atomics), also on repeat."""
+    p = cases.hex_pencil(8, 8, 8, 1, seed=5)
+    o = AmlsOptions(nev=40, nLevels=4, leafSize=200, refine=3)
+    solver.analyze(p.K, p.M, o)
+    kv = np.ascontiguousarray(p.K.data)
+    mv = np.ascontiguousarray(p.M.data)
+    th = [np.zeros(40) for _ in range(3)]
+    solver.set_profiling(True)           # eager launches, an event pair around each
+    solver.solve_values(kv.ctypes.data, mv.ctypes.data, False, th[0].ctypes.data, None, False)
+    solver.set_profiling(False)          # captured on first use, then replayed
+    for t in th[1:]:
+        solver.solve_values(kv.ctypes.data, mv.ctypes.data, False, t.ctypes.data, None, False)
+    assert rel_err(th[1], th[0]) < 1e-12
+    assert rel_err(th[2], th[0]) < 1e-12
+    wr, _ = R.LapackDense.solve_all(p.K.toarray(), p.M.toarray())
+    assert rel_err(th[2], wr[:40]) < 1e-8
