@@ -361,18 +361,24 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         cudaCheck(cudaMemcpyAsync(b.dev<GemmDesc>(oSweep), act.data(), sizeof(GemmDesc) * act.size(),
                                   cudaMemcpyHostToDevice, s), "lock");
     };
-    auto spmm = [&](const double* Y, double* out) {
+    auto spmm = [&](const double* Y, double* out, double* out2) {
         const int m = nq - lock;
         LAUNCH(launchSpmmSuperT(supDesc_.as<SpmmSuper>(), nSup_, supCols_.as<int32_t>(), supVal_.as<double>(),
-                                invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s));
+                                invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s,
+                                out2 ? out2 + lock : nullptr));
         catF_[8] += 2.0 * nnzM_ * m;
         catB_[8] += 12.0 * nnzM_ + 16.0 * dn * m;
     };
-    // the K^-1 M application on Y (nq x n): R = M Y (or the given M Y), X = K^-1 R
-    auto applyT = [&](const double* Y, const double* MY) {
-        if (MY) cudaCheck(cudaMemcpyAsync(R, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
-        else spmm(Y, R);
-        cudaCheck(cudaMemcpyAsync(X, R, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+    // the K^-1 M application on Y (nq x n): X = K^-1 (M Y), with M Y given or
+    // formed; keepR keeps R = M Y (= K X, for the Rayleigh-Ritz step), the
+    // filter's inner applications form M Y in X directly
+    auto applyT = [&](const double* Y, const double* MY, bool keepR) {
+        if (MY) {
+            cudaCheck(cudaMemcpyAsync(X, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+            if (keepR) cudaCheck(cudaMemcpyAsync(R, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
+        } else {
+            spmm(Y, X, keepR ? R : nullptr);
+        }
         const GemmDesc* sw = b.dev<GemmDesc>(oSweep);
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
@@ -404,11 +410,11 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         if (cheb >= 1) {
             double* Ym1 = Q;
             double* Yk = Y1;
-            applyT(Q, MYc);
+            applyT(Q, MYc, false);
             LAUNCH(launchAxpby3(sz, sc, X, -1.0, Q, 0.0, nullptr, Y1, s));     // Y1 = s T Q - Q
             for (int k = 1; k < cheb; ++k) {
                 double* Yn = (k == 1) ? Y2 : (Ym1 == Q ? Y2 : Ym1);
-                applyT(Yk, nullptr);
+                applyT(Yk, nullptr, false);
                 // Y_{k+1} = 2 (s T Y_k - Y_k) - Y_{k-1}
                 LAUNCH(launchAxpby3(sz, 2.0 * sc, X, -2.0, Yk, -1.0, Ym1, Yn, s));
                 Ym1 = Yk;
@@ -417,8 +423,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             Yc = Yk;
             MYc = nullptr;
         }
-        applyT(Yc, MYc);                                 // X = T Y_c, R = M Y_c = K X
-        spmm(X, MX);
+        applyT(Yc, MYc, true);                           // X = T Y_c, R = M Y_c = K X
+        spmm(X, MX, nullptr);
         if (lock > 0) {
             const size_t pitch = sizeof(double) * static_cast<size_t>(nq), w = sizeof(double) * lock;
             cudaCheck(cudaMemcpy2DAsync(X, pitch, Q, pitch, w, n, cudaMemcpyDeviceToDevice, s), "lock");

@@ -233,10 +233,11 @@ struct SpmmSuper {
     int64_t row0, colOff, valOff;
     int32_t rows, len;
 };
-// Rt[j + inv[o]*ld] = sum_c M[o, c] Qt[j + inv[c]*ld] for j < m <= ld.
+// Rt[j + inv[o]*ld] = sum_c M[o, c] Qt[j + inv[c]*ld] for j < m <= ld (also
+// into Rt2 when given).
 cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
                              const int64_t* inv, const double* Qt, int m, int64_t ld, double* Rt,
-                             cudaStream_t s);
+                             cudaStream_t s, double* Rt2 = nullptr);
 // M-norms of the columns of X held transposed in permuted order:
 // norms[j] = x_j^T M x_j with x[o, j] = zt[j + inv[o]*ld], j < m <= ld.
 cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,

@@ -209,7 +209,8 @@ template <int U, bool DOT>
 __device__ __forceinline__ void superRow(const SpmmSuper& S, const int32_t* __restrict__ ucols,
                                          const double* __restrict__ vals, const int64_t* __restrict__ inv,
                                          const double* __restrict__ Qt, int m, int64_t ld, int j0,
-                                         double* __restrict__ Rt, double (&dot)[U], double* sv, int64_t* sc) {
+                                         double* __restrict__ Rt, double* __restrict__ Rt2, double (&dot)[U],
+                                         double* sv, int64_t* sc) {
     constexpr int R = kSpmmSuperRows;
     double acc[R][U];
 #pragma unroll
@@ -254,7 +255,10 @@ __device__ __forceinline__ void superRow(const SpmmSuper& S, const int32_t* __re
                 const int j = j0 + threadIdx.x + kSpmmThreads * u;
                 if (j < m) {
                     if (DOT) dot[u] = fma(Qt[o + j], acc[r][u], dot[u]);
-                    else Rt[o + j] = acc[r][u];
+                    else {
+                        Rt[o + j] = acc[r][u];
+                        if (Rt2) Rt2[o + j] = acc[r][u];
+                    }
                 }
             }
         }
@@ -267,14 +271,14 @@ __global__ void __launch_bounds__(kSpmmThreads) spmmSuperKernel(const SpmmSuper*
                                                                 const double* __restrict__ vals,
                                                                 const int64_t* __restrict__ inv,
                                                                 const double* __restrict__ Qt, int m, int64_t ld,
-                                                                double* __restrict__ Rt) {
+                                                                double* __restrict__ Rt, double* __restrict__ Rt2) {
     __shared__ __align__(16) double sv[kSpmmStage * kSpmmSuperRows];
     __shared__ int64_t sc[kSpmmStage];
     double dot[U];
     for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x) {
         const SpmmSuper S = sup[g];
         for (int j0 = 0; j0 < m; j0 += kSpmmThreads * U)
-            superRow<U, false>(S, ucols, vals, inv, Qt, m, ld, j0, Rt, dot, sv, sc);
+            superRow<U, false>(S, ucols, vals, inv, Qt, m, ld, j0, Rt, Rt2, dot, sv, sc);
     }
 }
 
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(kSpmmThreads) mnormSuperKernel(const SpmmSuper
 #pragma unroll
     for (int u = 0; u < U; ++u) dot[u] = 0.0;
     for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x)
-        superRow<U, true>(sup[g], ucols, vals, inv, zt, m, ld, j0, nullptr, dot, sv, sc);
+        superRow<U, true>(sup[g], ucols, vals, inv, zt, m, ld, j0, nullptr, nullptr, dot, sv, sc);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int j = j0 + threadIdx.x + kSpmmThreads * u;
@@ -312,14 +316,14 @@ int spmmU(int m) {
 
 cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
                              const int64_t* inv, const double* Qt, int m, int64_t ld, double* Rt,
-                             cudaStream_t s) {
+                             cudaStream_t s, double* Rt2) {
     if (nsup <= 0 || m <= 0) return cudaSuccess;
     const int grid = gridFor(nsup * kSpmmThreads, kSpmmThreads);
     switch (spmmU(m)) {
-        case 2: spmmSuperKernel<2><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
-        case 4: spmmSuperKernel<4><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
-        case 6: spmmSuperKernel<6><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
-        default: spmmSuperKernel<8><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt); break;
+        case 2: spmmSuperKernel<2><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt, Rt2); break;
+        case 4: spmmSuperKernel<4><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt, Rt2); break;
+        case 6: spmmSuperKernel<6><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt, Rt2); break;
+        default: spmmSuperKernel<8><<<grid, kSpmmThreads, 0, s>>>(sup, nsup, ucols, vals, inv, Qt, m, ld, Rt, Rt2); break;
     }
     return cudaGetLastError();
 }
