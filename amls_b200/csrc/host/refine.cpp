@@ -86,6 +86,9 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     tiles(t3, n, want);
     const GemmBatch b1 = addBatch(b, g1, t1), b2 = addBatch(b, g2, t2), b3 = addBatch(b, g3, t3);
     FrontDesc fe{E, nn, n, n, -2, 0};
+    std::vector<TileRef> feT;                           // 32 x 32 tile pairs (tile units)
+    for (int bj = 0; bj < cdiv2(n, 32); ++bj)
+        for (int bi = bj; bi < cdiv2(n, 32); ++bi) feT.push_back({0, bi, bj, 0});
     EigDesc ed{};
     ed.A = E;
     ed.lda = nn;
@@ -100,7 +103,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     ed.kcap = want;
     ed.kOut = kOut;
     ed.work = work;
-    const size_t oFe = b.add(&fe, 1), oE = b.add(&ed, 1);
+    const size_t oFe = b.add(&fe, 1), oE = b.add(&ed, 1), oFeT = b.add(feT);
     std::vector<int> gOf, gFirst{0}, gSize;
     std::vector<int64_t> pOff{0};
     int nCta = 0;
@@ -122,7 +125,7 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     }
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b1.desc), b.dev<TileRef>(b1.tiles), b1.nTiles, s));
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b2.desc), b.dev<TileRef>(b2.tiles), b2.nTiles, s));
-    LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oFe), 1, s));
+    LAUNCH(launchSymmetrizeTiles(b.dev<FrontDesc>(oFe), b.dev<TileRef>(oFeT), static_cast<int>(feT.size()), s));
     const EigDesc* dE = b.dev<EigDesc>(oE);
     if (n <= kTridiagSmallMax) LAUNCH(launchTridiagSmall(dE, 1, s));
     else {
@@ -308,9 +311,11 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         g.ldc = nq;
         g.alpha = 1.0;
         g.kChunk = chunk;
+        // Kc and Mc are symmetric: the tiles on and below the diagonal, the
+        // upper triangle mirrored afterwards
         for (int kc = 0; kc < cdiv2(n, chunk); ++kc)
             for (int jt = 0; jt < cdiv2(nq, kTB); ++jt)
-                for (int it = 0; it < cdiv2(nq, kTB); ++it) rrT.push_back({q, it * kTB, jt * kTB, kc});
+                for (int it = jt; it < cdiv2(nq, kTB); ++it) rrT.push_back({q, it * kTB, jt * kTB, kc});
     }
     // subspace update Q = Vc^T X and, for the next iteration, M Q = Vc^T (M X)
     // (the first K^-1 M application's right-hand side, a GEMM instead of a
@@ -340,8 +345,12 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                 upT.push_back({q, it * kTB, jt * kTB, 0});
     const int nUp1 = cdiv2(n, kTB) * cdiv2(nq, kTB);     // the Q = Vc^T X tiles come first
     FrontDesc sym[2] = {{Kc, nq, nq, nq, -3, 0}, {Mc, nq, nq, nq, -3, 0}};
+    std::vector<TileRef> symT;                          // 32 x 32 tile pairs (tile units)
+    for (int q = 0; q < 2; ++q)
+        for (int bj = 0; bj < cdiv2(nq, 32); ++bj)
+            for (int bi = bj; bi < cdiv2(nq, 32); ++bi) symT.push_back({q, bi, bj, 0});
     const size_t oRR = b.add(rr), oRRT = b.add(rrT), oUP = b.add(up), oUPT = b.add(upT),
-                 oSym = b.add(sym, 2);
+                 oSym = b.add(sym, 2), oSymT = b.add(symT);
     b.upload(refBlob_, s);
 
     const double dn = static_cast<double>(n), dq = nq;
@@ -434,7 +443,8 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
         cudaCheck(cudaMemsetAsync(Kc, 0, sizeof(double) * nq * nq, s), "zero");
         cudaCheck(cudaMemsetAsync(Mc, 0, sizeof(double) * nq * nq, s), "zero");
         LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oRR), b.dev<TileRef>(oRRT), static_cast<int>(rrT.size()), s));
-        LAUNCH(launchSymmetrize(b.dev<FrontDesc>(oSym), 2, s));
+        LAUNCH(launchSymmetrizeTiles(b.dev<FrontDesc>(oSym), b.dev<TileRef>(oSymT), static_cast<int>(symT.size()),
+                                     s, true));
         denseGenEigDev(Kc, Mc, nq, nq, wd, Vc, nq, s);
         std::vector<double> th(static_cast<size_t>(nq));
         int st[2] = {0, 0};
@@ -454,7 +464,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
             --it;
             continue;
         }
-        catF_[2] += 2.0 * 2.0 * dn * dq * dq;
+        catF_[2] += 2.0 * dn * dq * dq;                 // lower triangles of Kc and Mc
         catB_[2] += 8.0 * (3.0 * dn * dq);
         // error estimate per wanted value: change * r / (1 - r), r the observed
         // contraction of the change (geometric convergence)

@@ -204,9 +204,10 @@ cudaError_t launchScatterAdd(const double* vals, const int64_t* dst, int64_t nnz
 cudaError_t launchSetDiagonal(double* C, const double* w, int64_t p, cudaStream_t s);
 // Symmetrise a batch of square blocks: A = (A + A^T)/2.
 cudaError_t launchSymmetrize(const FrontDesc* d, int nDesc, cudaStream_t s);
-// Symmetrise 32x32 tile pairs listed in tiles (desc, bi, bj with bi >= bj).
+// Symmetrise 32x32 tile pairs listed in tiles (desc, bi, bj with bi >= bj):
+// A = (A + A^T)/2, or with mirror the upper triangle from the lower.
 cudaError_t launchSymmetrizeTiles(const FrontDesc* d, const TileRef* tiles, int nTiles,
-                                  cudaStream_t s);
+                                  cudaStream_t s, bool mirror = false);
 // Transpose-copy: out(c x r) = in(r x c)^T  for a batch.
 struct CopyDesc {
     const double* in;

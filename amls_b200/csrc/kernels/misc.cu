@@ -363,8 +363,11 @@ cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const d
     return cudaGetLastError();
 }
 
-// A = (A + A^T) / 2 on the leading n x n block of each descriptor, one CTA
-// per 32x32 tile pair (TileRef: desc, m0 = bi, n0 = bj, bi >= bj).
+// A = (A + A^T) / 2 on the leading n x n block of each descriptor, or with
+// MIRROR the strict upper triangle copied from the lower one (A[i,j] =
+// A[j,i], i < j); one CTA per 32x32 tile pair (TileRef: desc, m0 = bi,
+// n0 = bj, bi >= bj, in tile units).
+template <bool MIRROR>
 __global__ void symmetrizeTilesKernel(const FrontDesc* __restrict__ descs,
                                       const TileRef* __restrict__ tiles) {
     __shared__ double t1[32][33], t2[32][33];
@@ -375,22 +378,29 @@ __global__ void symmetrizeTilesKernel(const FrontDesc* __restrict__ descs,
     for (int r = ty; r < 32; r += 8) {
         const int gi = bi * 32 + tx, gj = bj * 32 + r;
         t1[r][tx] = (gi < n && gj < n) ? F.F[gi + (int64_t)gj * F.ld] : 0.0;
-        const int hi = bj * 32 + tx, hj = bi * 32 + r;
-        t2[r][tx] = (hi < n && hj < n) ? F.F[hi + (int64_t)hj * F.ld] : 0.0;
+        if (!MIRROR) {
+            const int hi = bj * 32 + tx, hj = bi * 32 + r;
+            t2[r][tx] = (hi < n && hj < n) ? F.F[hi + (int64_t)hj * F.ld] : 0.0;
+        }
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
-        const int gi = bi * 32 + tx, gj = bj * 32 + r;
-        if (gi < n && gj < n) F.F[gi + (int64_t)gj * F.ld] = 0.5 * (t1[r][tx] + t2[tx][r]);
         const int hi = bj * 32 + tx, hj = bi * 32 + r;
-        if (hi < n && hj < n) F.F[hi + (int64_t)hj * F.ld] = 0.5 * (t2[r][tx] + t1[tx][r]);
+        if (MIRROR) {
+            if (hi < hj && hj < n) F.F[hi + (int64_t)hj * F.ld] = t1[tx][r];
+        } else {
+            const int gi = bi * 32 + tx, gj = bj * 32 + r;
+            if (gi < n && gj < n) F.F[gi + (int64_t)gj * F.ld] = 0.5 * (t1[r][tx] + t2[tx][r]);
+            if (hi < n && hj < n) F.F[hi + (int64_t)hj * F.ld] = 0.5 * (t2[r][tx] + t1[tx][r]);
+        }
     }
 }
 
 cudaError_t launchSymmetrizeTiles(const FrontDesc* d, const TileRef* tiles, int nTiles,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, bool mirror) {
     if (nTiles <= 0) return cudaSuccess;
-    symmetrizeTilesKernel<<<nTiles, 256, 0, s>>>(d, tiles);
+    if (mirror) symmetrizeTilesKernel<true><<<nTiles, 256, 0, s>>>(d, tiles);
+    else symmetrizeTilesKernel<false><<<nTiles, 256, 0, s>>>(d, tiles);
     return cudaGetLastError();
 }
 
