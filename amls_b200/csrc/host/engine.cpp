@@ -1290,7 +1290,7 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     if (opt_.refine) {
         backtransform(P, got, s);
         refineNq_ = got;
-        refineIters_ = refine(ztPool_.as<double>(), got, want, P.theta, s);
+        refineIters_ = refine(ztPool_.as<double>(), got, want, P.theta, recover, s);
         P.theta.resize(static_cast<size_t>(want));
         if (recover) finalizeVectors(ztPool_.as<double>(), got, want, s);
     } else if (recover) {

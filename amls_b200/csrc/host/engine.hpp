@@ -108,7 +108,7 @@ private:
     // Y <- Q Y for the matrices of `descs` with n > kTridiagSmallMax (k[i]
     // vectors each) by compact-WY blocks (eig_wy.cpp)
     void backTransformBig(const std::vector<EigDesc>& descs, const std::vector<int>& k, cudaStream_t s);
-    int refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s);
+    int refine(double* Q, int nq, int nev, std::vector<double>& theta, bool vectors, cudaStream_t s);
     void checkStatus(const char* phase);
     bool mixed() const { return opt_.precision == AMLS_PRECISION_MIXED; }
     int mTile() const { return mixed() ? kGemmTileMixed : kGemmTile; }

@@ -81,7 +81,8 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     set(g1[0], n, n, n, kTransB | kTriKUpTo, K, nn, Linv, nn, T, nn);              // T = K L^-T
     tiles(t1, n, n);
     set(g2[0], n, n, n, kTransA | kTransB | kTriKUpTo, T, nn, Linv, nn, E, nn);    // C = T^T L^-T
-    tiles(t2, n, n);
+    for (int j = 0; j < cdiv2(n, kT); ++j)              // C is symmetric: tiles on and below
+        for (int i = j; i < cdiv2(n, kT); ++i) t2.push_back({0, i * kT, j * kT, 0});   // the diagonal
     set(g3[0], n, want, n, kTransA, Linv, nn, Y, nn, V, ldv);                       // V = L^-T Y
     tiles(t3, n, want);
     const GemmBatch b1 = addBatch(b, g1, t1), b2 = addBatch(b, g2, t2), b3 = addBatch(b, g3, t3);
@@ -125,7 +126,8 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
     }
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b1.desc), b.dev<TileRef>(b1.tiles), b1.nTiles, s));
     LAUNCH(launchGemmBatched(b.dev<GemmDesc>(b2.desc), b.dev<TileRef>(b2.tiles), b2.nTiles, s));
-    LAUNCH(launchSymmetrizeTiles(b.dev<FrontDesc>(oFe), b.dev<TileRef>(oFeT), static_cast<int>(feT.size()), s));
+    LAUNCH(launchSymmetrizeTiles(b.dev<FrontDesc>(oFe), b.dev<TileRef>(oFeT), static_cast<int>(feT.size()), s,
+                                 true));
     const EigDesc* dE = b.dev<EigDesc>(oE);
     if (n <= kTridiagSmallMax) LAUNCH(launchTridiagSmall(dE, 1, s));
     else {
@@ -148,9 +150,9 @@ void Engine::denseGenEigDev(double* K, double* M, int n, int want, double* w, do
 }
 
 // Q (nq x n, transposed, permuted order) holds the AMLS Ritz vectors on entry
-// and the refined ones on exit; theta (host, nq) likewise.  Returns the
-// number of iterations.
-int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaStream_t s) {
+// and the refined ones on exit (its first nev rows, when `vectors`); theta
+// (host, nq) likewise.  Returns the number of iterations.
+int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool vectors, cudaStream_t s) {
     const int64_t n = n_;
     const int64_t sz = n * nq;
     double* R = static_cast<double*>(refR_.ensure(sizeof(double) * sz));
@@ -500,11 +502,20 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, cudaS
                       "lock");
         }
         // Q = Vc^T X, and M Q (and K Q on the rows to lock) for the next
-        // iteration unless this is the last
-        LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
-                                    last ? nUp1 : static_cast<int>(upT.size()), s));
-        catF_[2] += (last ? 1.0 : 2.0 + static_cast<double>(nextLock) / dq) * 2.0 * dn * dq * dq;
-        catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;
+        // iteration unless this is the last; the last needs only the nev
+        // wanted rows of Q, and none when no vectors are recovered
+        if (last) {
+            GemmDesc q0 = up[0];
+            q0.M = nev;
+            cudaCheck(cudaMemcpyAsync(b.dev<GemmDesc>(oUP), &q0, sizeof(q0), cudaMemcpyHostToDevice, s), "update");
+        }
+        if (!last || vectors) {
+            LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
+                                     last ? nUp1 : static_cast<int>(upT.size()), s));
+            catF_[2] += (last ? static_cast<double>(nev) / dq : 2.0 + static_cast<double>(nextLock) / dq) *
+                        2.0 * dn * dq * dq;
+            catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;
+        }
         haveMQ = !last;
         if (nextLock != lock) {
             if (opt_.verbosity > 1)
