@@ -47,9 +47,23 @@ __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_grou
 // one K slice of op(A) (kBM x kKs) and op(B) (kKs x kBN) into shared memory,
 // stored k-major: As[k][i], Bs[k][j]; global reads coalesced on the
 // contiguous side of each layout
+// Gathered A (GA): the column indices aMap[gk] of a slice, loaded one slice
+// ahead into registers so that the address of a gathered copy never waits
+// on the map.
+template <bool GA>
+__device__ __forceinline__ void loadMap(const GemmDesc& D, int k0, int kEnd, int32_t (&am)[kLA]) {
+    if constexpr (GA) {
+#pragma unroll
+        for (int u = 0; u < kLA; ++u) {
+            const int gk = k0 + (threadIdx.x + kGemmThreads * u) / kBM;
+            am[u] = gk < kEnd ? D.aMap[gk] : 0;
+        }
+    }
+}
+
 template <bool TA, bool TB, bool GA>
 __device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, int k0, int kEnd,
-                                           double* As, double* Bs) {
+                                           double* As, double* Bs, const int32_t (&am)[kLA]) {
 #pragma unroll
     for (int u = 0; u < kLA; ++u) {
         const int idx = threadIdx.x + kGemmThreads * u;
@@ -60,7 +74,7 @@ __device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, in
         const double* src = D.A;
         if (ok) {
             if (TA) src = D.A + gk + (int64_t)gi * D.lda;
-            else if (GA) src = D.A + gi + (int64_t)D.aMap[gk] * D.lda;
+            else if (GA) src = D.A + gi + (int64_t)am[u] * D.lda;
             else src = D.A + gi + (int64_t)gk * D.lda;
         }
         cpAsync8(As + k * kLdA + i, src, ok);
@@ -100,21 +114,25 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
     if (D.flags & kTriKFrom) kBeg = max(kBeg, n0);
     if (D.flags & kTriAUpTo) kEnd = min(kEnd, m0 + kBM);
     const int nSlices = kEnd > kBeg ? (kEnd - kBeg + kKs - 1) / kKs : 0;
+    int32_t am[kLA];
 #pragma unroll
     for (int st = 0; st < kStages - 1; ++st) {
         if (st < nSlices) {
             double* base = sm + st * kStage;
-            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + st * kKs, kEnd, base, base + kKs * kLdA);
+            loadMap<GA>(D, kBeg + st * kKs, kEnd, am);
+            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + st * kKs, kEnd, base, base + kKs * kLdA, am);
         }
         cpAsyncCommit();
     }
+    if (kStages - 1 < nSlices) loadMap<GA>(D, kBeg + (kStages - 1) * kKs, kEnd, am);
     for (int sl = 0; sl < nSlices; ++sl) {
         cpAsyncWait<kStages - 2>();
         __syncthreads();
         const int nx = sl + kStages - 1;
         if (nx < nSlices) {
             double* base = sm + (nx % kStages) * kStage;
-            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + nx * kKs, kEnd, base, base + kKs * kLdA);
+            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + nx * kKs, kEnd, base, base + kKs * kLdA, am);
+            if (nx + 1 < nSlices) loadMap<GA>(D, kBeg + (nx + 1) * kKs, kEnd, am);
         }
         cpAsyncCommit();
         const double* As = sm + (sl % kStages) * kStage;
