@@ -46,7 +46,7 @@ CONFIGS = {
 }
 
 
-REFINE = 4          # K^-1 M applications per Rayleigh-Ritz step (Chebyshev degree 3 + 1)
+REFINE = 3          # K^-1 M applications per Rayleigh-Ritz step (Chebyshev degree 2 + 1)
 REFINE_EXTRA = 200  # subspace vectors beyond nev
 REFINE_TOL = 1e-9   # target relative eigenvalue error
 
