@@ -23,7 +23,7 @@ namespace amls_b200 {
 namespace {
 constexpr int kT = kGemmTile;
 constexpr int kWyBlock = 64;
-constexpr int kSplitK = 512;
+constexpr int kSplitK = 128;
 int cdivW(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 GemmDesc gemmW(int64_t M, int64_t N, int64_t K, int flags, const double* A, int64_t lda,
