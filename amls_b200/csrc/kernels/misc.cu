@@ -1,7 +1,8 @@
 // Data-movement kernels of the AMLS pipeline: front assembly scatter,
-// symmetrisation, batched transposes, row-segment gathers, M-norms and the
-// final un-permutation.  All HBM-bound: grid-stride loops sized to the SM
-// count, coalesced on the contiguous side.
+// symmetrisation, batched transposes, row-segment gathers, the products
+// with M over super-rows (and the M-norms fused into them) and the final
+// un-permutation.  Memory-bound (HBM or L2): grid-stride loops sized to the
+// SM count, coalesced on the contiguous side.
 #include "common.cuh"
 #include "launch.hpp"
 

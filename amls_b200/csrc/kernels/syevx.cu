@@ -10,12 +10,15 @@
 // the reflectors (dormtr) - each written for the GPU:
 //   * tridiagSmall:  one CTA per matrix (batched), trailing matrix in L2;
 //   * tridiagLarge:  cooperative launch, the grid split into CTA groups, one
-//                    group per matrix, two grid barriers per column step;
-//   * bisect:        one thread per wanted eigenvalue;
-//   * inverseIter:   one CTA per cluster, members solved in sequence, the
-//                    tridiagonal LU/solve on one thread, the
-//                    reorthogonalisation and norms block-parallel;
-//   * backTransform: one warp per eigenvector column.
+//                    group per matrix, one grid barrier per column step;
+//   * bisect:        multisection, one warp (32 Sturm counts per round) per
+//                    wanted eigenvalue; division-free Sturm counts;
+//   * inverseIter:   one warp-sized CTA per cluster, members solved in
+//                    sequence, the tridiagonal LU/solve on one thread with
+//                    its operands staged through shared memory, the
+//                    reorthogonalisation and norms warp-parallel;
+//   * backTransform: columns and the reflector in shared memory (n <= 384),
+//                    blocked compact-WY GEMMs above (host/eig_wy.cpp).
 #include <cooperative_groups.h>
 
 #include <cfloat>
