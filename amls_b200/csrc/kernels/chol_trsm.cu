@@ -353,47 +353,6 @@ cudaError_t launchCholDiag64(const FrontDesc* fronts, const TrsmDesc* invd, int 
     return cudaGetLastError();
 }
 
-// ------------------------------------------------------------------------
-// inverses of the 64x64 diagonal blocks of a factored L (for trsmRows64)
-// ------------------------------------------------------------------------
-// inv[J] (64 x 64, column-major, lower) = L_JJ^-1 for J = 0 .. ceil(n/64)-1;
-// the last block of a partial size is padded with the identity.  One CTA per
-// (descriptor, block): 64 threads each solve L_JJ x = e_c by substitution.
-__global__ void __launch_bounds__(64) invDiagKernel(const TrsmDesc* __restrict__ descs,
-                                                    const TileRef* __restrict__ tiles) {
-    __shared__ double Ls[64][65];
-    const TileRef t = tiles[blockIdx.x];
-    const TrsmDesc D = descs[t.desc];
-    const int J = t.m0;                       // block index
-    const int j0 = J * 64, nb = min(64, D.n - j0);
-    double* out = D.inv + (int64_t)J * 4096;
-    const int c = threadIdx.x;
-    for (int r = 0; r < 64; ++r)
-        Ls[r][c] = (r < nb && c < nb) ? D.L[(j0 + r) + (int64_t)(j0 + c) * D.ldl] : (r == c ? 1.0 : 0.0);
-    __syncthreads();
-    // column c of the inverse: x_r = (delta_rc - sum_{q<r} L_rq x_q) / L_rr, x_r = 0 for r < c
-    double x[64];
-#pragma unroll
-    for (int r = 0; r < 64; ++r) x[r] = 0.0;
-#pragma unroll
-    for (int r = 0; r < 64; ++r) {
-        if (r >= c) {
-            double v = (r == c) ? 1.0 : 0.0;
-#pragma unroll
-            for (int q = 0; q < r; ++q) v -= Ls[r][q] * x[q];
-            x[r] = v / Ls[r][r];
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < 64; ++r) out[r + 64 * c] = x[r];
-}
-
-cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* tiles, int nTiles, cudaStream_t s) {
-    if (nTiles <= 0) return cudaSuccess;
-    invDiagKernel<<<nTiles, 64, 0, s>>>(d, tiles);
-    return cudaGetLastError();
-}
-
 // X[J*64 + r, J*64 + c] = inv[J][r + 64 c] for r, c < the block's size: the
 // diagonal blocks of L^-1 (X n x n, ld ldx), the start of its doubling
 // construction.  One CTA per (descriptor, block).
@@ -413,128 +372,6 @@ __global__ void __launch_bounds__(256) placeDiagInvKernel(const TrsmDesc* __rest
 cudaError_t launchPlaceDiagInv(const TrsmDesc* d, const TileRef* tiles, int nTiles, cudaStream_t s) {
     if (nTiles <= 0) return cudaSuccess;
     placeDiagInvKernel<<<nTiles, 256, 0, s>>>(d, tiles);
-    return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------------
-// row-panel TRSM with 64-row tiles and register tiling:
-//   forward:  X <- X L^-T    backward: X <- X L^-1     (X: r x n)
-// per 64-wide column block J: acc = X[R,J] - X[R,outside] * L[...] (4x4
-// accumulators per thread, K staged through shared memory 16 at a time),
-// then X[R,J] = acc * inv(L_JJ)^T (forward) or acc * inv(L_JJ) (backward).
-// ------------------------------------------------------------------------
-namespace {
-constexpr int T64 = 64, TK64 = 16;
-}
-
-__global__ void __launch_bounds__(256) trsmRows64Kernel(const TrsmDesc* __restrict__ descs,
-                                                        const TileRef* __restrict__ tiles) {
-    extern __shared__ double sm64[];
-    double (*As)[T64 + 2] = reinterpret_cast<double (*)[T64 + 2]>(sm64);                  // [TK][66]
-    double (*Bs)[T64 + 2] = reinterpret_cast<double (*)[T64 + 2]>(sm64 + TK64 * (T64 + 2)); // [TK][66]
-    double* accS = sm64 + 2 * TK64 * (T64 + 2);          // 64 x 65
-    double* invS = accS + 64 * 65;                       // 64 x 65
-    const TileRef t = tiles[blockIdx.x];
-    const TrsmDesc D = descs[t.desc];
-    const int r0 = t.m0;
-    const int nr = min(T64, D.r - r0);
-    if (nr <= 0) return;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int nblk = (D.n + T64 - 1) / T64;
-    for (int bi = 0; bi < nblk; ++bi) {
-        const int jb = D.backward ? (nblk - 1 - bi) : bi;
-        const int j0 = jb * T64, nb = min(T64, D.n - j0), j1 = j0 + nb;
-        double acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int row = tx + 16 * i, col = ty + 16 * j;
-                acc[i][j] = (row < nr && col < nb) ? D.X[(r0 + row) + (int64_t)(j0 + col) * D.ldx] : 0.0;
-            }
-        // K range of the update: forward [0, j0) with L[J, k]; backward [j1, n) with L[k, J]
-        const int kBeg = D.backward ? j1 : 0;
-        const int kEnd = D.backward ? D.n : j0;
-        for (int k0 = kBeg; k0 < kEnd; k0 += TK64) {
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int idx = threadIdx.x + 256 * u;
-                const int i = idx % T64, k = idx / T64;       // row i of the tile, k of the slice
-                const int gk = k0 + k;
-                As[k][i] = (i < nr && gk < kEnd) ? D.X[(r0 + i) + (int64_t)gk * D.ldx] : 0.0;
-                double b = 0.0;
-                if (i < nb && gk < kEnd)
-                    b = D.backward ? D.L[gk + (int64_t)(j0 + i) * D.ldl]      // L[k, J_i]
-                                   : D.L[(j0 + i) + (int64_t)gk * D.ldl];     // L[J_i, k]
-                Bs[k][i] = b;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int kk = 0; kk < TK64; ++kk) {
-                double a[4], b[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(-a[i], b[j], acc[i][j]);
-            }
-        }
-        // acc -> shared, inverse block -> shared
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) accS[(tx + 16 * i) * 65 + ty + 16 * j] = acc[i][j];
-        const double* inv = D.inv + (int64_t)jb * 4096;
-        for (int e = threadIdx.x; e < 4096; e += 256) {
-            const int r = e % 64, c = e / 64;
-            invS[r * 65 + c] = inv[e];     // invS[r][c] = inv(L_JJ)[r][c]
-        }
-        __syncthreads();
-        // X_J[row, col] = sum_k acc[row][k] * (forward: inv[col][k]; backward: inv[k][col])
-        double o[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) o[i][j] = 0.0;
-        for (int k = 0; k < 64; ++k) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = accS[(tx + 16 * i) * 65 + k];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                b[j] = D.backward ? invS[k * 65 + ty + 16 * j] : invS[(ty + 16 * j) * 65 + k];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) o[i][j] = fma(a[i], b[j], o[i][j]);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int row = tx + 16 * i, col = ty + 16 * j;
-                if (row < nr && col < nb) D.X[(r0 + row) + (int64_t)(j0 + col) * D.ldx] = o[i][j];
-            }
-        __syncthreads();
-    }
-}
-
-cudaError_t launchTrsmRows64(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s) {
-    if (nTiles <= 0) return cudaSuccess;
-    const size_t smem = sizeof(double) * (2 * TK64 * (T64 + 2) + 2 * 64 * 65);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(trsmRows64Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    trsmRows64Kernel<<<nTiles, 256, smem, s>>>(d, dTiles);
     return cudaGetLastError();
 }
 

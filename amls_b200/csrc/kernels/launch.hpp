@@ -111,19 +111,13 @@ struct TrsmDesc {
     int64_t ldx;
     int32_t n, r;
     int32_t rowTiles, backward;
-    double* inv;            // trsmRows64 / invDiag: inverses of the 64x64 diagonal blocks
+    double* inv;            // inverses of the 64x64 diagonal blocks (cholDiag64, placeDiagInv)
 };
 constexpr int kTrsmRows = 32;
 cudaError_t launchTrsmRows(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
-// Same operation with 64-row tiles (TileRef.m0 = first row), register-tiled,
-// diagonal blocks applied through inv (see launchInvDiag).
-constexpr int kTrsmRows64 = 64;
-cudaError_t launchTrsmRows64(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
-// inv + 4096*J = (L_JJ)^-1 for the 64x64 diagonal blocks J (TileRef.m0 = J).
-cudaError_t launchInvDiag(const TrsmDesc* d, const TileRef* dTiles, int nTiles, cudaStream_t s);
 // Right-looking variant, 64-wide blocks: factor the diagonal block J of each
 // front in place (fronts[i]) and write its inverse to invd[i].inv + 4096 J
-// (identity-padded, as launchInvDiag); panel and trailing update are GEMMs.
+// (identity-padded to 64 x 64); panel and trailing update are GEMMs.
 cudaError_t launchCholDiag64(const FrontDesc* fronts, const TrsmDesc* invd, int nFront, int J,
                              int* status, cudaStream_t s);
 // X (n x n, ld ldx) diagonal 64 x 64 blocks <- inv blocks (TileRef.m0 = J);
@@ -218,10 +212,6 @@ struct CopyDesc {
 };
 cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int nTiles,
                                    cudaStream_t s);
-// Segment copies: out[dstOff[g] + t] = in[srcOff[g] + t] for t < len[g].
-cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* out,
-                             const int64_t* dstOff, const int32_t* len, int nSeg,
-                             cudaStream_t s);
 // Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]), j < m.
 cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
                             const double* norms, double* Z, cudaStream_t s);
@@ -254,7 +244,5 @@ cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, cons
 // out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
 cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
                          double c, const double* z, double* out, cudaStream_t s);
-// out[i] = 1 / in[i]   (reciprocals, for eigenvalue maps)
-cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s);
 
 }  // namespace amls_b200

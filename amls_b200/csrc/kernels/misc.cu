@@ -1,5 +1,5 @@
 // Data-movement kernels of the AMLS pipeline: front assembly scatter,
-// symmetrisation, batched transposes, row-segment gathers, the products
+// symmetrisation, batched transposes, the products
 // with M over super-rows (and the M-norms fused into them) and the final
 // un-permutation.  Memory-bound (HBM or L2): grid-stride loops sized to the
 // SM count, coalesced on the contiguous side.
@@ -129,26 +129,6 @@ cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int 
     return cudaGetLastError();
 }
 
-// Contiguous segment copies: out[dstOff[g] + t] = in[srcOff[g] + t], t < len[g]
-// (one CTA per segment).
-__global__ void gatherSegKernel(const double* __restrict__ in, const int64_t* __restrict__ srcOff,
-                                double* __restrict__ out, const int64_t* __restrict__ dstOff,
-                                const int32_t* __restrict__ len) {
-    const int g = blockIdx.x;
-    const int L = len[g];
-    const double* src = in + srcOff[g];
-    double* dst = out + dstOff[g];
-    for (int t = threadIdx.x; t < L; t += blockDim.x) dst[t] = src[t];
-}
-
-cudaError_t launchGatherRows(const double* in, const int64_t* srcOff, double* out,
-                             const int64_t* dstOff, const int32_t* len, int nSeg,
-                             cudaStream_t s) {
-    if (nSeg <= 0) return cudaSuccess;
-    gatherSegKernel<<<nSeg, 128, 0, s>>>(in, srcOff, out, dstOff, len);
-    return cudaGetLastError();
-}
-
 // Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]); 32 x 32 tiles (d, j).
 __global__ void unpermuteKernel(const double* __restrict__ zt, int64_t ldz, int m, int64_t n,
                                 const int64_t* __restrict__ perm, const double* __restrict__ norms,
@@ -178,17 +158,6 @@ cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, con
     if (n <= 0 || m <= 0) return cudaSuccess;
     dim3 grid((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
     unpermuteKernel<<<grid, 256, 0, s>>>(zt, ldz, m, n, perm, norms, Z);
-    return cudaGetLastError();
-}
-
-__global__ void reciprocalKernel(const double* __restrict__ in, double* __restrict__ out, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = 1.0 / in[i];
-}
-
-cudaError_t launchReciprocal(const double* in, double* out, int n, cudaStream_t s) {
-    if (n <= 0) return cudaSuccess;
-    reciprocalKernel<<<(n + 255) / 256, 256, 0, s>>>(in, out, n);
     return cudaGetLastError();
 }
 
