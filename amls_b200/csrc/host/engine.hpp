@@ -187,7 +187,6 @@ private:
     std::vector<int64_t> hostKDst_, hostMDst_;
 
     // eigen
-    std::vector<EigDesc> eigDescs_;                // one per node (static part)
     bool tridiagDone_ = false;
 
     // per-pass device buffers
@@ -207,7 +206,7 @@ private:
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;
-    DevBuf senDof_, senEl_, senW_, senOut_;
+    DevBuf senDof_, senEl_, senOut_;
 
     // kernel profiling
     bool profiling_ = false;
