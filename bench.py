@@ -129,6 +129,19 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def max_over_ranks(x, dist):
+    """The largest x over all ranks (every multi-GPU time is the slowest
+    rank's).  Every rank must call it at the same point; the tensor lives
+    on the GPU for NCCL and on the host for gloo."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
@@ -191,11 +204,7 @@ def run_ours(args, rank, world, dist):
     s.set_profiling(False)
     info = s.info()
     work = s.work()
-    t_step = float(np.mean(dev_times))
-    if dist:
-        tt = torch.tensor([t_step], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = float(tt.item())
+    t_step = max_over_ranks(float(np.mean(dev_times)), dist)
 
     # accuracy of the timed solve's eigenvalues against the exact golden
     accuracy = {}
@@ -224,11 +233,7 @@ def run_ours(args, rank, world, dist):
             flush.zero_()
             torch.cuda.synchronize()
             t3.append(step3()["device"])
-        o_step = float(np.mean(t3))
-        if dist:
-            tt = torch.tensor([o_step], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            o_step = float(tt.item())
+        o_step = max_over_ranks(float(np.mean(t3)), dist)
         other = {"precision": oprec, "s": o_step}
         if args.config == "C5" and os.path.exists(gold):
             th3 = theta.cpu().numpy()
@@ -283,11 +288,7 @@ def run_ours(args, rank, world, dist):
     h2d = sum(a.nbytes for a in (p.K.indptr.astype(np.int64), p.K.indices, p.K.data,
                                  p.M.indptr.astype(np.int64), p.M.indices, p.M.data))
     d2h = nev * 8 + n * nev * 8
-    e2e_t = float(np.mean(e2e)) if e2e else None
-    if dist and e2e_t is not None:
-        tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t = max_over_ranks(float(np.mean(e2e)), dist) if e2e else None
 
     # roofline of the dominant kernel category
     pk, src = peaks()
