@@ -1446,6 +1446,11 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
         cp3.push_back(r);
     }
     Blob B;
+    std::vector<TileRef> symT;                          // 32 x 32 tile pairs of every C (tile units)
+    for (size_t q = 0; q < fE.size(); ++q)
+        for (int bj = 0; bj < cdiv(fE[q].n, 32); ++bj)
+            for (int bi = bj; bi < cdiv(fE[q].n, 32); ++bi) symT.push_back({static_cast<int32_t>(q), bi, bj, 0});
+    const size_t oSymT = B.add(symT);
     const size_t ofF = B.add(fF), ofE = B.add(fE), ot1 = B.add(t1), ot1T = B.add(t1T), ocp = B.add(cp),
                  ocpT = B.add(cpT), ot2 = B.add(t2), ot2T = B.add(t2T), oS = B.add(small), oL = B.add(large),
                  oA = B.add(all), ocp2 = B.add(cp2), ocp2T = B.add(cp2T), ot3 = B.add(t3), ot3T = B.add(t3T),
@@ -1460,7 +1465,7 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
     LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot1), B.dev<TileRef>(ot1T), static_cast<int>(t1T.size()), s));
     LAUNCH(launchTransposeBatched(B.dev<CopyDesc>(ocp), B.dev<TileRef>(ocpT), static_cast<int>(cpT.size()), s));
     LAUNCH(launchTrsmRows(B.dev<TrsmDesc>(ot2), B.dev<TileRef>(ot2T), static_cast<int>(t2T.size()), s));
-    LAUNCH(launchSymmetrize(B.dev<FrontDesc>(ofE), nb, s));
+    LAUNCH(launchSymmetrizeTiles(B.dev<FrontDesc>(ofE), B.dev<TileRef>(oSymT), static_cast<int>(symT.size()), s));
     if (!small.empty()) LAUNCH(launchTridiagSmall(B.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
     (void)oL;
     (void)maxLargeN;
