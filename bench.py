@@ -1,15 +1,20 @@
 """Benchmark: AMLS solve time of the 27-node hex elasticity pencil on a
 14^3 element cube (70,644 DOF, ~12.4M nnz per matrix), lowest 500
 eigenpairs, METIS nested dissection to 8 levels, eta = 2, two-pass
-truncation, FP64 - on one B200 (replicas on N GPUs).
+truncation - mixed precision (the FP64 arm timed beside it) on one B200
+(replicas on N GPUs).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Our arm: the pencil's pattern is analysed once (partition, permutation,
 symbolic fill: host work that depends only on the sparsity); each timed step
 is one numeric solve from K and M values already resident in HBM to theta and
-Z in HBM, timed with CUDA events on the solver's stream (amls_solve_values).
-The L2 is flushed (a 256 MiB write) between timed steps.  `e2e` is the
+Z in HBM, timed with CUDA events on the solver's stream (amls_solve_values),
+refined in FP64 to the metric's accuracy and checked against the exact
+golden eigenvalues.  The L2 is flushed (a 256 MiB write) between timed
+steps.  The same number of steps with a CUDA-event pair around every launch
+follows, for the per-category kernel times behind `roofline` (the events
+add about 2 % to a step, so they stay out of `value`).  `e2e` is the
 public C-ABI call amls_solve with host CSR arrays in and host theta/Z out,
 including partition, host->device and device->host copies, timed with the
 host clock around the synchronous call.
