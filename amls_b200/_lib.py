@@ -37,7 +37,7 @@ EXPORTS = [
     "amls_options_default", "amls_create", "amls_destroy", "amls_last_error", "amls_partition",
     "amls_solve", "amls_analyze", "amls_solve_values", "amls_info", "amls_work",
     "amls_sygvx_batched", "amls_set_profiling", "amls_kernel_times", "amls_category_work",
-    "amls_sygvx_lowest_noalloc", "amls_sensitivities",
+    "amls_sygvx_lowest_noalloc", "amls_sensitivities", "amls_permutation",
 ]
 NOALLOC_MAX_N = 128
 
@@ -81,11 +81,12 @@ def lib() -> C.CDLL:
         L.amls_set_profiling.argtypes = [P, C.c_int32]
         L.amls_kernel_times.argtypes = [P, P, P]
         L.amls_category_work.argtypes = [P, P, P]
-        L.amls_sensitivities.argtypes = [P, C.c_int64, C.c_int32, P, P, P, P, C.c_double, P, P,
-                                         P, P, P]
+        L.amls_sensitivities.argtypes = [P, C.c_int64, C.c_int32, P, C.c_int32, P, P, P, P,
+                                         C.c_double, P, P, P, P, P]
         L.amls_sygvx_lowest_noalloc.argtypes = [C.c_int64, P, P, C.c_int64, P, P,
                                                 C.POINTER(C.c_int64), P]
         L.amls_work.argtypes = [P, P]
+        L.amls_permutation.argtypes = [P, P]
         L.amls_sygvx_batched.argtypes = [P, C.c_int32, P, P, P, P, C.c_int32, C.c_int64,
                                          C.c_int64, C.c_double, C.c_double, P, P, P, P, P, P]
         _lib = L

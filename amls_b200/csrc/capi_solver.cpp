@@ -108,6 +108,16 @@ extern "C" int amls_info(amls_handle h, int64_t* info) {
     });
 }
 
+extern "C" int amls_permutation(amls_handle h, int64_t* perm) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!perm) return fail(AMLS_ERR_INVALID_ARGUMENT, "null perm");
+        if (!h->eng->analyzed()) return fail(AMLS_ERR_INVALID_ARGUMENT, "no analysis on the handle");
+        h->eng->permutation(perm);
+        return AMLS_OK;
+    });
+}
+
 extern "C" int amls_work(amls_handle h, double* work) {
     return guarded([&]() -> int {
         if (int e = checkHandle(h)) return e;
@@ -162,6 +172,7 @@ extern "C" int amls_category_work(amls_handle h, double* flops, double* bytes) {
 }
 
 extern "C" int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, const int64_t* dofmap,
+                                  int32_t ntypes, const int32_t* elemType,
                                   const double* Kbar, const double* Mbar, const double* weights,
                                   double gapTol, double* gE, double* gRho, double* dE, double* dRho,
                                   int32_t* simple) {
@@ -169,8 +180,8 @@ extern "C" int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, c
         if (int e = checkHandle(h)) return e;
         if (nelem <= 0 || !dofmap || !Kbar || !Mbar)
             return fail(AMLS_ERR_INVALID_ARGUMENT, "amls_sensitivities: bad element data");
-        h->eng->sensitivities(nelem, ndofe, dofmap, Kbar, Mbar, weights, gapTol, gE, gRho, dE, dRho,
-                              simple);
+        h->eng->sensitivities(nelem, ndofe, dofmap, ntypes, elemType, Kbar, Mbar, weights, gapTol, gE,
+                              gRho, dE, dRho, simple);
         return AMLS_OK;
     });
 }

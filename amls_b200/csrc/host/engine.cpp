@@ -1500,13 +1500,25 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
     (void)ko;
 }
 
-void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, int32_t ntypes,
+                           const int32_t* elemType, const double* Kbar,
                            const double* Mbar, const double* weights, double gapTol, double* gE,
                            double* gRho, double* dE, double* dRho, int32_t* simple) {
     if (!lastHasVectors_ || lastTheta_.empty())
         throw AmlsError(AMLS_ERR_INVALID_ARGUMENT,
                         "sensitivities need a preceding solve with recovered eigenvectors");
     if (nd <= 0 || nd > 96) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element DOF count must be 1..96");
+    if (ntypes < 1) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element type count must be >= 1");
+    if (elemType) {
+        for (int64_t e = 0; e < nelem; ++e)
+            if (elemType[e] < 0 || elemType[e] >= ntypes)
+                throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element type out of range");
+    } else if (ntypes != 1) {
+        throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element types needed when ntypes > 1");
+    }
+    for (int64_t q = 0; q < nelem * nd; ++q)
+        if (dofmap[q] < -1 || dofmap[q] >= n_)
+            throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "dofmap entry out of range");
     cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
     cudaStream_t s = stream_;
     const int nm = static_cast<int>(lastTheta_.size());
@@ -1522,20 +1534,26 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const d
         w[static_cast<size_t>(k)] = ok ? (weights ? weights[k] : 0.0) : std::nan("");
     }
     int64_t* dDof = static_cast<int64_t*>(senDof_.ensure(sizeof(int64_t) * nelem * nd));
-    double* dEl = static_cast<double*>(senEl_.ensure(sizeof(double) * (2 * nd * nd + 2 * nm)));
+    const int64_t nmat = static_cast<int64_t>(ntypes) * nd * nd;
+    double* dEl = static_cast<double*>(senEl_.ensure(sizeof(double) * (2 * nmat + 2 * nm)));
+    int32_t* dType = nullptr;
+    if (elemType) {
+        dType = static_cast<int32_t*>(senType_.ensure(sizeof(int32_t) * nelem));
+        cudaCheck(cudaMemcpyAsync(dType, elemType, sizeof(int32_t) * nelem, cudaMemcpyHostToDevice, s), "types");
+    }
     const size_t outN = static_cast<size_t>(nelem) * (2 + (dE ? nm : 0) + (dRho ? nm : 0));
     double* dOut = static_cast<double*>(senOut_.ensure(sizeof(double) * outN));
     cudaCheck(cudaMemcpyAsync(dDof, dofmap, sizeof(int64_t) * nelem * nd, cudaMemcpyHostToDevice, s), "dofmap");
-    cudaCheck(cudaMemcpyAsync(dEl, Kbar, sizeof(double) * nd * nd, cudaMemcpyHostToDevice, s), "Kbar");
-    cudaCheck(cudaMemcpyAsync(dEl + nd * nd, Mbar, sizeof(double) * nd * nd, cudaMemcpyHostToDevice, s), "Mbar");
-    cudaCheck(cudaMemcpyAsync(dEl + 2 * nd * nd, lastTheta_.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "theta");
-    cudaCheck(cudaMemcpyAsync(dEl + 2 * nd * nd + nm, w.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "weights");
+    cudaCheck(cudaMemcpyAsync(dEl, Kbar, sizeof(double) * nmat, cudaMemcpyHostToDevice, s), "Kbar");
+    cudaCheck(cudaMemcpyAsync(dEl + nmat, Mbar, sizeof(double) * nmat, cudaMemcpyHostToDevice, s), "Mbar");
+    cudaCheck(cudaMemcpyAsync(dEl + 2 * nmat, lastTheta_.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "theta");
+    cudaCheck(cudaMemcpyAsync(dEl + 2 * nmat + nm, w.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s), "weights");
     double* oE = dOut;
     double* oR = dOut + nelem;
     double* odE = dE ? dOut + 2 * nelem : nullptr;
     double* odR = dRho ? dOut + 2 * nelem + (dE ? nelem * nm : 0) : nullptr;
-    LAUNCH(launchSensitivity(nelem, nd, dDof, dEl, dEl + nd * nd, zOut_.as<double>(), n_, nm,
-                             dEl + 2 * nd * nd, dEl + 2 * nd * nd + nm, oE, oR, odE, odR, s));
+    LAUNCH(launchSensitivity(nelem, nd, dDof, dType, dEl, dEl + nmat, zOut_.as<double>(), n_, nm,
+                             dEl + 2 * nmat, dEl + 2 * nmat + nm, oE, oR, odE, odR, s));
     if (gE) cudaCheck(cudaMemcpyAsync(gE, oE, sizeof(double) * nelem, cudaMemcpyDeviceToHost, s), "gE");
     if (gRho) cudaCheck(cudaMemcpyAsync(gRho, oR, sizeof(double) * nelem, cudaMemcpyDeviceToHost, s), "gRho");
     if (dE) cudaCheck(cudaMemcpyAsync(dE, odE, sizeof(double) * nelem * nm, cudaMemcpyDeviceToHost, s), "dE");
@@ -1566,6 +1584,11 @@ void Engine::info(int64_t* out) const {
     out[6] = launches_;
     out[7] = refineIters_;
     out[8] = refineNq_;
+    out[9] = n_;
+}
+
+void Engine::permutation(int64_t* out) const {
+    std::copy(perm_.begin(), perm_.end(), out);
 }
 
 void Engine::categoryWork(double* flops, double* bytes) const {

@@ -1,6 +1,6 @@
 // AMLS engine: host analysis + device numeric pipeline for one handle.
 //
-// Algorithm (the reference's AmlsSolver::solve, src/amls/solver.cpp:154-373,
+// Algorithm (the reference's AmlsSolver::solve, src/amls/solver.cpp:100-319,
 // re-designed for one B200):
 //   analysis (host):  shift pattern, METIS nested dissection, post-order
 //     offsets, symbolic fill of every node's coupling set S_i (the rows of
@@ -20,7 +20,7 @@
 //     subspace_condensation.cpp:129-261 on per-node panels.
 //   reduced eigensolve: the largest eigenvalues of Kp^-1/2 Mp Kp^-1/2.
 //   back-transform z = L^-T S q (subspace_condensation.cpp:263-319),
-//     un-permutation and M-normalisation (solver.cpp:350-365).
+//     un-permutation and M-normalisation (solver.cpp:302-311).
 #pragma once
 #include <cstdint>
 #include <map>
@@ -52,10 +52,14 @@ public:
                       double* V, int64_t* m);
 
     // per-element sensitivities of the last solve's eigenpairs
-    void sensitivities(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+    void sensitivities(int64_t nelem, int nd, const int64_t* dofmap, int32_t ntypes,
+                       const int32_t* elemType, const double* Kbar,
                        const double* Mbar, const double* weights, double gapTol, double* gE,
                        double* gRho, double* dE, double* dRho, int32_t* simple);
     void info(int64_t* out) const;
+    // permutation of the last analysis (perm[new] = old, n entries)
+    void permutation(int64_t* out) const;
+    int64_t size() const { return n_; }
     // per-category kernel timing with CUDA events on the engine stream
     static constexpr int kProfCats = 9;
     void setProfiling(bool on);
@@ -206,7 +210,7 @@ private:
     int refineIters_ = 0, refineNq_ = 0;
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;
-    DevBuf senDof_, senEl_, senOut_;
+    DevBuf senDof_, senEl_, senOut_, senType_;
 
     // kernel profiling
     bool profiling_ = false;

@@ -3,7 +3,7 @@
 // Semantics follow the reference's SeparatorTree (src/amls/separator_tree.cpp:
 // node ids in creation order, children {left, right}, post-order = children
 // then self, ancestors = parent .. root) and MetisPartitioner
-// (src/partition/metis_partitioner.cpp:143-212: perm[new] = old, the
+// (src/partition/metis_partitioner.cpp:110-179: perm[new] = old, the
 // concatenation of node index lists in post-order).
 #pragma once
 #include <cstdint>

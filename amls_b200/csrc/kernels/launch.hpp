@@ -235,9 +235,11 @@ cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* 
                              const int64_t* inv, const double* zt, int m, int64_t ld, double* norms,
                              cudaStream_t s);
 // Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
-// (n x nmodes, original order): see sensitivity.cu.  weight[k] NaN marks a
-// non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.
-cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+// (n x nmodes, original order): see sensitivity.cu.  elemType[e] (null: all
+// 0) selects element e's matrices Kbar/Mbar + type * nd * nd.  weight[k] NaN
+// marks a non-simple eigenvalue.  Any of gE/gRho/dE/dRho may be null.
+cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, const int32_t* elemType,
+                              const double* Kbar,
                               const double* Mbar, const double* X, int64_t n, int nmodes,
                               const double* lambda, const double* weight, double* gE,
                               double* gRho, double* dE, double* dRho, cudaStream_t s);

@@ -1,25 +1,31 @@
 // Allocation-free variant of the dense generalized eigensolver.
 //
-// Some callers cannot call cudaMalloc at all: code running inside a CUDA
-// graph that is being captured, a host that owns every allocation through
-// its own memory pool and forbids outside allocations, or a real-time loop
-// that must not enter the driver's allocator.  amls_sygvx_lowest_noalloc
-// serves them: the caller passes device pointers for the inputs and outputs,
-// and every intermediate (factor, reduced matrix, tridiagonal form,
-// eigenvector workspace, launch tables, status word) lives in the
-// file-scope device array below, of fixed size.  The array exists on every
-// GPU that loads this library and stays allocated until the process exits.
+// Some callers cannot call cudaMalloc at all: a host application whose own
+// memory pool owns every device allocation and forbids allocations from
+// outside it, or a real-time loop that must never enter the driver's
+// allocator (an allocation can block on the device and take milliseconds).
+// amls_sygvx_lowest_noalloc serves them: the caller passes device pointers
+// for the inputs and outputs, and every intermediate (factor, reduced
+// matrix, tridiagonal form, eigenvector workspace, launch tables, status
+// word) lives in the file-scope device array below, of fixed size.  The
+// array exists on every GPU that loads this library and stays allocated
+// until the process exits.
 //
 // Host code may not use `g_noallocScratch` as a device address (in host code
 // the name is a host-side stand-in); its device address is obtained once per
-// device with cudaGetSymbolAddress, with that device current, the first time
-// the entry point runs on the device.  That first call therefore does a
-// CUDA runtime query and should come before any stream capture.
+// device (per CUDA context on it) with cudaGetSymbolAddress, with that device
+// current, the first time the entry point runs there.  If the context is torn
+// down and created again (cudaDeviceReset), the module is loaded again and the
+// array may move: the address is looked up again when the context changes.
+//
+// The call is synchronous: it ends by reading the status word back and
+// synchronising the caller's stream.
 //
 // All calls share the one array and it keeps the last call's contents:
 // everything that must start at zero is cleared by each call, and calls that
 // overlap on the GPU (different streams, or different host threads) race on
 // the array - serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -49,20 +55,57 @@ static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 namespace {
 
 std::mutex g_setupMutex;
-void* g_scratchAddr[64] = {nullptr};   // per device ordinal
+struct ScratchSlot {
+    void* addr = nullptr;
+    unsigned long long ctxId = 0;   // context the address belongs to
+};
+ScratchSlot g_scratch[64];          // per device ordinal
 
-// Device address of the scratch array on the current device (set-up once per
-// device).
+// Unique id of the current CUDA context (cuCtxGetId through the runtime's
+// driver entry points, so the library needs no link against libcuda).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+bool currentContextId(unsigned long long* id) {
+    static CtxGetCurrentFn getCurrent = nullptr;
+    static CtxGetIdFn getId = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getCurrent = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getId = reinterpret_cast<CtxGetIdFn>(f);
+    }
+    if (!getCurrent || !getId) return false;
+    CUcontext c = nullptr;
+    if (getCurrent(&c) != CUDA_SUCCESS || !c) return false;
+    return getId(c, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch array on the current device: looked up once
+// per device and context, with that device current.
 cudaError_t scratchAddress(int dev, unsigned char** out) {
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_setupMutex);
-    if (!g_scratchAddr[dev]) {
+    // make the device's primary context current (and initialised)
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    unsigned long long id = 0;
+    const bool haveId = currentContextId(&id);
+    ScratchSlot& slot = g_scratch[dev];
+    if (!slot.addr || !haveId || slot.ctxId != id) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+        e = cudaGetSymbolAddress(&p, g_noallocScratch);
         if (e != cudaSuccess) return e;
-        g_scratchAddr[dev] = p;
+        slot.addr = p;
+        slot.ctxId = haveId ? id : 0;
     }
-    *out = static_cast<unsigned char*>(g_scratchAddr[dev]);
+    *out = static_cast<unsigned char*>(slot.addr);
     return cudaSuccess;
 }
 
@@ -179,8 +222,8 @@ extern "C" int amls_sygvx_lowest_noalloc(int64_t n, const double* K, const doubl
     run(launchSymmetrize(reinterpret_cast<const FrontDesc*>(T(oFe)), 1, s));
     const EigDesc* dE = reinterpret_cast<const EigDesc*>(T(oE));
     run(launchTridiagSmall(dE, 1, s));
-    run(launchBisect(dE, 1, 2, ki, 0.0, ki, nullptr, s));
-    run(launchInverseIter(dE, 1, ki, nullptr, s));
+    run(launchBisect(dE, 1, 2, ki, 0.0, ki, status, s));
+    run(launchInverseIter(dE, 1, ki, status, s));
     run(launchBackTransform(dE, 1, ki, s));
     run(launchTransposeBatched(reinterpret_cast<const CopyDesc*>(T(oC2)),
                                reinterpret_cast<const TileRef*>(T(oYk)), nYk, s));
@@ -196,7 +239,13 @@ extern "C" int amls_sygvx_lowest_noalloc(int64_t n, const double* K, const doubl
         cudaGetLastError();
         return err == cudaErrorMemoryAllocation ? AMLS_ERR_OOM : AMLS_ERR_CUDA;
     }
-    if (hs[0] == kDevNotSpd) return AMLS_ERR_NOT_SPD;
+    switch (hs[0]) {
+        case kDevOk: break;
+        case kDevNotSpd: return AMLS_ERR_NOT_SPD;
+        case kDevIterCap: return AMLS_ERR_ITERATION;
+        case kDevTimeout: return AMLS_ERR_TIMEOUT;
+        default: return AMLS_ERR_NUMERIC;
+    }
     *m = hs[2];
     return AMLS_OK;
 }

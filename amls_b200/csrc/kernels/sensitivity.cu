@@ -1,16 +1,17 @@
 // Per-element eigenvalue sensitivities (adjoint form).
 //
-// For a pencil assembled as K = sum_e E_e Kbar, M = sum_e rho_e Mbar (one
-// reference element pair, per-element modulus and density scale) and
-// M-normalised eigenvectors x_k:
-//   d lambda_k / d E_e   =  x_{k,e}^T Kbar x_{k,e}
-//   d lambda_k / d rho_e = -lambda_k x_{k,e}^T Mbar x_{k,e}
+// For a pencil assembled as K = sum_e E_e Kbar_t(e), M = sum_e rho_e
+// Mbar_t(e) (reference element pairs indexed by an element type t(e), with a
+// per-element modulus and density scale) and M-normalised eigenvectors x_k:
+//   d lambda_k / d E_e   =  x_{k,e}^T Kbar_t(e) x_{k,e}
+//   d lambda_k / d rho_e = -lambda_k x_{k,e}^T Mbar_t(e) x_{k,e}
 // (simple eigenvalues only; modes whose relative gap to a neighbour is below
 // gapTol get weight 0 in the weighted sums and NaN in the per-mode output).
 //
-// One CTA per element at a time (persistent over elements): Kbar and Mbar in
-// shared memory, the element's rows of X gathered 32 modes at a time, the
-// two quadratic forms per mode as shared-memory matrix products.
+// One CTA per element at a time (persistent over elements): the element
+// type's Kbar and Mbar in shared memory (reloaded when the type changes), the
+// element's rows of X gathered 32 modes at a time, the two quadratic forms
+// per mode as shared-memory matrix products.
 #include <cmath>
 
 #include "common.cuh"
@@ -24,7 +25,8 @@ constexpr int kModes = 32;
 }
 
 __global__ void __launch_bounds__(256) sensitivityKernel(
-    int64_t nelem, int nd, const int64_t* __restrict__ dofmap, const double* __restrict__ Kbar,
+    int64_t nelem, int nd, const int64_t* __restrict__ dofmap, const int32_t* __restrict__ elemType,
+    const double* __restrict__ Kbar,
     const double* __restrict__ Mbar, const double* __restrict__ X, int64_t n, int nmodes,
     const double* __restrict__ lambda, const double* __restrict__ weight,
     double* __restrict__ gE, double* __restrict__ gRho, double* __restrict__ dE,
@@ -35,12 +37,19 @@ __global__ void __launch_bounds__(256) sensitivityKernel(
     double* sX = sM + nd * nd;                // nd x kModes
     __shared__ int64_t sDof[kMaxDofE];
     __shared__ double sA[kModes], sB[kModes];
-    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
-        sK[t] = Kbar[t];
-        sM[t] = Mbar[t];
-    }
+    int loaded = -1;                          // element type held in sK / sM
     for (int64_t e = blockIdx.x; e < nelem; e += gridDim.x) {
         __syncthreads();
+        const int ty = elemType ? elemType[e] : 0;
+        if (ty != loaded) {
+            const double* kb = Kbar + (int64_t)ty * nd * nd;
+            const double* mb = Mbar + (int64_t)ty * nd * nd;
+            for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
+                sK[t] = kb[t];
+                sM[t] = mb[t];
+            }
+            loaded = ty;
+        }
         for (int t = threadIdx.x; t < nd; t += blockDim.x) sDof[t] = dofmap[e * nd + t];
         double accE = 0.0, accR = 0.0;   // weighted sums (thread 0 keeps them)
         for (int k0 = 0; k0 < nmodes; k0 += kModes) {
@@ -104,7 +113,8 @@ __global__ void __launch_bounds__(256) sensitivityKernel(
     }
 }
 
-cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, const double* Kbar,
+cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, const int32_t* elemType,
+                              const double* Kbar,
                               const double* Mbar, const double* X, int64_t n, int nmodes,
                               const double* lambda, const double* weight, double* gE,
                               double* gRho, double* dE, double* dRho, cudaStream_t s) {
@@ -120,7 +130,7 @@ cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t grid = nelem < (int64_t)sms ? nelem : (int64_t)sms;
-    sensitivityKernel<<<(int)grid, 256, smem, s>>>(nelem, nd, dofmap, Kbar, Mbar, X, n, nmodes,
+    sensitivityKernel<<<(int)grid, 256, smem, s>>>(nelem, nd, dofmap, elemType, Kbar, Mbar, X, n, nmodes,
                                                     lambda, weight, gE, gRho, dE, dRho);
     return cudaGetLastError();
 }

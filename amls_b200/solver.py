@@ -1,7 +1,7 @@
 """Host-side mirror of the reference's solver interface over the C ABI.
 
 ``AmlsSolver.solve(K, M, opt)`` corresponds to ``AmlsSolver::solve``
-(src/amls/solver.cpp:154-373): same options and defaults, same exceptions
+(src/amls/solver.cpp:100-319): same options and defaults, same exceptions
 (``ValueError`` for std::invalid_argument, ``RuntimeError`` subclasses for
 std::runtime_error), ``Solution`` with theta ascending, Z M-normalised in the
 original ordering, the reduced size p and the phase timings.
@@ -164,16 +164,25 @@ class AmlsSolver:
         out["p"] = int(p.value)
         return out
 
-    def sensitivities(self, pencil, weights=None, per_mode: bool = False, gap_tol: float = 1e-6):
+    def sensitivities(self, pencil, weights=None, per_mode: bool = False, gap_tol: float = 1e-6,
+                      elem_type=None):
         """Per-element eigenvalue sensitivities of the last solve's eigenpairs
-        for a hex pencil (K = sum E_e Kbar, M = sum rho_e Mbar).  Returns
-        dict(gE, gRho, simple[, dE, dRho]) with gE/gRho the gradient of
+        for an element pencil (K = sum E_e Kbar_t(e), M = sum rho_e Mbar_t(e)).
+        ``pencil.Kbar``/``pencil.Mbar`` are one element pair (nd x nd) or a
+        stack (ntypes x nd x nd) indexed by ``elem_type`` (nelem ints).
+        Returns dict(gE, gRho, simple[, dE, dRho]) with gE/gRho the gradient of
         sum_k w_k lambda_k over simple modes (zeros without weights) and
         dE/dRho of shape (nelem, nev) when per_mode."""
         dm = np.ascontiguousarray(pencil.dofmap, dtype=np.int64)
         nelem, nd = dm.shape
-        Kb = np.asfortranarray(pencil.Kbar, dtype=np.float64).ravel(order="F")
-        Mb = np.asfortranarray(pencil.Mbar, dtype=np.float64).ravel(order="F")
+        Kbar = np.asarray(pencil.Kbar, dtype=np.float64)
+        Mbar = np.asarray(pencil.Mbar, dtype=np.float64)
+        if Kbar.ndim == 2:
+            Kbar, Mbar = Kbar[None], Mbar[None]
+        ntypes = Kbar.shape[0]
+        Kb = np.ascontiguousarray(Kbar.transpose(0, 2, 1)).ravel()      # column-major per type
+        Mb = np.ascontiguousarray(Mbar.transpose(0, 2, 1)).ravel()
+        et = None if elem_type is None else np.ascontiguousarray(elem_type, dtype=np.int32)
         nev = self._last_nev
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
         gE = np.zeros(nelem)
@@ -182,7 +191,8 @@ class AmlsSolver:
         dE = np.zeros((nev, nelem)) if per_mode else None
         dR = np.zeros((nev, nelem)) if per_mode else None
         _lib.check(_lib.lib().amls_sensitivities(
-            self._h, nelem, nd, _lib.ptr(dm), _lib.ptr(Kb), _lib.ptr(Mb), _lib.ptr(w),
+            self._h, nelem, nd, _lib.ptr(dm), int(ntypes), _lib.ptr(et), _lib.ptr(Kb), _lib.ptr(Mb),
+            _lib.ptr(w),
             float(gap_tol), _lib.ptr(gE), _lib.ptr(gR), _lib.ptr(dE), _lib.ptr(dR),
             _lib.ptr(simple)))
         out = dict(gE=gE, gRho=gR, simple=simple.astype(bool))
@@ -211,8 +221,14 @@ class AmlsSolver:
         buf = np.zeros(_lib.INFO_SLOTS, np.int64)
         _lib.check(_lib.lib().amls_info(self._h, _lib.ptr(buf)))
         keys = ["tree_nodes", "levels", "p_passA", "p", "front_doubles", "device_bytes",
-                "launches", "refine_iters", "refine_nq"]
+                "launches", "refine_iters", "refine_nq", "n"]
         return {k: int(v) for k, v in zip(keys, buf)}
+
+    def permutation(self) -> np.ndarray:
+        """perm[new] = old of the last analysis on this handle."""
+        out = np.zeros(self.info()["n"], np.int64)
+        _lib.check(_lib.lib().amls_permutation(self._h, _lib.ptr(out)))
+        return out
 
     def work(self) -> dict:
         buf = np.zeros(_lib.WORK_SLOTS, np.float64)

@@ -35,8 +35,8 @@ extern "C" {
 #define AMLS_ERR_TIMEOUT 4          /* a bounded device-side wait expired         */
 #define AMLS_ERR_OOM 5              /* device allocation failed                   */
 #define AMLS_ERR_CUDA 6             /* other CUDA runtime error                   */
-#define AMLS_ERR_NUMERIC 7          /* reference: std::runtime_error (solver.cpp:202-203, 308-310) */
-#define AMLS_ERR_PARTITION 8        /* METIS failure (metis_partitioner.cpp:128-137) */
+#define AMLS_ERR_NUMERIC 7          /* reference: std::runtime_error (solver.cpp:107-111, 148-149, 254-256) */
+#define AMLS_ERR_PARTITION 8        /* METIS failure (metis_partitioner.cpp:95-96, 103-104) */
 #define AMLS_ERR_NO_DEVICE 9        /* no usable CUDA device                      */
 
 /* Options: the fields and defaults of AmlsOptions (src/amls/solver.hpp:18-30). */
@@ -47,7 +47,7 @@ typedef struct amls_options {
     double thresholdFactor;     /* 2.0  (eta) */
     int64_t fixedKeep;          /* 0    */
     int64_t nev;                /* 100  */
-    int64_t denseProjectedMax;  /* 5000 (warning only, as in solver.cpp:339-342) */
+    int64_t denseProjectedMax;  /* 5000 (warning only, as in solver.cpp:285-288) */
     double shift;               /* 0.0  K <- K + shift*M */
     int32_t numThreads;         /* 0    host threads (partition/analysis)  */
     int32_t recoverVectors;     /* 1    */
@@ -106,7 +106,7 @@ const char* amls_last_error(void);
 
 /* Nested dissection of the graph of |K|+|M| (host only, no GPU needed).
  * Replaces MetisPartitioner::recursiveBisection
- * (src/partition/metis_partitioner.cpp:143-212).  All output arrays are
+ * (src/partition/metis_partitioner.cpp:110-179).  All output arrays are
  * caller-owned with capacity n (idx_ptr: n+1):
  *   perm[n]            perm[new] = old
  *   *n_nodes           number of tree nodes N
@@ -121,7 +121,7 @@ int amls_partition(int64_t n, const int64_t* k_rowptr, const int32_t* k_col,
                    int64_t* idx);
 
 /* Whole AMLS solve from host CSR arrays.  Replaces AmlsSolver::solve
- * (src/amls/solver.cpp:154-373): optional shift, partition + permutation,
+ * (src/amls/solver.cpp:100-319): optional shift, partition + permutation,
  * two-pass truncation (k0 = max(4, ceil(3 nev / N)), lambda_cut = eta *
  * lambda_hat) or fixedKeep, reduced eigensolve, back-transform, un-permute
  * and M-normalisation.  Outputs (host, caller-owned):
@@ -152,9 +152,16 @@ int amls_solve_values(amls_handle h, const double* k_val, const double* m_val,
  *   info[0] tree nodes, [1] levels, [2] p of pass A, [3] p of the final pass,
  *   [4] sum of front sizes (doubles), [5] device bytes in use,
  *   [6] kernel launches in the last numeric solve,
- *   [7] refinement iterations, [8] refinement subspace size */
+ *   [7] refinement iterations, [8] refinement subspace size,
+ *   [9] order n of the analysed pencil */
 #define AMLS_INFO_SLOTS 16
 int amls_info(amls_handle h, int64_t* info);
+
+/* Permutation of the last analysis on the handle (amls_solve or
+ * amls_analyze): perm[n] with perm[new] = old, the post-order concatenation
+ * of the separator tree's node index lists (the reference's
+ * IPartitioner::Result::perm, src/partition/metis_partitioner.cpp:168-175). */
+int amls_permutation(amls_handle h, int64_t* perm);
 
 /* Algorithmic work of the last numeric solve, from the host ledger built
  * from the tree and the symbolic fronts (independent of the kernels):
@@ -198,30 +205,34 @@ int amls_sygvx_batched(amls_handle h, int32_t batch, const int64_t* n, const int
 
 /* Per-element eigenvalue sensitivities of the last amls_solve /
  * amls_solve_values on the handle (no counterpart in the reference).  For a
- * pencil assembled from one reference element pair with per-element scales,
- * K = sum_e E_e Kbar, M = sum_e rho_e Mbar, and the solve's M-normalised
- * eigenvectors x_k (kept on the device):
- *   dlambda_k/dE_e = x_{k,e}^T Kbar x_{k,e},
- *   dlambda_k/drho_e = -lambda_k x_{k,e}^T Mbar x_{k,e}
+ * pencil assembled from reference element pairs with per-element scales,
+ * K = sum_e E_e Kbar_t(e), M = sum_e rho_e Mbar_t(e) (t(e) the element's
+ * type), and the solve's M-normalised eigenvectors x_k (kept on the device):
+ *   dlambda_k/dE_e = x_{k,e}^T Kbar_t(e) x_{k,e},
+ *   dlambda_k/drho_e = -lambda_k x_{k,e}^T Mbar_t(e) x_{k,e}
  * (adjoint form, simple eigenvalues only).  Inputs (host):
  *   dofmap[nelem * ndofe]   global DOF of each element DOF, -1 = constrained
- *   Kbar, Mbar [ndofe^2]     column-major element matrices (ndofe <= 96)
+ *   ntypes, elemType[nelem] element types 0 .. ntypes-1 (elemType NULL: one
+ *                           type, ntypes must be 1)
+ *   Kbar, Mbar [ntypes * ndofe^2]  column-major element matrices per type
+ *                           (ndofe <= 96)
  *   weights[nev] or NULL     w_k of the weighted sum sum_k w_k lambda_k
  *   gapTol                   modes with relative gap <= gapTol are not simple
  * Outputs (host, NULL to skip): gE[nelem], gRho[nelem] the gradient of
  * sum_k w_k lambda_k over the simple modes; dE, dRho [nelem * nev]
  * (column-major, NaN for non-simple modes); simple[nev] 1/0. */
 int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, const int64_t* dofmap,
-                       const double* Kbar, const double* Mbar, const double* weights,
-                       double gapTol, double* gE, double* gRho, double* dE, double* dRho,
-                       int32_t* simple);
+                       int32_t ntypes, const int32_t* elemType, const double* Kbar,
+                       const double* Mbar, const double* weights, double gapTol, double* gE,
+                       double* gRho, double* dE, double* dRho, int32_t* simple);
 
 /* Allocation-free dense generalized eigensolver (no counterpart in the
- * reference).  For callers that cannot allocate device memory: code inside a
- * CUDA graph capture, hosts whose memory pool owns every allocation, or
- * loops that must not enter the allocator.  Lowest k eigenpairs of one dense
- * pencil (K, M), M positive definite, of order n <= AMLS_NOALLOC_MAX_N:
- * same semantics as amls_sygvx_batched in index mode (il = 1, iu = k).
+ * reference).  For callers that cannot allocate device memory: a host
+ * application whose own memory pool owns every device allocation, or a
+ * real-time loop that must never enter the driver's allocator.  Lowest k
+ * eigenpairs of one dense pencil (K, M), M positive definite, of order
+ * n <= AMLS_NOALLOC_MAX_N: same semantics as amls_sygvx_batched in index
+ * mode (il = 1, iu = k).
  *   K, M   device pointers, n x n column-major (read only)
  *   w      device pointer, k eigenvalues ascending
  *   V      device pointer, n x k M-orthonormal eigenvectors, column-major
@@ -230,10 +241,13 @@ int amls_sensitivities(amls_handle h, int64_t nelem, int32_t ndofe, const int64_
  * No handle, and no cudaMalloc/cudaFree or other allocating call: every
  * intermediate lives in a fixed-size device array inside the library
  * (about 1.5 MB, held on each GPU that loads the library until exit).  The
- * first call on a device looks up that array's address (make it before any
- * stream capture).  Calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller.  The call is synchronous on
- * `stream`.  Sizes beyond the limit return AMLS_ERR_INVALID_ARGUMENT. */
+ * first call on a device (and the first after its context is re-created)
+ * looks up that array's device address.  The call is synchronous: it reads
+ * a status word back and synchronises `stream` before returning.  Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Sizes beyond the limit return
+ * AMLS_ERR_INVALID_ARGUMENT; an M that is not positive definite returns
+ * AMLS_ERR_NOT_SPD. */
 #define AMLS_NOALLOC_MAX_N 128
 int amls_sygvx_lowest_noalloc(int64_t n, const double* K, const double* M, int64_t k,
                               double* w, double* V, int64_t* m, void* stream);

@@ -17,7 +17,7 @@ yuesewuta/AMLS after partitioning:
   ``sil_*``                    src/amls/shift_invert_lanczos.hpp:32-203.
 * truncation policies          src/amls/spectral_truncation.hpp:35-88.
 * ``SubspaceCondensationRef``  src/amls/subspace_condensation.cpp:18-319.
-* ``amls_solve_ref``           src/amls/solver.cpp:154-373.
+* ``amls_solve_ref``           src/amls/solver.cpp:100-319.
 
 Third-party arithmetic: LAPACK dsygvd/dsygvx (reference: netlib LAPACK,
 unpinned) is scipy's bundled LAPACK; Eigen's SimplicialLDLT/LDLT
@@ -564,7 +564,7 @@ class SubspaceCondensationRef:
 
 
 def assemble_mproj(r: CondResult) -> np.ndarray:
-    """solver.cpp:125-138: I + symmetric tree blocks."""
+    """solver.cpp:71-84: I + symmetric tree blocks."""
     Mp = np.eye(r.p)
     for (ri, ci, blk) in r.mproj_blocks:
         r0, c0 = r.proj_offset[ri], r.proj_offset[ci]
@@ -574,7 +574,7 @@ def assemble_mproj(r: CondResult) -> np.ndarray:
 
 
 def assemble_kproj(r: CondResult) -> np.ndarray:
-    """solver.cpp:140-150: diag(mu)."""
+    """solver.cpp:86-96: diag(mu)."""
     Kp = np.zeros((r.p, r.p))
     for i in range(len(r.k)):
         o = r.proj_offset[i]
@@ -584,7 +584,7 @@ def assemble_kproj(r: CondResult) -> np.ndarray:
 
 
 def solve_projected(r: CondResult, want: int):
-    """solver.cpp:199-215."""
+    """solver.cpp:145-161."""
     if r.p <= 0:
         raise RuntimeError("reduced problem is empty (all nodes truncated)")
     Mp = assemble_mproj(r)
@@ -629,7 +629,7 @@ def permute_symmetric(A: sp.csr_matrix, perm: np.ndarray) -> sp.csr_matrix:
 
 
 def amls_solve_ref(K: sp.csr_matrix, M: sp.csr_matrix, tree: Tree, opt: OptionsRef) -> SolutionRef:
-    """AmlsSolver::solve (solver.cpp:154-373) on a given partition tree."""
+    """AmlsSolver::solve (solver.cpp:100-319) on a given partition tree."""
     if opt.nev <= 0:
         raise ValueError("nev must be positive")
     n = K.shape[0]
