@@ -37,7 +37,8 @@ EXPORTS = [
     "amls_options_default", "amls_create", "amls_destroy", "amls_last_error", "amls_partition",
     "amls_solve", "amls_analyze", "amls_solve_values", "amls_info", "amls_work",
     "amls_sygvx_batched", "amls_set_profiling", "amls_kernel_times", "amls_category_work",
-    "amls_sygvx_lowest_noalloc", "amls_sensitivities", "amls_permutation",
+    "amls_sygvx_lowest_noalloc", "amls_sensitivities", "amls_permutation", "amls_solve_batch",
+    "amls_analyze_batch", "amls_solve_values_batch",
 ]
 NOALLOC_MAX_N = 128
 
@@ -50,7 +51,7 @@ class Options(C.Structure):
         ("denseProjectedMax", C.c_int64), ("shift", C.c_double), ("numThreads", C.c_int32),
         ("recoverVectors", C.c_int32), ("verbosity", C.c_int32), ("refine", C.c_int32),
         ("refineMaxIter", C.c_int32), ("refineExtra", C.c_int32), ("refineTol", C.c_double),
-        ("precision", C.c_int32),
+        ("precision", C.c_int32), ("silMode", C.c_int32),
     ]
 
 
@@ -87,6 +88,9 @@ def lib() -> C.CDLL:
                                                 C.POINTER(C.c_int64), P]
         L.amls_work.argtypes = [P, P]
         L.amls_permutation.argtypes = [P, P]
+        L.amls_solve_batch.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, C.POINTER(Options), P, P, P, P]
+        L.amls_analyze_batch.argtypes = [P, C.c_int32, P, P, P, P, P, C.POINTER(Options)]
+        L.amls_solve_values_batch.argtypes = [P, P, P, C.c_int32, P, P, P, C.c_int32, P]
         L.amls_sygvx_batched.argtypes = [P, C.c_int32, P, P, P, P, C.c_int32, C.c_int64,
                                          C.c_int64, C.c_double, C.c_double, P, P, P, P, P, P]
         _lib = L

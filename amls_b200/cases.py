@@ -286,7 +286,15 @@ def config_pencil(name: str, seed: int = 0) -> Pencil:
     return hex_pencil(e, e, e, order, seed=seed)
 
 
-def batch_shapes(count: int = 256, seed: int = 0):
-    """Box shapes (a, b, c) ~ U{4..12} for the uneven pencil batch."""
+def batch_shapes(count: int = 256, seed: int = 0, lo: int = 4, hi: int = 12):
+    """Box shapes (a, b, c) ~ U{lo..hi} for the uneven pencil batch."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    return [tuple(int(v) for v in rng.integers(4, 13, size=3)) for _ in range(count)]
+    return [tuple(int(v) for v in rng.integers(lo, hi + 1, size=3)) for _ in range(count)]
+
+
+def batch_pencils(count: int = 256, seed: int = 0, lo: int = 4, hi: int = 12) -> list[Pencil]:
+    """The uneven batch: 8-node hex elasticity boxes of a x b x c elements
+    (a, b, c ~ U{lo..hi}), face x = 0 clamped, the E / rho perturbation law
+    of hex_pencil with a seed per pencil (seed * 1000003 + b + 1)."""
+    return [hex_pencil(a, b_, c, 1, seed=seed * 1000003 + q + 1)
+            for q, (a, b_, c) in enumerate(batch_shapes(count, seed, lo, hi))]

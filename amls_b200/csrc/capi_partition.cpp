@@ -37,6 +37,7 @@ extern "C" int amls_options_default(amls_options* opt) {
     opt->refineExtra = -1;
     opt->refineTol = 1e-9;
     opt->precision = AMLS_PRECISION_FP64;
+    opt->silMode = 0;
     return AMLS_OK;
 }
 

@@ -23,6 +23,8 @@ int checkOptions(const amls_options* opt) {
     if (opt->nev <= 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
     if (opt->leafSize < 1) return fail(AMLS_ERR_INVALID_ARGUMENT, "leafSize must be >= 1");
     if (opt->nLevels < 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "nLevels must be >= 0");
+    if (opt->silMode < -1 || opt->silMode > 1)
+        return fail(AMLS_ERR_INVALID_ARGUMENT, "silMode must be -1, 0 or 1");
     return AMLS_OK;
 }
 }  // namespace
@@ -91,6 +93,52 @@ extern "C" int amls_solve(amls_handle h, int64_t n, const int64_t* kp, const int
         h->eng->analyze(n, kp, kc, mp, mc, *opt);
         const auto t1 = std::chrono::steady_clock::now();
         h->eng->solveValues(kv, mv, false, theta, opt->recoverVectors ? Z : nullptr, false, p_out, t);
+        t[AMLS_T_PARTITION] = std::chrono::duration<double>(t1 - t0).count();
+        t[AMLS_T_TOTAL] += t[AMLS_T_PARTITION];
+        if (timing) std::memcpy(timing, t, sizeof(t));
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_analyze_batch(amls_handle h, int32_t batch, const int64_t* pencil_off,
+                                  const int64_t* kp, const int32_t* kc, const int64_t* mp,
+                                  const int32_t* mc, const amls_options* opt) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (int e = checkOptions(opt)) return e;
+        if (batch < 1 || !pencil_off) return fail(AMLS_ERR_INVALID_ARGUMENT, "empty batch");
+        if (pencil_off[0] != 0) return fail(AMLS_ERR_INVALID_ARGUMENT, "pencil_off[0] must be 0");
+        for (int b = 0; b < batch; ++b)
+            if (pencil_off[b + 1] <= pencil_off[b]) return fail(AMLS_ERR_INVALID_ARGUMENT, "empty pencil in the batch");
+        if (!kp || !kc || !mp || !mc) return fail(AMLS_ERR_INVALID_ARGUMENT, "null CSR array");
+        if (batch > 1 && opt->refine) return fail(AMLS_ERR_INVALID_ARGUMENT, "refinement needs a single pencil");
+        h->eng->analyzeBatch(batch, pencil_off, kp, kc, mp, mc, *opt);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_solve_values_batch(amls_handle h, const double* kv, const double* mv,
+                                       int32_t values_on_device, double* theta, int64_t* m, double* Z,
+                                       int32_t outputs_on_device, double* timing) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!kv || !mv || !theta || !m) return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        h->eng->solveValues(kv, mv, values_on_device != 0, theta, Z, outputs_on_device != 0, nullptr, timing, m);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_solve_batch(amls_handle h, int32_t batch, const int64_t* pencil_off, const int64_t* kp,
+                                const int32_t* kc, const double* kv, const int64_t* mp, const int32_t* mc,
+                                const double* mv, const amls_options* opt, double* theta, int64_t* m,
+                                double* Z, double* timing) {
+    return guarded([&]() -> int {
+        if (!kv || !mv || !theta || !m) return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        const auto t0 = std::chrono::steady_clock::now();
+        if (int e = amls_analyze_batch(h, batch, pencil_off, kp, kc, mp, mc, opt)) return e;
+        const auto t1 = std::chrono::steady_clock::now();
+        double t[AMLS_T_SLOTS] = {0};
+        h->eng->solveValues(kv, mv, false, theta, opt->recoverVectors ? Z : nullptr, false, nullptr, t, m);
         t[AMLS_T_PARTITION] = std::chrono::duration<double>(t1 - t0).count();
         t[AMLS_T_TOTAL] += t[AMLS_T_PARTITION];
         if (timing) std::memcpy(timing, t, sizeof(t));

@@ -179,6 +179,18 @@ double Engine::elapsed(cudaEvent_t a, cudaEvent_t b) {
 // ---------------------------------------------------------------------------
 void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
                      const int32_t* mc, const amls_options& opt) {
+    const int64_t off[2] = {0, n};
+    analyzeBatch(1, off, kp, kc, mp, mc, opt);
+}
+
+// A batch of independent pencils is one block-diagonal pencil whose diagonal
+// blocks (pencil b: rows and columns pOff[b] .. pOff[b+1]) are partitioned
+// separately, as the reference solves each pencil on its own; the trees form
+// a forest, and every level-batched launch below covers the same tree level
+// of all pencils at once.
+void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const int32_t* kc,
+                          const int64_t* mp, const int32_t* mc, const amls_options& opt) {
+    const int64_t n = pOff[P];
     cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
     analyzed_ = false;
     tridiagDone_ = false;
@@ -196,29 +208,82 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     nnzM_ = mp[n];
 
     const Clock::time_point ta0 = Clock::now();
-    PartitionResult pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize, opt.numThreads);
+    // forest: the trees of the pencils with global node ids and DOF indices
+    struct FNode {
+        std::vector<int64_t> idx;
+        int64_t parent = -1;
+        std::vector<int64_t> children;
+    };
+    std::vector<FNode> forest;
+    std::vector<int64_t> post;
+    nPencils_ = P;
+    pOff_.assign(pOff, pOff + P + 1);
+    pencilOf_.clear();
+    pNodes_.assign(static_cast<size_t>(P), 0);
+    perm_.clear();
+    for (int b = 0; b < P; ++b) {
+        const int64_t o = pOff[b], nb = pOff[b + 1] - pOff[b];
+        if (nb <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty pencil in the batch");
+        PartitionResult pr;
+        if (P == 1) {
+            pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize, opt.numThreads);
+        } else {
+            // the pencil's diagonal block with local indices
+            std::vector<int64_t> bkp(static_cast<size_t>(nb + 1)), bmp(static_cast<size_t>(nb + 1));
+            std::vector<int32_t> bkc(static_cast<size_t>(kp[o + nb] - kp[o])), bmc(static_cast<size_t>(mp[o + nb] - mp[o]));
+            for (int pass = 0; pass < 2; ++pass) {
+                const int64_t* rp = pass ? mp : kp;
+                const int32_t* ci = pass ? mc : kc;
+                std::vector<int64_t>& orp = pass ? bmp : bkp;
+                std::vector<int32_t>& oci = pass ? bmc : bkc;
+                for (int64_t r = 0; r <= nb; ++r) orp[static_cast<size_t>(r)] = rp[o + r] - rp[o];
+                for (int64_t e = rp[o]; e < rp[o + nb]; ++e) {
+                    const int64_t c = ci[e] - o;
+                    if (c < 0 || c >= nb) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "batch pencils are coupled");
+                    oci[static_cast<size_t>(e - rp[o])] = static_cast<int32_t>(c);
+                }
+            }
+            // one in-process METIS call at a time (it re-seeds at every call)
+            pr = recursiveBisection(nb, bkp.data(), bkc.data(), bmp.data(), bmc.data(), opt.nLevels,
+                                    opt.leafSize, 1);
+        }
+        const int64_t base = static_cast<int64_t>(forest.size());
+        for (int64_t id = 0; id < pr.tree.nNodes(); ++id) {
+            const TreeNode& t = pr.tree.node(id);
+            FNode f;
+            f.idx.reserve(t.indices.size());
+            for (int64_t v : t.indices) f.idx.push_back(v + (P == 1 ? 0 : o));
+            f.parent = t.parent < 0 ? -1 : t.parent + base;
+            for (int64_t c : t.children) f.children.push_back(c + base);
+            forest.push_back(std::move(f));
+            pencilOf_.push_back(b);
+        }
+        for (int64_t id : pr.tree.postOrder()) {
+            post.push_back(id + base);
+            for (int64_t v : pr.tree.node(id).indices) perm_.push_back(v + (P == 1 ? 0 : o));
+        }
+        pNodes_[static_cast<size_t>(b)] = static_cast<int>(pr.tree.nNodes());
+    }
     const Clock::time_point ta1 = Clock::now();
-    perm_ = pr.perm;
     inv_.assign(static_cast<size_t>(n), 0);
     for (int64_t j = 0; j < n; ++j) inv_[static_cast<size_t>(perm_[static_cast<size_t>(j)])] = j;
-    const SeparatorTree& T = pr.tree;
-    const int N = static_cast<int>(T.nNodes());
+    const int N = static_cast<int>(forest.size());
     nodes_.assign(static_cast<size_t>(N), Node());
     order_.clear();
-    for (int64_t id : T.postOrder()) order_.push_back(static_cast<int>(id));
+    for (int64_t id : post) order_.push_back(static_cast<int>(id));
     int64_t acc = 0;
     for (int i : order_) {
         Node& nd = nodes_[static_cast<size_t>(i)];
         nd.off = acc;
-        nd.n = static_cast<int64_t>(T.node(i).indices.size());
-        nd.parent = static_cast<int>(T.node(i).parent);
-        for (int64_t a : T.ancestors(i)) nd.anc.push_back(static_cast<int>(a));
+        nd.n = static_cast<int64_t>(forest[static_cast<size_t>(i)].idx.size());
+        nd.parent = static_cast<int>(forest[static_cast<size_t>(i)].parent);
+        for (int64_t a = nd.parent; a >= 0; a = forest[static_cast<size_t>(a)].parent) nd.anc.push_back(static_cast<int>(a));
         acc += nd.n;
     }
     maxLevel_ = 0;
     for (int i : order_) {
         int l = 0;
-        for (int64_t c : T.node(i).children) l = std::max(l, nodes_[static_cast<size_t>(c)].level + 1);
+        for (int64_t c : forest[static_cast<size_t>(i)].children) l = std::max(l, nodes_[static_cast<size_t>(c)].level + 1);
         nodes_[static_cast<size_t>(i)].level = l;
         maxLevel_ = std::max(maxLevel_, l);
     }
@@ -235,7 +300,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     std::vector<int64_t> subStart(static_cast<size_t>(N));
     for (int i : order_) {
         int64_t s = nodes_[static_cast<size_t>(i)].off;
-        for (int64_t c : T.node(i).children) s = std::min(s, subStart[static_cast<size_t>(c)]);
+        for (int64_t c : forest[static_cast<size_t>(i)].children) s = std::min(s, subStart[static_cast<size_t>(c)]);
         subStart[static_cast<size_t>(i)] = s;
     }
 
@@ -386,6 +451,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
             }
             SpmmSuper S{};
             S.row0 = r;
+            S.pencil = static_cast<int32_t>(std::upper_bound(pOff_.begin(), pOff_.end(), r) - pOff_.begin() - 1);
             S.rows = static_cast<int32_t>(e - r);
             S.colOff = static_cast<int64_t>(ucols.size());
             S.len = static_cast<int32_t>(uni.size());
@@ -418,6 +484,17 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     cudaCheck(cudaMemcpyAsync(mCi_.as<int32_t>(), mc, sizeof(int32_t) * nnzM_, cudaMemcpyHostToDevice, stream_), "upload");
     cudaCheck(cudaMemcpyAsync(invDev_.as<int64_t>(), inv_.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, stream_), "upload");
     cudaCheck(cudaMemcpyAsync(permDev_.as<int64_t>(), perm_.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, stream_), "upload");
+    if (P > 1) {
+        // pencil of every permuted DOF (the M-norms of a batch are per pencil)
+        std::vector<int32_t> pd(static_cast<size_t>(n));
+        for (int i = 0; i < N; ++i)
+            for (int64_t r = nodes_[static_cast<size_t>(i)].off; r < nodes_[static_cast<size_t>(i)].off + nodes_[static_cast<size_t>(i)].n; ++r)
+                pd[static_cast<size_t>(r)] = pencilOf_[static_cast<size_t>(i)];
+        pencilDev_.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+        cudaCheck(cudaMemcpyAsync(pencilDev_.as<int32_t>(), pd.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream_),
+                  "upload");
+        cudaCheck(cudaStreamSynchronize(stream_), "upload");
+    }
     cudaCheck(cudaMemcpyAsync(kDst_.as<int64_t>(), hostKDst_.data(), sizeof(int64_t) * nnzK_, cudaMemcpyHostToDevice, stream_), "upload");
     cudaCheck(cudaMemcpyAsync(mDst_.as<int64_t>(), hostMDst_.data(), sizeof(int64_t) * nnzM_, cudaMemcpyHostToDevice, stream_), "upload");
     kVal_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(nnzK_, 1)));
@@ -435,6 +512,7 @@ void Engine::analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int6
     ePool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     tauPool_.ensure(sizeof(double) * static_cast<size_t>(vecTotal_));
     invPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(invTotal_, 1)));
+    silAnalyze(kp, kc, mp, mc);
     const Clock::time_point ta4 = Clock::now();
     buildStatic();
     cudaCheck(cudaStreamSynchronize(stream_), "analyze");
@@ -584,6 +662,7 @@ void Engine::buildStatic() {
         L.uTiles = sblob_.add(ut);
         L.nUTiles = static_cast<int>(ut.size());
     }
+    silBuildStatic();
     sblob_.upload(staticBlob_, stream_);
 
     // ---- ledger: elimination flops/bytes (total and per kernel category) ----
@@ -658,6 +737,9 @@ void Engine::dropGraphs() {
 void Engine::eliminateLaunches(cudaStream_t s) {
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelPlan& L = levelPlans_[static_cast<size_t>(l)];
+        const SilLevelCopy& sc = silCopy_[static_cast<size_t>(l)];
+        if (sc.nTiles > 0)       // K^_ii of the level's shift-invert nodes, before it is factored in place
+            LAUNCH(launchSilSymCopy(sblob_.dev<SilCopyDesc>(sc.desc), sblob_.dev<TileRef>(sc.tiles), sc.nTiles, s));
         runCholPlan(sblob_, L.chol, s);
         LAUNCH(launchGemmM(sblob_.dev<GemmDesc>(L.w.desc), sblob_.dev<TileRef>(L.w.tiles), L.w.nTiles, s));
         LAUNCH(launchGemmM(sblob_.dev<GemmDesc>(L.c.desc), sblob_.dev<TileRef>(L.c.tiles), L.c.nTiles, s));
@@ -795,8 +877,12 @@ void Engine::tridiagonalizeAll(cudaStream_t s) {
 }
 
 // modes: 0 = index (the `want` largest nu), 1 = interval (nu >= thr)
-void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
+void Engine::condense(int mode, const std::vector<int>& wantP, const std::vector<double>& thrP,
+                      const std::vector<double>& hiP, Pass& P, cudaStream_t s) {
     const int N = static_cast<int>(nodes_.size());
+    const int Pn = nPencils_;
+    int want = 0;
+    for (int b = 0; b < Pn; ++b) want = std::max(want, wantP[static_cast<size_t>(b)]);
     if (!tridiagDone_) tridiagonalizeAll(s);
     // ---- counts ----
     P.k.assign(static_cast<size_t>(N), 0);
@@ -813,26 +899,45 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
         e.n = static_cast<int32_t>(nd.n);
         e.id = i;
         e.kOut = kOutDev_.as<int32_t>() + i;
-        e.kcap = (mode == 0) ? static_cast<int32_t>(std::min<int64_t>(want, nd.n)) : static_cast<int32_t>(nd.n);
+        e.kcap = (mode == 0) ? static_cast<int32_t>(std::min<int64_t>(wantP[static_cast<size_t>(pencilOf_[static_cast<size_t>(i)])], nd.n))
+                             : static_cast<int32_t>(nd.n);
         descs[static_cast<size_t>(i)] = e;
     }
+    // per-node thresholds of the interval mode (the pencil's 1 / lambda_cut)
+    std::vector<double> thrNode(static_cast<size_t>(N), 0.0);
+    for (int i = 0; i < N; ++i) thrNode[static_cast<size_t>(i)] = thrP[static_cast<size_t>(pencilOf_[static_cast<size_t>(i)])];
+    // shift-invert Lanczos nodes first (the reference's SIL branch); a node it
+    // serves takes no part in the dense eigensolves below
+    std::vector<int> kSil;
+    silSelect(mode, wantP, hiP, kSil, s);
+    for (int i = 0; i < N; ++i)
+        if (kSil[static_cast<size_t>(i)] > 0) descs[static_cast<size_t>(i)].kcap = 0;
     {
         Blob b;
         const size_t o = b.add(descs);
+        const size_t oThr = b.add(thrNode);
         b.upload(passBlob_, s);
-        LAUNCH(launchBisect(b.dev<EigDesc>(o), N, mode == 0 ? 0 : 1, want, thr, 0, nullptr, s));
+        LAUNCH(launchBisect(b.dev<EigDesc>(o), N, mode == 0 ? 0 : 1, 1 << 30, 0.0, 0, nullptr, s,
+                            b.dev<double>(oThr)));
         std::vector<int32_t> kh(static_cast<size_t>(N));
         cudaCheck(cudaMemcpyAsync(kh.data(), kOutDev_.as<int32_t>(), sizeof(int32_t) * N, cudaMemcpyDeviceToHost, s), "k");
         cudaCheck(cudaStreamSynchronize(s), "counts");
-        for (int i = 0; i < N; ++i) P.k[static_cast<size_t>(i)] = kh[static_cast<size_t>(i)];
+        for (int i = 0; i < N; ++i)
+            P.k[static_cast<size_t>(i)] = kSil[static_cast<size_t>(i)] > 0 ? kSil[static_cast<size_t>(i)]
+                                                                         : kh[static_cast<size_t>(i)];
     }
     // ---- offsets, buffers ----
     P.projOff.assign(static_cast<size_t>(N), 0);
+    P.localOff.assign(static_cast<size_t>(N), 0);
+    P.pp.assign(static_cast<size_t>(Pn), 0);
     int64_t p = 0, ysz = 0, wsz = 0;
     yOff_.assign(static_cast<size_t>(N), 0);
     int maxK = 0;
     for (int i = 0; i < N; ++i) {
         P.projOff[static_cast<size_t>(i)] = p;     // by node id, as the reference's finalize
+        int64_t& pb = P.pp[static_cast<size_t>(pencilOf_[static_cast<size_t>(i)])];
+        P.localOff[static_cast<size_t>(i)] = pb;   // inside the node's own pencil
+        pb += P.k[static_cast<size_t>(i)];
         p += P.k[static_cast<size_t>(i)];
         yOff_[static_cast<size_t>(i)] = ysz;
         ysz += nodes_[static_cast<size_t>(i)].n * P.k[static_cast<size_t>(i)];
@@ -840,20 +945,32 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
         maxK = std::max(maxK, P.k[static_cast<size_t>(i)]);
     }
     P.p = p;
-    if (p <= 0) throw AmlsError(AMLS_ERR_NUMERIC, "reduced problem is empty (all nodes truncated)");
+    P.credOff.assign(static_cast<size_t>(Pn), 0);
+    P.credTotal = 0;
+    for (int b = 0; b < Pn; ++b) {
+        const int64_t pb = P.pp[static_cast<size_t>(b)];
+        if (pb <= 0) throw AmlsError(AMLS_ERR_NUMERIC, "reduced problem is empty (all nodes truncated)");
+        P.credOff[static_cast<size_t>(b)] = P.credTotal;
+        P.credTotal += pb * pb;
+    }
     yPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(ysz, 1)));
     wPool_.ensure(sizeof(double) * static_cast<size_t>(p));
     iiWork_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(wsz, 1)));
     int64_t workOff = 0;
     for (int i = 0; i < N; ++i) {
         EigDesc& e = descs[static_cast<size_t>(i)];
-        e.kcap = P.k[static_cast<size_t>(i)];
+        e.kcap = kSil[static_cast<size_t>(i)] > 0 ? 0 : P.k[static_cast<size_t>(i)];
         e.w = wPool_.as<double>() + P.projOff[static_cast<size_t>(i)];
         e.Y = yPool_.as<double>() + yOff_[static_cast<size_t>(i)];
         e.ldy = std::max<int64_t>(nodes_[static_cast<size_t>(i)].n, 1);
         e.work = iiWork_.as<double>() + workOff;
         workOff += 6 * nodes_[static_cast<size_t>(i)].n * P.k[static_cast<size_t>(i)];
     }
+
+    // Ritz vectors of the shift-invert nodes in the engine's local form
+    silVectors(kSil, P.projOff, s);
+    silServed_ = 0;
+    for (int i = 0; i < N; ++i) silServed_ += kSil[static_cast<size_t>(i)] > 0 ? 1 : 0;
 
     // ---- projection tables (all levels) ----
     const double* F = kPool_.as<double>();
@@ -869,7 +986,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
         }
     }
     panelPool_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(panelTot, 1)));
-    credPool_.ensure(sizeof(double) * static_cast<size_t>(p * p));
+    credPool_.ensure(sizeof(double) * static_cast<size_t>(P.credTotal));
     double* panel = panelPool_.as<double>();
     double* cred = credPool_.as<double>();
     // descendants with k > 0, in post-order, per node; Wt sizes
@@ -895,6 +1012,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
 
     Blob b;
     const size_t oDescs = b.add(descs);
+    const size_t oThrNode = b.add(thrNode);
     // per-node index arrays for the scatters (own blob, uploaded first so the
     // GEMM descriptors can point into it)
     std::vector<int32_t> descRowIdx, nodeRowIdx;
@@ -902,25 +1020,30 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     std::vector<int64_t> oDescRow(static_cast<size_t>(N)), oDescCol(static_cast<size_t>(N)),
         oNodeRow(static_cast<size_t>(N)), oNodeCol(static_cast<size_t>(N)),
         oPanelCol(static_cast<size_t>(N)), oInitCol(static_cast<size_t>(N));
+    std::vector<int64_t> diagDst;                  // reduced-matrix diagonal of every mode
     for (int i = 0; i < N; ++i) {
+        const int pc = pencilOf_[static_cast<size_t>(i)];
+        const int64_t pb = P.pp[static_cast<size_t>(pc)], cb = P.credOff[static_cast<size_t>(pc)];
+        for (int a = 0; a < P.k[static_cast<size_t>(i)]; ++a)
+            diagDst.push_back(cb + (P.localOff[static_cast<size_t>(i)] + a) * (pb + 1));
         oDescRow[static_cast<size_t>(i)] = static_cast<int64_t>(descRowIdx.size());
         oDescCol[static_cast<size_t>(i)] = static_cast<int64_t>(descColOff.size());
         oPanelCol[static_cast<size_t>(i)] = static_cast<int64_t>(panelColOff.size());
         for (int kk : descK[static_cast<size_t>(i)]) {
-            const int64_t pk = P.projOff[static_cast<size_t>(kk)];
+            const int64_t pk = P.localOff[static_cast<size_t>(kk)];
             for (int bcol = 0; bcol < P.k[static_cast<size_t>(kk)]; ++bcol) {
                 descRowIdx.push_back(static_cast<int32_t>(pk + bcol));
-                descColOff.push_back((pk + bcol) * p);
+                descColOff.push_back(cb + (pk + bcol) * pb);
                 panelColOff.push_back(panelOff_[static_cast<size_t>(kk)] + bcol * nodes_[static_cast<size_t>(kk)].pathPrefix);
             }
         }
         oNodeRow[static_cast<size_t>(i)] = static_cast<int64_t>(nodeRowIdx.size());
         oNodeCol[static_cast<size_t>(i)] = static_cast<int64_t>(nodeColOff.size());
         oInitCol[static_cast<size_t>(i)] = static_cast<int64_t>(initColOff.size());
-        const int64_t pi = P.projOff[static_cast<size_t>(i)];
+        const int64_t pi = P.localOff[static_cast<size_t>(i)];
         for (int a = 0; a < P.k[static_cast<size_t>(i)]; ++a) {
             nodeRowIdx.push_back(static_cast<int32_t>(pi + a));
-            nodeColOff.push_back((pi + a) * p);
+            nodeColOff.push_back(cb + (pi + a) * pb);
             initColOff.push_back(panelOff_[static_cast<size_t>(i)] + a * nodes_[static_cast<size_t>(i)].pathPrefix);
         }
     }
@@ -931,7 +1054,8 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     std::vector<LevelTabs> tabs(static_cast<size_t>(maxLevel_) + 1);
     Blob idx;
     const size_t xDR = idx.add(descRowIdx), xDC = idx.add(descColOff), xNR = idx.add(nodeRowIdx),
-                 xNC = idx.add(nodeColOff), xPC = idx.add(panelColOff), xIC = idx.add(initColOff);
+                 xNC = idx.add(nodeColOff), xPC = idx.add(panelColOff), xIC = idx.add(initColOff),
+                 xDD = idx.add(diagDst);
     idx.upload(idxBlob_, s);
     const int32_t* dDR = idx.dev<int32_t>(xDR);
     const int64_t* dDC = idx.dev<int64_t>(xDC);
@@ -939,6 +1063,7 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     const int64_t* dNC = idx.dev<int64_t>(xNC);
     const int64_t* dPC = idx.dev<int64_t>(xPC);
     const int64_t* dIC = idx.dev<int64_t>(xIC);
+    const int64_t* dDD = idx.dev<int64_t>(xDD);
     const double* wDev = wPool_.as<double>();
 
     double fc = 0, bc = 0;
@@ -973,12 +1098,12 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                 }
                 fc += static_cast<double>(Ki) * ni * ni;
                 if (ki > 0) {
-                    GemmDesc a = gemm(ki, Ki, ni, kTransA | kTransB | kScatter, Yi, ni, wti, Ki, cred, p, 1.0, 0.0);
+                    GemmDesc a = gemm(ki, Ki, ni, kTransA | kTransB | kScatter, Yi, ni, wti, Ki, cred, 0, 1.0, 0.0);
                     a.rowIdx = dNR + oNodeRow[static_cast<size_t>(i)];
                     a.colOff = dDC + oDescCol[static_cast<size_t>(i)];
                     gemmTiles(g1T, static_cast<int>(g1.size()), ki, Ki, mTile());
                     g1.push_back(a);
-                    GemmDesc a2 = gemm(Ki, ki, ni, kScatter, wti, Ki, Yi, ni, cred, p, 1.0, 0.0);
+                    GemmDesc a2 = gemm(Ki, ki, ni, kScatter, wti, Ki, Yi, ni, cred, 0, 1.0, 0.0);
                     a2.rowIdx = dDR + oDescRow[static_cast<size_t>(i)];
                     a2.colOff = dNC + oNodeCol[static_cast<size_t>(i)];
                     gemmTiles(g2T, static_cast<int>(g2.size()), Ki, ki, mTile());
@@ -1001,11 +1126,16 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
                 a.colOff = dIC + oInitCol[static_cast<size_t>(i)];
                 gemmTiles(i1T, static_cast<int>(i1.size()), si, ki, mTile());
                 i1.push_back(a);
-                GemmDesc a2 = gemm(si, ki, ni, kScatter | kAccumulate | kColScale, F + nd.frontOff + ni, nd.ld, Yi,
-                                   ni, panel, 0, -0.5, 0.0);
+                // - L_Si C_i Y / 2: C_i Y = Y diag(nu) for exact local
+                // eigenvectors; shift-invert Ritz vectors bring C_i Y itself
+                const double* cy = silCYPtr_.empty() ? nullptr : silCYPtr_[static_cast<size_t>(i)];
+                GemmDesc a2 = cy ? gemm(si, ki, ni, kScatter | kAccumulate, F + nd.frontOff + ni, nd.ld, cy, ni,
+                                        panel, 0, -0.5, 0.0)
+                                 : gemm(si, ki, ni, kScatter | kAccumulate | kColScale, F + nd.frontOff + ni,
+                                        nd.ld, Yi, ni, panel, 0, -0.5, 0.0);
                 a2.rowIdx = rowSDev_ + nd.rowS;
                 a2.colOff = dIC + oInitCol[static_cast<size_t>(i)];
-                a2.colScale = wDev + P.projOff[static_cast<size_t>(i)];
+                if (!cy) a2.colScale = wDev + P.projOff[static_cast<size_t>(i)];
                 gemmTiles(i2T, static_cast<int>(i2.size()), si, ki, mTile());
                 i2.push_back(a2);
                 fc += 4.0 * si * ki * ni;
@@ -1026,18 +1156,20 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     const EigDesc* dd = b.dev<EigDesc>(oDescs);
     int maxNodeN = 1;
     for (const Node& nd : nodes_) maxNodeN = std::max<int>(maxNodeN, static_cast<int>(nd.n));
-    LAUNCH(launchBisectWarp(dd, N, mode == 0 ? 0 : 1, want, thr, maxK, s));
+    LAUNCH(launchBisectWarp(dd, N, mode == 0 ? 0 : 1, 1 << 30, 0.0, maxK, s, b.dev<double>(oThrNode)));
     LAUNCH(launchInverseIter(dd, N, maxK, nullptr, s));
     LAUNCH(launchBackTransformSmem(dd, N, maxK, std::min(maxNodeN, kTridiagSmallMax), s));
     {
         std::vector<int> kv(P.k.begin(), P.k.end());
+        for (int i = 0; i < N; ++i)
+            if (kSil[static_cast<size_t>(i)] > 0) kv[static_cast<size_t>(i)] = 0;
         backTransformBig(descs, kv, s);
     }
 
     // ---- projection ----
     LAUNCH(launchZero(panel, panelTot, s));
-    LAUNCH(launchZero(cred, p * p, s));
-    LAUNCH(launchSetDiagonal(cred, wDev, p, s));
+    LAUNCH(launchZero(cred, P.credTotal, s));
+    LAUNCH(launchScatterAdd(wDev, dDD, p, 1.0, cred, s));    // diagonal blocks: diag(nu)
     for (int l = 0; l <= maxLevel_; ++l) {
         const LevelTabs& T = tabs[static_cast<size_t>(l)];
         LAUNCH(launchGemmM(b.dev<GemmDesc>(T.pjD), b.dev<TileRef>(T.pjT), T.npjT, s));
@@ -1065,81 +1197,120 @@ void Engine::condense(int mode, int want, double thr, Pass& P, cudaStream_t s) {
     cudaCheck(cudaStreamSynchronize(s), "condense");
 }
 
-// largest `want` eigenpairs of the reduced matrix; fills P.theta ascending
-int Engine::reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors) {
-    const int64_t p = P.p;
-    want = static_cast<int>(std::min<int64_t>(want, p));
-    redD_.ensure(sizeof(double) * static_cast<size_t>(p));
-    redE_.ensure(sizeof(double) * static_cast<size_t>(p));
-    redTau_.ensure(sizeof(double) * static_cast<size_t>(p));
-    redW_.ensure(sizeof(double) * static_cast<size_t>(want));
-    redY_.ensure(sizeof(double) * static_cast<size_t>(p * want));
-    redWork_.ensure(sizeof(double) * static_cast<size_t>(6 * p * want));
-    redK_.ensure(sizeof(int32_t) * 4);
-    EigDesc e{};
-    e.A = credPool_.as<double>();
-    e.lda = p;
-    e.d = redD_.as<double>();
-    e.e = redE_.as<double>();
-    e.tau = redTau_.as<double>();
-    e.n = static_cast<int32_t>(p);
-    e.id = -1;
-    e.w = redW_.as<double>();
-    e.Y = redY_.as<double>();
-    e.ldy = p;
-    e.kcap = want;
-    e.kOut = redK_.as<int32_t>();
-    e.work = redWork_.as<double>();
+// per pencil the largest wantP[b] eigenvalues nu of its reduced matrix
+// Kp^-1/2 Mp Kp^-1/2 (theta = 1/nu ascending) and, with vectors, their
+// eigenvectors at redY_ + P.vOff[b] (pp_b x mMax, ld pp_b; columns beyond
+// the pencil's count are zero)
+void Engine::reducedSolve(Pass& P, const std::vector<int>& wantP, cudaStream_t s, bool vectors) {
+    const int Pn = nPencils_;
+    std::vector<int> want(static_cast<size_t>(Pn));
+    int wMax = 0;
+    int64_t pTot = 0, workTot = 0;
+    for (int b = 0; b < Pn; ++b) {
+        const int64_t pb = P.pp[static_cast<size_t>(b)];
+        want[static_cast<size_t>(b)] = static_cast<int>(std::min<int64_t>(wantP[static_cast<size_t>(b)], pb));
+        wMax = std::max(wMax, want[static_cast<size_t>(b)]);
+        pTot += pb;
+        workTot += 6 * pb * want[static_cast<size_t>(b)];
+    }
+    P.vOff.assign(static_cast<size_t>(Pn), 0);
+    int64_t yTot = 0;
+    for (int b = 0; b < Pn; ++b) {
+        P.vOff[static_cast<size_t>(b)] = yTot;
+        yTot += P.pp[static_cast<size_t>(b)] * wMax;
+    }
+    redD_.ensure(sizeof(double) * static_cast<size_t>(pTot));
+    redE_.ensure(sizeof(double) * static_cast<size_t>(pTot));
+    redTau_.ensure(sizeof(double) * static_cast<size_t>(pTot));
+    redW_.ensure(sizeof(double) * static_cast<size_t>(std::max(1, Pn * wMax)));
+    redY_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(yTot, 1)));
+    redWork_.ensure(sizeof(double) * static_cast<size_t>(std::max<int64_t>(workTot, 1)));
+    redK_.ensure(sizeof(int32_t) * static_cast<size_t>(Pn));
+    if (vectors && Pn > 1) LAUNCH(launchZero(redY_.as<double>(), yTot, s));
+    std::vector<EigDesc> all, small, large;
+    int64_t vo = 0, wo = 0;
+    int maxSmallN = 1;
+    for (int b = 0; b < Pn; ++b) {
+        const int64_t pb = P.pp[static_cast<size_t>(b)];
+        EigDesc e{};
+        e.A = credPool_.as<double>() + P.credOff[static_cast<size_t>(b)];
+        e.lda = pb;
+        e.d = redD_.as<double>() + vo;
+        e.e = redE_.as<double>() + vo;
+        e.tau = redTau_.as<double>() + vo;
+        e.n = static_cast<int32_t>(pb);
+        e.id = -1 - b;
+        e.w = redW_.as<double>() + static_cast<int64_t>(b) * wMax;
+        e.Y = redY_.as<double>() + P.vOff[static_cast<size_t>(b)];
+        e.ldy = pb;
+        e.kcap = want[static_cast<size_t>(b)];
+        e.kOut = redK_.as<int32_t>() + b;
+        e.work = redWork_.as<double>() + wo;
+        vo += pb;
+        wo += 6 * pb * want[static_cast<size_t>(b)];
+        all.push_back(e);
+        if (pb <= kSmallEig) {
+            small.push_back(e);
+            maxSmallN = std::max<int>(maxSmallN, static_cast<int>(pb));
+        } else {
+            large.push_back(e);
+        }
+    }
     Blob b;
-    const size_t o = b.add(&e, 1);
-    std::vector<int> gOf, gFirst{0}, gSize;
-    std::vector<int64_t> pOff{0};
-    int nCta = 0;
-    if (p > kSmallEig) {
-        nCta = tridiagLargeMaxCtas(static_cast<int>(p));
-        gOf.assign(static_cast<size_t>(nCta), 0);
-        gSize.push_back(nCta);
-    }
-    const size_t oGo = b.add(gOf), oGf = b.add(gFirst), oGs = b.add(gSize), oPo = b.add(pOff);
+    const size_t oA = b.add(all), oS = b.add(small);
     b.upload(redBlob_, s);
-    const EigDesc* dd = b.dev<EigDesc>(o);
-    if (p <= kSmallEig) LAUNCH(launchTridiagSmall(dd, 1, s));
-    else {
-        redP_.ensure(sizeof(double) * static_cast<size_t>(kTridiagPBufs * p));
-        LAUNCH(launchTridiagLargeGroups(dd, b.dev<int>(oGo), b.dev<int>(oGf), b.dev<int>(oGs), nCta,
-                                        redP_.as<double>(), b.dev<int64_t>(oPo), static_cast<int>(p), s));
-    }
-    LAUNCH(launchBisectWarp(dd, 1, 0, want, 0.0, want, s));
+    if (!small.empty()) LAUNCH(launchTridiagSmall(b.dev<EigDesc>(oS), static_cast<int>(small.size()), s));
+    if (!large.empty()) tridiagLargeAll(large, redP_, tlLargeBlob_, s);
+    LAUNCH(launchBisectWarp(b.dev<EigDesc>(oA), Pn, 0, wMax, 0.0, wMax, s));
     if (vectors) {
-        LAUNCH(launchInverseIter(dd, 1, want, nullptr, s));
-        if (p <= kSmallEig) LAUNCH(launchBackTransformSmem(dd, 1, want, static_cast<int>(p), s));
-        else backTransformBig({e}, {want}, s);
+        LAUNCH(launchInverseIter(b.dev<EigDesc>(oA), Pn, wMax, nullptr, s));
+        LAUNCH(launchBackTransformSmem(b.dev<EigDesc>(oA), Pn, wMax, std::min(maxSmallN, kTridiagSmallMax), s));
+        if (!large.empty()) {
+            std::vector<int> kv;
+            for (const EigDesc& e : large) kv.push_back(e.kcap);
+            backTransformBig(large, kv, s);
+        }
     }
-    std::vector<double> nu(static_cast<size_t>(want));
-    cudaCheck(cudaMemcpyAsync(nu.data(), redW_.as<double>(), sizeof(double) * want, cudaMemcpyDeviceToHost, s), "theta");
+    std::vector<double> nu(static_cast<size_t>(std::max(1, Pn * wMax)));
+    std::vector<int32_t> kk(static_cast<size_t>(Pn));
+    cudaCheck(cudaMemcpyAsync(nu.data(), redW_.as<double>(), sizeof(double) * Pn * wMax, cudaMemcpyDeviceToHost, s),
+              "theta");
+    cudaCheck(cudaMemcpyAsync(kk.data(), redK_.as<int32_t>(), sizeof(int32_t) * Pn, cudaMemcpyDeviceToHost, s), "k");
     cudaCheck(cudaStreamSynchronize(s), "reduced");
-    P.theta.resize(static_cast<size_t>(want));
-    for (int j = 0; j < want; ++j) P.theta[static_cast<size_t>(j)] = 1.0 / nu[static_cast<size_t>(j)];
-    const double pp = static_cast<double>(p);
-    catF_[4] += 4.0 / 3.0 * pp * pp * pp;
-    catB_[4] += 8.0 / 3.0 * pp * pp * pp;
-    catF_[5] += 60.0 * 6.0 * pp * want;
-    catF_[6] += 4.0 * 12.0 * pp * want;
-    catB_[6] += 8.0 * 6.0 * pp * want;
-    catF_[7] += 4.0 * pp * pp * want;
-    catB_[7] += 8.0 * (pp * pp / 2.0 + 2.0 * pp * want);
-    work_[4] += 4.0 / 3.0 * pp * pp * pp + 4.0 * pp * pp * want;
-    work_[5] += 8.0 * pp * pp * pp / 3.0;
-    return want;
+    P.theta.assign(static_cast<size_t>(Pn), {});
+    P.got.assign(static_cast<size_t>(Pn), 0);
+    P.mMax = 0;
+    for (int q = 0; q < Pn; ++q) {
+        const int g = std::min<int>(kk[static_cast<size_t>(q)], want[static_cast<size_t>(q)]);
+        P.got[static_cast<size_t>(q)] = g;
+        P.mMax = std::max(P.mMax, g);
+        auto& th = P.theta[static_cast<size_t>(q)];
+        th.resize(static_cast<size_t>(g));
+        for (int j = 0; j < g; ++j) th[static_cast<size_t>(j)] = 1.0 / nu[static_cast<size_t>(q * wMax + j)];
+        const double pp = static_cast<double>(P.pp[static_cast<size_t>(q)]);
+        catF_[4] += 4.0 / 3.0 * pp * pp * pp;
+        catB_[4] += 8.0 / 3.0 * pp * pp * pp;
+        catF_[5] += 60.0 * 6.0 * pp * g;
+        catF_[6] += 4.0 * 12.0 * pp * g;
+        catB_[6] += 8.0 * 6.0 * pp * g;
+        catF_[7] += 4.0 * pp * pp * g;
+        catB_[7] += 8.0 * (pp * pp / 2.0 + 2.0 * pp * g);
+        work_[4] += 4.0 / 3.0 * pp * pp * pp + 4.0 * pp * pp * g;
+        work_[5] += 8.0 * pp * pp * pp / 3.0;
+    }
 }
 
 void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
     const int N = static_cast<int>(nodes_.size());
+    const int Pn = nPencils_;
     ztPool_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
-    sqrtTheta_.ensure(sizeof(double) * static_cast<size_t>(m));
-    std::vector<double> st(static_cast<size_t>(m));
-    for (int j = 0; j < m; ++j) st[static_cast<size_t>(j)] = std::sqrt(P.theta[static_cast<size_t>(j)]);
-    cudaCheck(cudaMemcpyAsync(sqrtTheta_.as<double>(), st.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s), "sqrt theta");
+    sqrtTheta_.ensure(sizeof(double) * static_cast<size_t>(m * Pn));
+    std::vector<double> st(static_cast<size_t>(m * Pn), 0.0);       // per pencil, zero beyond its count
+    for (int q = 0; q < Pn; ++q)
+        for (int j = 0; j < std::min<int>(m, P.got[static_cast<size_t>(q)]); ++j)
+            st[static_cast<size_t>(q * m + j)] = std::sqrt(P.theta[static_cast<size_t>(q)][static_cast<size_t>(j)]);
+    cudaCheck(cudaMemcpyAsync(sqrtTheta_.as<double>(), st.data(), sizeof(double) * m * Pn, cudaMemcpyHostToDevice, s),
+              "sqrt theta");
     double* zt = ztPool_.as<double>();
     // u_i = (y v_i D_theta)^T - z_S L_Si, then z_i = u_i L_ii^-1 (transposed
     // layout, m x n_i blocks); u lives in a second buffer of the same layout
@@ -1161,9 +1332,12 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
             if (ni == 0) continue;
             double* zi = zt + nd.off * m;
             double* ui = ut + nd.off * m;
-            GemmDesc a = gemm(m, ni, ki, kTransA | kTransB | kRowScale, V + P.projOff[static_cast<size_t>(i)], P.p,
-                              Y + yOff_[static_cast<size_t>(i)], std::max<int64_t>(ni, 1), ui, m, 1.0, 0.0);
-            a.rowScale = sqrtTheta_.as<double>();
+            const int pc = pencilOf_[static_cast<size_t>(i)];
+            GemmDesc a = gemm(m, ni, ki, kTransA | kTransB | kRowScale,
+                              V + P.vOff[static_cast<size_t>(pc)] + P.localOff[static_cast<size_t>(i)],
+                              P.pp[static_cast<size_t>(pc)], Y + yOff_[static_cast<size_t>(i)],
+                              std::max<int64_t>(ni, 1), ui, m, 1.0, 0.0);
+            a.rowScale = sqrtTheta_.as<double>() + static_cast<int64_t>(pc) * m;
             gemmTiles(g1T, static_cast<int>(g1.size()), m, ni, mTile());
             g1.push_back(a);
             if (si > 0) {
@@ -1202,7 +1376,7 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
 // numeric solve
 // ---------------------------------------------------------------------------
 void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
-                         double* Z, bool outputsOnDevice, int64_t* pOut, double* timing) {
+                         double* Z, bool outputsOnDevice, int64_t* pOut, double* timing, int64_t* mOut) {
     if (!analyzed_) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_solve_values before amls_analyze");
     cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
     if (opt_.nev <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
@@ -1242,79 +1416,125 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     LAUNCH(launchScatterAdd(mVal_.as<double>(), supDst_.as<int64_t>(), nnzM_, 1.0, supVal_.as<double>(), s));
     eliminate(s);
     checkStatus("elimination");
+    silPrepare(s);
     const auto t2 = Clock::now();
     double tRed = 0;
     Pass P;
-    const int N = static_cast<int>(nodes_.size());
+    const int Pn = nPencils_;
+    std::vector<int> nevP(static_cast<size_t>(Pn));
+    for (int q = 0; q < Pn; ++q)
+        nevP[static_cast<size_t>(q)] = static_cast<int>(std::min<int64_t>(opt_.nev, pOff_[q + 1] - pOff_[q]));
+    const std::vector<double> zeroP(static_cast<size_t>(Pn), 0.0);
     if (opt_.fixedKeep > 0) {
-        condense(0, static_cast<int>(opt_.fixedKeep), 0.0, P, s);
+        condense(0, std::vector<int>(static_cast<size_t>(Pn), static_cast<int>(opt_.fixedKeep)), zeroP, zeroP, P, s);
         pA_ = P.p;
     } else {
         if (!opt_.twoPass)
             throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "twoPass=false with fixedKeep=0 cannot set the cut");
-        const int64_t k0 = std::max<int64_t>(4, (3 * nev + N - 1) / N);
+        // pass A: k0 = max(4, ceil(3 nev / N)) per pencil (solver.cpp:246-248)
+        std::vector<int> k0(static_cast<size_t>(Pn));
+        for (int q = 0; q < Pn; ++q) {
+            const int64_t Nq = pNodes_[static_cast<size_t>(q)];
+            k0[static_cast<size_t>(q)] = static_cast<int>(std::max<int64_t>(4, (3 * nevP[static_cast<size_t>(q)] + Nq - 1) / Nq));
+        }
         Pass A;
-        condense(0, static_cast<int>(k0), 0.0, A, s);
+        condense(0, k0, zeroP, zeroP, A, s);
         pA_ = A.p;
         const auto ta = Clock::now();
-        const int got = reducedSolve(A, static_cast<int>(std::min<int64_t>(nev, A.p)), s, false);
+        std::vector<int> wA(static_cast<size_t>(Pn));
+        for (int q = 0; q < Pn; ++q)
+            wA[static_cast<size_t>(q)] = static_cast<int>(std::min<int64_t>(nevP[static_cast<size_t>(q)], A.pp[static_cast<size_t>(q)]));
+        reducedSolve(A, wA, s, false);
         tRed += secs(ta, Clock::now());
-        if (got < nev)
-            throw AmlsError(AMLS_ERR_NUMERIC, "pass A reduced problem too small (p < nev); reduce nLevels or grow leafSize");
-        const double lambdaHat = A.theta[static_cast<size_t>(nev - 1)];
-        const double lambdaCut = opt_.thresholdFactor * lambdaHat;
-        if (opt_.verbosity > 0)
-            std::fprintf(stderr, "[amls_b200] pass A: p0=%lld lambda_hat=%.10g lambda_cut=%.10g\n",
-                         static_cast<long long>(A.p), lambdaHat, lambdaCut);
-        // keep mu <= lambda_cut  <=>  nu >= 1 / lambda_cut (all local mu > 0)
-        const double thr = lambdaCut > 0 ? 1.0 / lambdaCut : 1e300;
-        condense(1, 0, thr, P, s);
+        // lambda_cut = eta * lambda_hat per pencil (:252-258)
+        std::vector<double> thr(static_cast<size_t>(Pn)), hi(static_cast<size_t>(Pn));
+        for (int q = 0; q < Pn; ++q) {
+            const int nq = nevP[static_cast<size_t>(q)];
+            if (A.got[static_cast<size_t>(q)] < nq)
+                throw AmlsError(AMLS_ERR_NUMERIC, "pass A reduced problem too small (p < nev); reduce nLevels or grow leafSize");
+            const double lambdaHat = A.theta[static_cast<size_t>(q)][static_cast<size_t>(nq - 1)];
+            const double lambdaCut = opt_.thresholdFactor * lambdaHat;
+            if (opt_.verbosity > 0 && Pn == 1)
+                std::fprintf(stderr, "[amls_b200] pass A: p0=%lld lambda_hat=%.10g lambda_cut=%.10g\n",
+                             static_cast<long long>(A.p), lambdaHat, lambdaCut);
+            // keep mu <= lambda_cut  <=>  nu >= 1 / lambda_cut (all local mu > 0)
+            thr[static_cast<size_t>(q)] = lambdaCut > 0 ? 1.0 / lambdaCut : 1e300;
+            hi[static_cast<size_t>(q)] = lambdaCut;
+        }
+        condense(1, std::vector<int>(static_cast<size_t>(Pn), 0), thr, hi, P, s);
     }
     const auto t3 = Clock::now();
     pFinal_ = P.p;
-    if (P.p > opt_.denseProjectedMax && opt_.verbosity > 0)
-        std::fprintf(stderr, "[amls_b200] warning: p=%lld exceeds denseProjectedMax=%lld (dense solve used)\n",
-                     static_cast<long long>(P.p), static_cast<long long>(opt_.denseProjectedMax));
-    int64_t nq = std::min<int64_t>(nev, P.p);
+    for (int q = 0; q < Pn; ++q)
+        if (P.pp[static_cast<size_t>(q)] > opt_.denseProjectedMax && opt_.verbosity > 0)
+            std::fprintf(stderr, "[amls_b200] warning: p=%lld exceeds denseProjectedMax=%lld (dense solve used)\n",
+                         static_cast<long long>(P.pp[static_cast<size_t>(q)]),
+                         static_cast<long long>(opt_.denseProjectedMax));
+    std::vector<int> nq(static_cast<size_t>(Pn));
+    for (int q = 0; q < Pn; ++q)
+        nq[static_cast<size_t>(q)] = static_cast<int>(std::min<int64_t>(nevP[static_cast<size_t>(q)], P.pp[static_cast<size_t>(q)]));
     if (opt_.refine) {
+        if (Pn > 1) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "refinement is available for a single pencil only");
         const int64_t extra = opt_.refineExtra >= 0 ? opt_.refineExtra : nev / 2 + 16;
-        nq = std::min<int64_t>(P.p, std::min<int64_t>(n_, nev + extra));
+        nq[0] = static_cast<int>(std::min<int64_t>(P.p, std::min<int64_t>(n_, nev + extra)));
     }
-    const int got = reducedSolve(P, static_cast<int>(nq), s);
-    const int want = static_cast<int>(std::min<int64_t>(nev, got));
+    reducedSolve(P, nq, s);
+    std::vector<int> want(static_cast<size_t>(Pn));
+    for (int q = 0; q < Pn; ++q)
+        want[static_cast<size_t>(q)] = std::min(nevP[static_cast<size_t>(q)], P.got[static_cast<size_t>(q)]);
     const auto t4 = Clock::now();
     tRed += secs(t3, t4);
     const bool recover = opt_.recoverVectors && Z != nullptr;
     refineIters_ = 0;
     refineNq_ = 0;
+    int mZ = 0;                        // columns of zOut_
     if (opt_.refine) {
+        const int got = P.got[0];
         backtransform(P, got, s);
         refineNq_ = got;
-        refineIters_ = refine(ztPool_.as<double>(), got, want, P.theta, recover, s);
-        P.theta.resize(static_cast<size_t>(want));
-        if (recover) finalizeVectors(ztPool_.as<double>(), got, want, s);
+        refineIters_ = refine(ztPool_.as<double>(), got, want[0], P.theta[0], recover, s);
+        P.theta[0].resize(static_cast<size_t>(want[0]));
+        if (recover) finalizeVectors(ztPool_.as<double>(), got, want[0], s);
+        mZ = want[0];
     } else if (recover) {
-        backtransform(P, want, s);
-        finalizeVectors(ztPool_.as<double>(), want, want, s);
+        mZ = P.mMax;
+        backtransform(P, mZ, s);
+        finalizeVectors(ztPool_.as<double>(), mZ, mZ, s);
     }
-    P.theta.resize(static_cast<size_t>(want));
+    for (int q = 0; q < Pn; ++q) P.theta[static_cast<size_t>(q)].resize(static_cast<size_t>(want[static_cast<size_t>(q)]));
     const auto t5 = Clock::now();
-    // outputs
-    if (outputsOnDevice) {
-        cudaCheck(cudaMemcpyAsync(theta, P.theta.data(), sizeof(double) * want, cudaMemcpyHostToDevice, s), "theta");
-        if (recover)
-            cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * want * n_, cudaMemcpyDeviceToDevice, s), "Z");
-    } else {
-        std::copy(P.theta.begin(), P.theta.end(), theta);
-        if (recover)
-            cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * want * n_, cudaMemcpyDeviceToHost, s), "Z");
+    // outputs: pencil q's values at theta + q * nev (one pencil: theta[0 ..
+    // want)); Z is n x nev column-major, pencil q in its own rows, columns
+    // beyond its count zero
+    const int64_t zCols = Pn == 1 ? want[0] : nev;
+    std::vector<double> th(static_cast<size_t>(Pn == 1 ? std::max(want[0], 1) : Pn * nev), 0.0);
+    for (int q = 0; q < Pn; ++q)
+        std::copy(P.theta[static_cast<size_t>(q)].begin(), P.theta[static_cast<size_t>(q)].end(),
+                  th.begin() + static_cast<int64_t>(q) * (Pn == 1 ? 0 : nev));
+    const int64_t thN = Pn == 1 ? want[0] : Pn * nev;
+    if (mOut)
+        for (int q = 0; q < Pn; ++q) mOut[q] = want[static_cast<size_t>(q)];
+    const cudaMemcpyKind zk = outputsOnDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (outputsOnDevice)
+        cudaCheck(cudaMemcpyAsync(theta, th.data(), sizeof(double) * thN, cudaMemcpyHostToDevice, s), "theta");
+    else
+        std::copy(th.begin(), th.begin() + thN, theta);
+    if (recover) {
+        const int64_t mc = std::min<int64_t>(mZ, zCols);
+        if (mc > 0) cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * mc * n_, zk, s), "Z");
+        if (zCols > mc) {
+            if (outputsOnDevice)
+                cudaCheck(cudaMemsetAsync(Z + mc * n_, 0, sizeof(double) * (zCols - mc) * n_, s), "Z");
+            else
+                std::fill(Z + mc * n_, Z + zCols * n_, 0.0);
+        }
     }
     cudaCheck(cudaEventRecord(evSolve1_, s), "cudaEventRecord");
     cudaCheck(cudaStreamSynchronize(s), "outputs");
     const auto t6 = Clock::now();
     profCollect();
-    lastTheta_ = P.theta;
-    lastHasVectors_ = recover;
+    lastTheta_ = P.theta[0];
+    lastHasVectors_ = recover && Pn == 1;
     if (pOut) *pOut = P.p;
     if (timing) {
         timing[AMLS_T_UPLOAD] = secs(t0, t1);
@@ -1563,11 +1783,12 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, int32_t
 
 
 void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
-    norms_.ensure(sizeof(double) * static_cast<size_t>(m));
+    norms_.ensure(sizeof(double) * static_cast<size_t>(m) * nPencils_);
     zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));
     LAUNCH(launchMNormSuper(supDesc_.as<SpmmSuper>(), nSup_, supCols_.as<int32_t>(), supVal_.as<double>(),
-                            invDev_.as<int64_t>(), zt, m, ldz, norms_.as<double>(), s));
-    LAUNCH(launchUnpermute(zt, ldz, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s));
+                            invDev_.as<int64_t>(), zt, m, ldz, norms_.as<double>(), nPencils_, s));
+    LAUNCH(launchUnpermute(zt, ldz, m, n_, permDev_.as<int64_t>(), norms_.as<double>(), zOut_.as<double>(), s,
+                           nPencils_ > 1 ? pencilDev_.as<int32_t>() : nullptr));
     cudaCheck(cudaStreamSynchronize(s), "finalize");
 }
 
@@ -1585,6 +1806,8 @@ void Engine::info(int64_t* out) const {
     out[7] = refineIters_;
     out[8] = refineNq_;
     out[9] = n_;
+    out[10] = static_cast<int64_t>(sil_.size());
+    out[11] = silServed_;
 }
 
 void Engine::permutation(int64_t* out) const {

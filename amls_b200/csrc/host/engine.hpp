@@ -43,8 +43,16 @@ public:
 
     void analyze(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
                  const int32_t* mc, const amls_options& opt);
+    // P independent pencils as one block-diagonal CSR (pencil b: rows and
+    // columns pOff[b] .. pOff[b+1]), each partitioned on its own
+    void analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const int32_t* kc,
+                      const int64_t* mp, const int32_t* mc, const amls_options& opt);
+    int pencils() const { return nPencils_; }
+    // theta: one pencil theta[nev]; a batch theta[q * nev + j] with
+    // mOut[q] values per pencil.  Z: n x (nev or fewer for one pencil).
     void solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
-                     double* Z, bool outputsOnDevice, int64_t* pOut, double* timing);
+                     double* Z, bool outputsOnDevice, int64_t* pOut, double* timing,
+                     int64_t* mOut = nullptr);
     // dense batched generalized eigensolver (amls_sygvx_batched)
     void sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, const double* K,
                       const double* M, int mode, int64_t il, int64_t iu, double lo, double hi,
@@ -90,9 +98,16 @@ private:
     // pass-dependent state
     struct Pass {
         std::vector<int32_t> k;      // kept modes per node
-        std::vector<int64_t> projOff;
-        int64_t p = 0;
-        std::vector<double> theta;   // host copy of reduced eigenvalues (ascending)
+        std::vector<int64_t> projOff;   // first mode of each node over all pencils (node-id order)
+        std::vector<int64_t> localOff;  // first mode of each node in its pencil's reduced problem
+        std::vector<int64_t> pp;        // reduced size per pencil
+        std::vector<int64_t> credOff;   // per pencil: doubles into credPool_ (pp x pp, ld pp)
+        int64_t credTotal = 0;
+        int64_t p = 0;                  // modes over all pencils
+        std::vector<std::vector<double>> theta;   // per pencil: reduced eigenvalues ascending
+        std::vector<int> got;           // per pencil: eigenpairs of the last reduced solve
+        std::vector<int64_t> vOff;      // per pencil: its eigenvectors at redY_ + vOff (ld pp)
+        int mMax = 0;                   // largest got
     };
 
     void buildStatic();
@@ -101,8 +116,13 @@ private:
     void dropGraphs();
     void tridiagonalizeAll(cudaStream_t s);
     void tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, DevBuf& blob, cudaStream_t s);
-    void condense(int mode, int want, double thr, Pass& P, cudaStream_t s);
-    int reducedSolve(Pass& P, int want, cudaStream_t s, bool vectors = true);
+    // per pencil b: mode 0 index [1, wantP[b]]; mode 1 interval nu >= thrP[b]
+    // (mu <= hiP[b] = 1 / thrP[b])
+    void condense(int mode, const std::vector<int>& wantP, const std::vector<double>& thrP,
+                  const std::vector<double>& hiP, Pass& P, cudaStream_t s);
+    // per pencil the largest wantP[b] eigenpairs of its reduced matrix: fills
+    // P.theta, P.got, P.vOff, P.mMax
+    void reducedSolve(Pass& P, const std::vector<int>& wantP, cudaStream_t s, bool vectors = true);
     // z^T (m x n, permuted order) into ztPool_
     void backtransform(const Pass& P, int m, cudaStream_t s);
     // M-normalise the first m rows of zt (ld ldz) and un-permute into zOut_
@@ -131,8 +151,14 @@ private:
     bool analyzed_ = false;
     amls_options opt_{};
 
-    // problem
+    // problem (a batch of nPencils_ independent pencils as one block-diagonal
+    // pencil; one pencil for amls_solve)
     int64_t n_ = 0, nnzK_ = 0, nnzM_ = 0;
+    int nPencils_ = 1;
+    std::vector<int64_t> pOff_;                    // DOF offsets of the pencils (P + 1)
+    std::vector<int> pencilOf_;                    // node -> pencil
+    std::vector<int> pNodes_;                      // tree nodes per pencil
+    DevBuf pencilDev_;                             // pencil of each permuted DOF (batches)
     std::vector<int64_t> perm_, inv_;
     std::vector<Node> nodes_;
     std::vector<int> order_;                       // post-order
@@ -192,6 +218,48 @@ private:
 
     // eigen
     bool tridiagDone_ = false;
+
+    // ---- shift-invert Lanczos nodes (the reference's SIL, sil.cpp) ----
+    struct SilNode {
+        int node = -1;
+        int64_t mat = 0;                           // doubles into the n^2 pools
+        int64_t vec = 0;                           // doubles into silVec_ (5 n)
+        int64_t inv = 0;                           // doubles into silInv_
+        int64_t csr = 0;                           // row pointers of M^_ii in silMRow_ (n + 1, node-relative)
+        int64_t ent = 0;                           // first entry in silMCol_ / silMOff_
+    };
+    struct SilLevelCopy {
+        size_t desc = 0, tiles = 0;
+        int nTiles = 0;
+    };
+    void silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc);
+    void silBuildStatic();                         // tables into sblob_ (before its upload)
+    void silPrepare(cudaStream_t s);               // per solve: sigma, factor, (K^ - sigma M^)^-1
+    // Lanczos runs and Ritz selection of one pass (mode 0 index [1, want],
+    // mode 1 interval (-inf, hi]): kSel[node] = kept pairs, -1 = dense solver
+    void silSelect(int mode, const std::vector<int>& wantP, const std::vector<double>& hiP,
+                   std::vector<int>& kSel, cudaStream_t s);
+    // Ritz vectors of the selected pairs into the engine's local form (Y, nu,
+    // C Y) at the pass's offsets
+    void silVectors(const std::vector<int>& kSel, const std::vector<int64_t>& projOff, cudaStream_t s);
+    std::vector<SilNode> sil_;
+    std::vector<int> silOf_;                       // node -> index into sil_ (-1)
+    std::vector<int32_t> silMRowH_, silMColH_;
+    std::vector<int64_t> silMOffH_;
+    int64_t silMatTotal_ = 0, silVecTotal_ = 0, silInvTotal_ = 0;
+    DevBuf silA_, silL_, silLinv_, silScratch_, silInv_, silB_, silQ_, silMQ_, silQT_, silVec_;
+    DevBuf silState_, silSigma_, silMRow_, silMCol_, silMOff_, silRunBlob_, silThr_;
+    DevBuf silS_, silX_, silP_, silYt_, silCY_, silNu_, silRs_, silWork_, silKOut_, silEigBlob_;
+    CholPlan silChol_;
+    GemmBatch silBGemm_;
+    size_t silShiftDesc_ = 0, silLowerDesc_ = 0, silLowerTiles_ = 0;
+    int silLowerNTiles_ = 0;
+    std::vector<SilLevelCopy> silCopy_;            // per level: K^_ii before the in-place Cholesky
+    std::vector<const double*> silCYPtr_;          // per node: C_i Y_i of the pass (SIL nodes)
+    // per SIL node after silSelect: Lanczos steps and T eigen offsets of the pass
+    std::vector<int> silM_;
+    std::vector<int64_t> silSOff_, silNuOff_;
+    int64_t silServed_ = 0;                        // nodes served by shift-invert Lanczos in the last pass
 
     // per-pass device buffers
     DevBuf yPool_, wPool_, kOutDev_, iiWork_, panelPool_, wtPool_, credPool_;

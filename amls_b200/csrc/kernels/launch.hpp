@@ -159,11 +159,12 @@ cudaError_t launchTridiagLargeGroups(const EigDesc* dDescs, const int* dGroupOf,
 // Co-resident CTA count for the cooperative kernel at a given maxN.
 int tridiagLargeMaxCtas(int maxN);
 // Select eigenvalues of T: mode 0 = the k largest (k = want), mode 1 = all
-// >= thr; mode 2 = the k smallest, mode 3 = all <= thr.  Bisection.
-// Selected values are written in "wanted" order (largest first for modes
-// 0/1, smallest first for modes 2/3).
+// >= thr (thrArr[b] per descriptor when given); mode 2 = the k smallest,
+// mode 3 = all <= thr; each count capped by the descriptor's kcap.
+// Bisection.  Selected values are written in "wanted" order (largest first
+// for modes 0/1, smallest first for modes 2/3).
 cudaError_t launchBisect(const EigDesc* d, int nDesc, int mode, int want, double thr,
-                         int maxN, int* status, cudaStream_t s);
+                         int maxN, int* status, cudaStream_t s, const double* thrArr = nullptr);
 // Inverse iteration for the selected eigenvalues (clusters reorthogonalised).
 cudaError_t launchInverseIter(const EigDesc* d, int nDesc, int maxK, int* status,
                               cudaStream_t s);
@@ -185,7 +186,62 @@ cudaError_t launchZeroUpper(const EigDesc* d, int nDesc, cudaStream_t s);
 cudaError_t launchWyT(const WyBlock* blocks, int nBlocks, cudaStream_t s);
 // Bisection with one warp per eigenvalue (32-point multisection per round).
 cudaError_t launchBisectWarp(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
-                             cudaStream_t s);
+                             cudaStream_t s, const double* thrArr = nullptr);
+
+// Count of the eigenvalues of T >= thr[b] per descriptor (Sturm counts),
+// written to kOut (capped by kcap); thr[b] = +inf counts none.
+cudaError_t launchCountAbove(const EigDesc* d, int nDesc, const double* thr, cudaStream_t s);
+
+// ------------------------------------------- shift-invert Lanczos (sil.cu) --
+// Copy of a front's diagonal block: mode 0 the full symmetric matrix from
+// its lower triangle, mode 1 the lower triangle with zeros above.
+struct SilCopyDesc {
+    const double* src;     // front diagonal block, ld
+    int64_t ld;
+    double* dst;           // n x n, ld n
+    int32_t n, mode;
+};
+cudaError_t launchSilSymCopy(const SilCopyDesc* d, const TileRef* tiles, int nTiles, cudaStream_t s);
+// sigma = -max(1e-10, 1e-9 max_j |A_jj|), then A <- A - sigma M (M: lower
+// triangle of the M front's diagonal block, ld ldm).  One CTA per node.
+struct SilShiftDesc {
+    double* A;             // n x n, K^_ii on entry
+    const double* M;
+    int64_t ldm;
+    double* sigma;
+    int32_t n, pad;
+};
+cudaError_t launchSilShift(const SilShiftDesc* d, int nDesc, cudaStream_t s);
+// Lanczos state of one node (all n x n arrays ld n).
+struct SilDesc {
+    int32_t n, target, active, pad;
+    int32_t* state;        // [0] steps done, [1] stopped (breakdown or full)
+    const double* B;       // (K^ - sigma M^)^-1
+    double* Q;             // basis q_l (columns)
+    double* MQ;            // M^ q_l
+    double* QT;            // Q^T
+    double* w;
+    double* mw;
+    double* coef;
+    double* alpha;         // T diagonal
+    double* beta;          // T off-diagonal (beta[j] couples j, j+1)
+    const int32_t* mRow;   // local CSR of M^_ii (n + 1)
+    const int32_t* mCol;
+    const int64_t* mOff;   // value offsets into mBase (lower triangle)
+    const double* mBase;
+};
+cudaError_t launchSilLanczos(const SilDesc* d, int nDesc, int maxSteps, cudaStream_t s);
+// thr[b] = 1 / (hi[b] - sigma[b]) (+inf when hi[b] <= sigma[b])
+cudaError_t launchSilThreshold(const double* sigma, int nDesc, const double* hi, double* thr, cudaStream_t s);
+// lambda_t = 1/nu_t + sigma; rs[t] = lambda_t^-1/2, wEng[t] = 1/lambda_t (t < *kOut)
+struct SilRitzDesc {
+    const int32_t* kOut;
+    const double* nu;
+    const double* sigma;
+    double* rs;
+    double* wEng;
+};
+cudaError_t launchSilRitzScale(const SilRitzDesc* d, int nDesc, cudaStream_t s);
 
 // --------------------------------------------------------------- misc ---
 // Zero a list of (pointer, count) ranges.
@@ -212,9 +268,11 @@ struct CopyDesc {
 };
 cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int nTiles,
                                    cudaStream_t s);
-// Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]), j < m.
+// Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[q * m + j]), j < m, with q
+// = pencil[d] (permuted row d; null: one pencil).
 cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
-                            const double* norms, double* Z, cudaStream_t s);
+                            const double* norms, double* Z, cudaStream_t s,
+                            const int32_t* pencil = nullptr);
 // Products with M in the transposed layout over super-rows (see misc.cu):
 // rows row0 .. row0 + rows - 1 (original order, rows <= kSpmmSuperRows) with
 // the union column pattern ucols[colOff .. colOff + len) and the dense block
@@ -223,6 +281,7 @@ constexpr int kSpmmSuperRows = 12;
 struct SpmmSuper {
     int64_t row0, colOff, valOff;
     int32_t rows, len;
+    int32_t pencil, pad;   // pencil of the rows (batches of independent pencils)
 };
 // Rt[j + inv[o]*ld] = sum_c M[o, c] Qt[j + inv[c]*ld] for j < m <= ld (also
 // into Rt2 when given).
@@ -230,10 +289,12 @@ cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* 
                              const int64_t* inv, const double* Qt, int m, int64_t ld, double* Rt,
                              cudaStream_t s, double* Rt2 = nullptr);
 // M-norms of the columns of X held transposed in permuted order:
-// norms[j] = x_j^T M x_j with x[o, j] = zt[j + inv[o]*ld], j < m <= ld.
+// norms[q * m + j] = x_j^T M_q x_j over the rows of pencil q (the super-row's
+// pencil), x[o, j] = zt[j + inv[o]*ld], j < m <= ld; norms holds
+// pencils * m doubles.
 cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
                              const int64_t* inv, const double* zt, int m, int64_t ld, double* norms,
-                             cudaStream_t s);
+                             int pencils, cudaStream_t s);
 // Per-element eigenvalue sensitivities of the M-normalised eigenvectors X
 // (n x nmodes, original order): see sensitivity.cu.  elemType[e] (null: all
 // 0) selects element e's matrices Kbar/Mbar + type * nd * nd.  weight[k] NaN

@@ -132,7 +132,7 @@ cudaError_t launchTransposeBatched(const CopyDesc* d, const TileRef* tiles, int 
 // Z[perm[d] + j*n] = zt[j + d*ldz] / sqrt(norms[j]); 32 x 32 tiles (d, j).
 __global__ void unpermuteKernel(const double* __restrict__ zt, int64_t ldz, int m, int64_t n,
                                 const int64_t* __restrict__ perm, const double* __restrict__ norms,
-                                double* __restrict__ Z) {
+                                double* __restrict__ Z, const int32_t* __restrict__ pencil) {
     __shared__ double t[32][33];
     const int64_t d0 = (int64_t)blockIdx.x * 32;
     const int j0 = blockIdx.y * 32;
@@ -147,17 +147,19 @@ __global__ void unpermuteKernel(const double* __restrict__ zt, int64_t ldz, int 
         const int j = j0 + r;
         const int64_t d = d0 + tx;
         if (d < n && j < m) {
-            const double s = 1.0 / sqrt(fmax(norms[j], 1e-300));
+            const double nj = norms[(pencil ? (int64_t)pencil[d] * m : 0) + j];
+            // a pencil with fewer eigenpairs than m has zero columns there
+            const double s = nj > 0.0 ? 1.0 / sqrt(nj) : 0.0;
             Z[perm[d] + (int64_t)j * n] = t[tx][r] * s;
         }
     }
 }
 
 cudaError_t launchUnpermute(const double* zt, int64_t ldz, int m, int64_t n, const int64_t* perm,
-                            const double* norms, double* Z, cudaStream_t s) {
+                            const double* norms, double* Z, cudaStream_t s, const int32_t* pencil) {
     if (n <= 0 || m <= 0) return cudaSuccess;
     dim3 grid((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));
-    unpermuteKernel<<<grid, 256, 0, s>>>(zt, ldz, m, n, perm, norms, Z);
+    unpermuteKernel<<<grid, 256, 0, s>>>(zt, ldz, m, n, perm, norms, Z, pencil);
     return cudaGetLastError();
 }
 
@@ -267,13 +269,25 @@ __global__ void __launch_bounds__(kSpmmThreads) mnormSuperKernel(const SpmmSuper
     double dot[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) dot[u] = 0.0;
-    for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x)
-        superRow<U, true>(sup[g], ucols, vals, inv, zt, m, ld, j0, nullptr, nullptr, dot, sv, sc);
+    int cur = -1;                       // pencil of the sums in dot[]
+    auto flush = [&]() {
+        if (cur < 0) return;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int j = j0 + threadIdx.x + kSpmmThreads * u;
-        if (j < m) atomicAdd(norms + j, dot[u]);
+        for (int u = 0; u < U; ++u) {
+            const int j = j0 + threadIdx.x + kSpmmThreads * u;
+            if (j < m) atomicAdd(norms + (int64_t)cur * m + j, dot[u]);
+            dot[u] = 0.0;
+        }
+    };
+    for (int64_t g = blockIdx.x; g < nsup; g += gridDim.x) {
+        const int pc = sup[g].pencil;   // uniform over the CTA
+        if (pc != cur) {
+            flush();
+            cur = pc;
+        }
+        superRow<U, true>(sup[g], ucols, vals, inv, zt, m, ld, j0, nullptr, nullptr, dot, sv, sc);
     }
+    flush();
 }
 
 namespace {
@@ -300,8 +314,8 @@ cudaError_t launchSpmmSuperT(const SpmmSuper* sup, int64_t nsup, const int32_t* 
 
 cudaError_t launchMNormSuper(const SpmmSuper* sup, int64_t nsup, const int32_t* ucols, const double* vals,
                              const int64_t* inv, const double* zt, int m, int64_t ld, double* norms,
-                             cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * (size_t)(m > 0 ? m : 0), s);
+                             int pencils, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * (size_t)(m > 0 ? m : 0) * (size_t)pencils, s);
     if (e != cudaSuccess || nsup <= 0 || m <= 0) return e;
     const int u = spmmU(m);
     const dim3 grid(gridFor(nsup * kSpmmThreads, kSpmmThreads), (m + kSpmmThreads * u - 1) / (kSpmmThreads * u));

@@ -495,7 +495,7 @@ __device__ void gershgorin(const double* d, const double* e, int n, double& lo, 
 
 // count kernel: kOut[b] for modes 0/2 (min(want, n, kcap)) and 1/3 (threshold)
 __global__ void bisectCountKernel(const EigDesc* __restrict__ descs, int nDesc, int mode, int want,
-                                  double thr) {
+                                  double thr, const double* __restrict__ thrArr) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nDesc) return;
     const EigDesc D = descs[b];
@@ -506,7 +506,7 @@ __global__ void bisectCountKernel(const EigDesc* __restrict__ descs, int nDesc, 
     else {
         double lo, hi, pivmin, tn;
         gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
-        const int less = sturmLess(D.d, D.e, n, thr, pivmin, tn);
+        const int less = sturmLess(D.d, D.e, n, thrArr ? thrArr[b] : thr, pivmin, tn);
         k = (mode == 1) ? (n - less) : less;
     }
     *D.kOut = min(k, D.kcap);
@@ -536,13 +536,36 @@ __global__ void bisectKernel(const EigDesc* __restrict__ descs, int mode, int ma
 }
 
 cudaError_t launchBisect(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
-                         int*, cudaStream_t s) {
+                         int*, cudaStream_t s, const double* thrArr) {
     if (nDesc <= 0) return cudaSuccess;
-    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr);
+    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr, thrArr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || maxK <= 0) return e;
     dim3 grid((maxK + 63) / 64, nDesc);
     bisectKernel<<<grid, 64, 0, s>>>(d, mode, maxK);
+    return cudaGetLastError();
+}
+
+// count of eigenvalues >= thr[b] (descriptor b), capped by kcap
+__global__ void countAboveKernel(const EigDesc* __restrict__ descs, int nDesc,
+                                 const double* __restrict__ thr) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nDesc) return;
+    const EigDesc D = descs[b];
+    const int n = D.n;
+    const double x = thr[b];
+    int k = 0;
+    if (n > 0 && x < INFINITY) {
+        double lo, hi, pivmin, tn;
+        gershgorin(D.d, D.e, n, lo, hi, pivmin, tn);
+        k = n - sturmLess(D.d, D.e, n, x, pivmin, tn);
+    }
+    *D.kOut = min(k, D.kcap);
+}
+
+cudaError_t launchCountAbove(const EigDesc* d, int nDesc, const double* thr, cudaStream_t s) {
+    if (nDesc <= 0) return cudaSuccess;
+    countAboveKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, thr);
     return cudaGetLastError();
 }
 
@@ -848,9 +871,9 @@ __global__ void __launch_bounds__(256) bisectWarpKernel(const EigDesc* __restric
 }
 
 cudaError_t launchBisectWarp(const EigDesc* d, int nDesc, int mode, int want, double thr, int maxK,
-                             cudaStream_t s) {
+                             cudaStream_t s, const double* thrArr) {
     if (nDesc <= 0) return cudaSuccess;
-    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr);
+    bisectCountKernel<<<(nDesc + 127) / 128, 128, 0, s>>>(d, nDesc, mode, want, thr, thrArr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || maxK <= 0) return e;
     dim3 grid((maxK + 7) / 8, nDesc);

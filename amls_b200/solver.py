@@ -40,6 +40,9 @@ class AmlsOptions:
     # "fp64" or "mixed" (M-side AMLS products on the BF16 tensor cores, split
     # operands; not in the reference)
     precision: str = "fp64"
+    # local eigensolver per node (EigenpairSolver::silMode): 0 automatic by
+    # sparsity, 1 shift-invert Lanczos everywhere, -1 dense everywhere
+    silMode: int = 0
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -62,6 +65,9 @@ class AmlsOptions:
         if self.precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', not {self.precision!r}")
         o.precision = 0 if self.precision == "fp64" else 1
+        if int(self.silMode) not in (-1, 0, 1):
+            raise ValueError("silMode must be -1, 0 or 1")
+        o.silMode = int(self.silMode)
         return o
 
 
@@ -139,6 +145,66 @@ class AmlsSolver:
         self._last_nev = nev
         return Solution(theta[:nev].copy(), None if Z is None else Z.T.copy(), int(p.value),
                         dict(zip(_lib.TIMING_KEYS, timing.tolist())), self.info())
+
+    # ---- batch of independent pencils (one launch sequence) ----
+    def solve_batch(self, Ks, Ms, opt: AmlsOptions):
+        """Each pencil (Ks[b], Ms[b]) solved as by ``solve`` (its own
+        partition and two-pass truncation), all of them level-batched on the
+        GPU.  Returns a list of Solution (theta, Z per pencil; p and timing of
+        the whole batch)."""
+        K = sp.block_diag([sp.csr_matrix(k) for k in Ks], format="csr")
+        M = sp.block_diag([sp.csr_matrix(m) for m in Ms], format="csr")
+        off = np.zeros(len(Ks) + 1, np.int64)
+        off[1:] = np.cumsum([k.shape[0] for k in Ks])
+        kp, kc, kv = _csr_arrays(K)
+        mp, mc, mv = _csr_arrays(M)
+        n = int(off[-1])
+        nev = max(1, min(int(opt.nev), n))
+        B = len(Ks)
+        theta = np.zeros(B * nev, np.float64)
+        m = np.zeros(B, np.int64)
+        Z = np.zeros((nev, n), np.float64) if opt.recoverVectors else None
+        timing = np.zeros(_lib.T_SLOTS, np.float64)
+        o = opt.to_c()
+        _lib.check(_lib.lib().amls_solve_batch(self._h, B, _lib.ptr(off), _lib.ptr(kp), _lib.ptr(kc),
+                                               _lib.ptr(kv), _lib.ptr(mp), _lib.ptr(mc), _lib.ptr(mv),
+                                               C.byref(o), _lib.ptr(theta), _lib.ptr(m), _lib.ptr(Z),
+                                               _lib.ptr(timing)))
+        info = self.info()
+        tim = dict(zip(_lib.TIMING_KEYS, timing.tolist()))
+        out = []
+        for b in range(B):
+            mb = int(m[b])
+            Zb = None if Z is None else Z[:mb, off[b]:off[b + 1]].T.copy()
+            out.append(Solution(theta[b * nev:b * nev + mb].copy(), Zb, -1, tim, info))
+        return out
+
+    def analyze_batch(self, Ks, Ms, opt: AmlsOptions):
+        """Pattern analysis of a batch; returns the block-diagonal (K, M) whose
+        .data arrays are the value order of solve_values_batch."""
+        K = sp.block_diag([sp.csr_matrix(k) for k in Ks], format="csr")
+        M = sp.block_diag([sp.csr_matrix(m) for m in Ms], format="csr")
+        K.sort_indices()
+        M.sort_indices()
+        off = np.zeros(len(Ks) + 1, np.int64)
+        off[1:] = np.cumsum([k.shape[0] for k in Ks])
+        kp, kc, _ = _csr_arrays(K)
+        mp, mc, _ = _csr_arrays(M)
+        o = opt.to_c()
+        _lib.check(_lib.lib().amls_analyze_batch(self._h, len(Ks), _lib.ptr(off), _lib.ptr(kp),
+                                                 _lib.ptr(kc), _lib.ptr(mp), _lib.ptr(mc), C.byref(o)))
+        self._batch_off = off
+        return K, M
+
+    def solve_values_batch(self, k_val_ptr: int, m_val_ptr: int, values_on_device: bool,
+                           theta_ptr: int, m_ptr: int, z_ptr: int | None,
+                           outputs_on_device: bool) -> dict:
+        timing = np.zeros(_lib.T_SLOTS, np.float64)
+        _lib.check(_lib.lib().amls_solve_values_batch(
+            self._h, C.c_void_p(k_val_ptr), C.c_void_p(m_val_ptr), 1 if values_on_device else 0,
+            C.c_void_p(theta_ptr), C.c_void_p(m_ptr), None if z_ptr is None else C.c_void_p(z_ptr),
+            1 if outputs_on_device else 0, _lib.ptr(timing)))
+        return dict(zip(_lib.TIMING_KEYS, timing.tolist()))
 
     # ---- split form: analysis once, numeric solves on resident values ----
     def analyze(self, K, M, opt: AmlsOptions) -> None:
@@ -221,7 +287,7 @@ class AmlsSolver:
         buf = np.zeros(_lib.INFO_SLOTS, np.int64)
         _lib.check(_lib.lib().amls_info(self._h, _lib.ptr(buf)))
         keys = ["tree_nodes", "levels", "p_passA", "p", "front_doubles", "device_bytes",
-                "launches", "refine_iters", "refine_nq", "n"]
+                "launches", "refine_iters", "refine_nq", "n", "sil_nodes", "sil_served"]
         return {k: int(v) for k, v in zip(keys, buf)}
 
     def permutation(self) -> np.ndarray:

@@ -75,6 +75,15 @@ typedef struct amls_options {
      * Schur updates, the eigensolvers and the refinement stay FP64, so the
      * refined eigenpairs reach the same accuracy. */
     int32_t precision;          /* 0    */
+    /* Local eigensolver choice per node, the reference's
+     * EigenpairSolver::silMode (src/amls/eigenpair_solver.hpp:28-29, 68-82):
+     * 0 = automatic (shift-invert Lanczos when nnz(K^_ii) < 0.15 n_i^2 and
+     * n_i >= 200, the nonzeros counted from the sparsity structure after
+     * fill), 1 = shift-invert Lanczos for every node, -1 = dense for every
+     * node.  Index requests with k >= 4 n_i / 5 and Lanczos runs that return
+     * fewer pairs than asked (index) or none (interval) fall back to the
+     * dense solver, as in the reference (:38-63). */
+    int32_t silMode;            /* 0    */
 } amls_options;
 
 #define AMLS_PRECISION_FP64 0
@@ -148,12 +157,45 @@ int amls_solve_values(amls_handle h, const double* k_val, const double* m_val,
                       int32_t values_on_device, double* theta, double* Z,
                       int32_t outputs_on_device, int64_t* p_out, double* timing);
 
+/* Batch of independent pencils in one launch sequence (no counterpart in
+ * the reference, which solves one pencil per AmlsSolver::solve call,
+ * src/amls/solver.cpp:100-319): every pencil gets the reference's own solve
+ * (its own nested dissection, two-pass truncation and reduced eigenproblem),
+ * while the numeric phases run level by level over all pencils' tree nodes
+ * at once.  The pencils come as one block-diagonal CSR over
+ * n = pencil_off[batch] rows: pencil b owns rows and columns pencil_off[b]
+ * .. pencil_off[b+1] (pencil_off[0] = 0) and has no entry outside its
+ * block.  Options as for amls_solve (refine must be 0).  Outputs (host,
+ * caller-owned):
+ *   theta[batch * nev]  pencil b's ascending Ritz values at theta + b * nev
+ *                       (nev = min(opt->nev, n))
+ *   m[batch]            values per pencil (min(nev, rows of the pencil))
+ *   Z[n * nev]          M-normalised vectors, column-major: pencil b's
+ *                       vectors in its own rows, columns beyond m[b] zero;
+ *                       may be NULL
+ *   timing[AMLS_T_SLOTS] as for amls_solve, may be NULL */
+int amls_solve_batch(amls_handle h, int32_t batch, const int64_t* pencil_off,
+                     const int64_t* k_rowptr, const int32_t* k_col, const double* k_val,
+                     const int64_t* m_rowptr, const int32_t* m_col, const double* m_val,
+                     const amls_options* opt, double* theta, int64_t* m, double* Z,
+                     double* timing);
+/* Split form of amls_solve_batch (pattern analysis once, numeric solves on
+ * host or device values, as amls_analyze / amls_solve_values). */
+int amls_analyze_batch(amls_handle h, int32_t batch, const int64_t* pencil_off,
+                       const int64_t* k_rowptr, const int32_t* k_col, const int64_t* m_rowptr,
+                       const int32_t* m_col, const amls_options* opt);
+int amls_solve_values_batch(amls_handle h, const double* k_val, const double* m_val,
+                            int32_t values_on_device, double* theta, int64_t* m, double* Z,
+                            int32_t outputs_on_device, double* timing);
+
 /* Diagnostics of the last analysis/solve on the handle:
  *   info[0] tree nodes, [1] levels, [2] p of pass A, [3] p of the final pass,
  *   [4] sum of front sizes (doubles), [5] device bytes in use,
  *   [6] kernel launches in the last numeric solve,
  *   [7] refinement iterations, [8] refinement subspace size,
- *   [9] order n of the analysed pencil */
+ *   [9] order n of the analysed pencil, [10] nodes taking the shift-invert
+ *   Lanczos branch (silMode), [11] nodes it served in the last pass (the
+ *   others fell back to the dense solver) */
 #define AMLS_INFO_SLOTS 16
 int amls_info(amls_handle h, int64_t* info);
 

@@ -23,7 +23,8 @@ Third-party arithmetic: LAPACK dsygvd/dsygvx (reference: netlib LAPACK,
 unpinned) is scipy's bundled LAPACK; Eigen's SimplicialLDLT/LDLT
 (unpinned) becomes a dense Cholesky (scipy.linalg.cho_factor) - the same
 factorisation up to rounding for SPD blocks; Eigen's random start vector of
-the Lanczos (std::srand(12345)) becomes a seeded numpy vector.
+the Lanczos (std::srand(12345), Vec::Random) is restated for Eigen 3.4 over
+the Microsoft C runtime's rand() (``reference_start_vector``).
 """
 from __future__ import annotations
 
@@ -93,6 +94,28 @@ class LapackDense:
 # shift-invert Lanczos (shift_invert_lanczos.hpp)
 # --------------------------------------------------------------------------
 
+def msvcrt_rand(seed: int, count: int) -> np.ndarray:
+    """std::rand() after std::srand(seed) in the Microsoft C runtime that the
+    reference's documented toolchain (MSYS2 mingw64, docs/环境与构建说明.md:4)
+    links: state <- 214013 state + 2531011 (mod 2^32), value
+    (state >> 16) & 0x7fff, RAND_MAX = 0x7fff."""
+    out = np.empty(count, np.int64)
+    x = seed & 0xFFFFFFFF
+    for i in range(count):
+        x = (x * 214013 + 2531011) & 0xFFFFFFFF
+        out[i] = (x >> 16) & 0x7FFF
+    return out
+
+
+def reference_start_vector(n: int, seed: int = 12345) -> np.ndarray:
+    """The Lanczos start vector of shift_invert_lanczos.hpp:49-50:
+    std::srand(seed) then Eigen's Vec::Random(n), which in Eigen 3.4 draws
+    -1 + 2 rand() / RAND_MAX per entry in order.  (Eigen 3.4 is an
+    assumption: the reference leaves its version unpinned, and later Eigen
+    releases draw random bits differently.)"""
+    return -1.0 + 2.0 * msvcrt_rand(seed, n).astype(np.float64) / 32767.0
+
+
 class _SIL:
     """M-inner-product Lanczos on C = (K - sigma M)^-1 M with full double
     reorthogonalisation (shift_invert_lanczos.hpp:32-122)."""
@@ -100,8 +123,9 @@ class _SIL:
     def __init__(self, Kd, Md, sigma):
         self.n = Kd.shape[0]
         self.shift = sigma
-        Ks = np.where(np.abs(Kd) > 1e-14, Kd, 0.0)          # sparseView(1e-14)
-        self.M = np.where(np.abs(Md) > 1e-14, Md, 0.0)
+        # Eigen's sparseView(1e-14) keeps |x| > 1e-14 * dummy_precision (1e-12)
+        Ks = np.where(np.abs(Kd) > 1e-26, Kd, 0.0)
+        self.M = np.where(np.abs(Md) > 1e-26, Md, 0.0)
         A = Ks - sigma * self.M
         try:
             self.fact = sla.cho_factor(A, lower=True, check_finite=False)
@@ -115,9 +139,8 @@ class _SIL:
         ncv = min(ncv, self.n)
         alpha = np.zeros(ncv)
         beta = np.zeros(ncv)
-        rng = np.random.Generator(np.random.PCG64(seed))
         Q = np.zeros((self.n, ncv))
-        q0 = rng.uniform(-1.0, 1.0, self.n)
+        q0 = reference_start_vector(self.n, seed)
         q0 /= math.sqrt(max(q0 @ (self.M @ q0), 1e-300))
         Q[:, 0] = q0
         m = 0

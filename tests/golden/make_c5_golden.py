@@ -6,10 +6,13 @@
   c5_exact.npz   the 520 smallest exact eigenvalues by shift-invert Lanczos
                  (scipy ARPACK, sigma = 0, tol 1e-13), standing in for the
                  reference's Spectra SymGEigsShiftSolver path
-                 (src/reference/reference_solver.cpp:39-94).
+                 (src/reference/reference_solver.cpp:39-94);
+  c5_tree.npz    the separator tree of the partition (parent, role, left,
+                 right, node index lists), so that the CPU baseline runs the
+                 oracle on the same tree without calling the partitioner.
 
 Run from the repository root (takes several minutes):
-  python tests/golden/make_c5_golden.py [oracle|exact|both]
+  python tests/golden/make_c5_golden.py [oracle|exact|tree|both]
 """
 import os
 import sys
@@ -23,6 +26,7 @@ sys.path.insert(0, ROOT)
 
 from amls_b200 import cases  # noqa: E402
 from oracle import amls_ref as R  # noqa: E402
+from amls_b200.solver import recursive_bisection  # noqa: E402
 from tests.helpers import partition  # noqa: E402
 
 
@@ -36,6 +40,12 @@ def main(which):
         print("oracle", time.time() - t, "p", s.p, "pA", s.p_passA, flush=True)
         np.savez(os.path.join(HERE, "c5_oracle.npz"), theta=s.theta, p=s.p, p_passA=s.p_passA,
                  perm=perm, lambda_cut=s.lambda_cut)
+    if which in ("tree", "both"):
+        perm, t = recursive_bisection(p.K, p.M, 8, 500)
+        np.savez_compressed(os.path.join(HERE, "c5_tree.npz"), perm=perm.astype(np.int32),
+                            parent=t["parent"].astype(np.int32), role=t["role"].astype(np.int32),
+                            left=t["left"].astype(np.int32), right=t["right"].astype(np.int32),
+                            idx_ptr=t["idx_ptr"].astype(np.int32), idx=t["idx"].astype(np.int32))
     if which in ("exact", "both"):
         import scipy.sparse as sp
         import scipy.sparse.linalg as spla

@@ -195,3 +195,14 @@ def test_permute_symmetric_convention():
     A = p.K.toarray()
     assert np.array_equal(B.toarray(), A[np.ix_(perm, perm)])
     assert sp.issparse(B)
+
+
+def test_reference_start_vector_generator():
+    """The SIL start vector: std::srand / std::rand of the Microsoft C
+    runtime (first values after srand(1) are the documented 41, 18467, 6334,
+    26500, 19169) mapped to [-1, 1] as Eigen 3.4's Random does."""
+    assert R.msvcrt_rand(1, 5).tolist() == [41, 18467, 6334, 26500, 19169]
+    v = R.reference_start_vector(1000)
+    assert v.min() >= -1.0 and v.max() <= 1.0
+    r = R.msvcrt_rand(12345, 3)
+    assert np.allclose(v[:3], -1.0 + 2.0 * r / 32767.0)
