@@ -5,6 +5,6 @@ Python face of libamls_b200.so, mirroring the reference's C++ API:
 ``recursive_bisection`` (src/partition/partitioner.hpp:8-31) and the batched
 dense generalized eigensolver (src/linalg/dense_eigensolver.hpp:11-31).
 """
-from .solver import (AmlsOptions, AmlsSolver, Solution, recursive_bisection,  # noqa: F401
-                     sygvx_batched)
+from .solver import (AmlsOptions, AmlsSolver, Solution, read_matrix_market,  # noqa: F401
+                     recursive_bisection, sygvx_batched, write_matrix_market)
 from ._lib import AmlsStatusError, NotSPDError  # noqa: F401

@@ -38,7 +38,7 @@ EXPORTS = [
     "amls_solve", "amls_analyze", "amls_solve_values", "amls_info", "amls_work",
     "amls_sygvx_batched", "amls_set_profiling", "amls_kernel_times", "amls_category_work",
     "amls_sygvx_lowest_noalloc", "amls_sensitivities", "amls_permutation", "amls_solve_batch",
-    "amls_analyze_batch", "amls_solve_values_batch",
+    "amls_analyze_batch", "amls_solve_values_batch", "amls_mm_read", "amls_mm_write",
 ]
 NOALLOC_MAX_N = 128
 
@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
                                                 C.POINTER(C.c_int64), P]
         L.amls_work.argtypes = [P, P]
         L.amls_permutation.argtypes = [P, P]
+        L.amls_mm_read.argtypes = [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P]
+        L.amls_mm_write.argtypes = [C.c_char_p, C.c_int64, P, P, P]
         L.amls_solve_batch.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, C.POINTER(Options), P, P, P, P]
         L.amls_analyze_batch.argtypes = [P, C.c_int32, P, P, P, P, P, C.POINTER(Options)]
         L.amls_solve_values_batch.argtypes = [P, P, P, C.c_int32, P, P, P, C.c_int32, P]

@@ -1414,6 +1414,7 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     LAUNCH(launchScatterAdd(mVal_.as<double>(), mDst_.as<int64_t>(), nnzM_, 1.0, mPool_.as<double>(), s));
     LAUNCH(launchZero(supVal_.as<double>(), supValTotal_, s));
     LAUNCH(launchScatterAdd(mVal_.as<double>(), supDst_.as<int64_t>(), nnzM_, 1.0, supVal_.as<double>(), s));
+    silChoose(s);            // shift-invert nodes of this solve (leaves by their nonzero values)
     eliminate(s);
     checkStatus("elimination");
     silPrepare(s);

@@ -233,7 +233,9 @@ private:
         int nTiles = 0;
     };
     void silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc);
-    void silBuildStatic();                         // tables into sblob_ (before its upload)
+    void silBuildStatic();                         // separator copies and leaf counts (into sblob_)
+    void silChoose(cudaStream_t s);                // per solve, after front assembly: the SIL node set
+    void silPlan(const std::vector<int>& set);     // buffers and tables of a SIL node set
     void silPrepare(cudaStream_t s);               // per solve: sigma, factor, (K^ - sigma M^)^-1
     // Lanczos runs and Ritz selection of one pass (mode 0 index [1, want],
     // mode 1 interval (-inf, hi]): kSel[node] = kept pairs, -1 = dense solver
@@ -242,6 +244,19 @@ private:
     // Ritz vectors of the selected pairs into the engine's local form (Y, nu,
     // C Y) at the pass's offsets
     void silVectors(const std::vector<int>& kSel, const std::vector<int64_t>& projOff, cudaStream_t s);
+    std::vector<int> silSep_;                      // separators picked at analysis (structure)
+    std::map<int, int64_t> silSepOff_;             // their K^_ii copies in silSepK_
+    int64_t silSepTotal_ = 0;
+    std::vector<int> silLeafCand_;                 // leaves decided per solve
+    std::vector<std::vector<int32_t>> silMPat_;    // leaf M_ii patterns (row-major keys r n + c)
+    std::vector<SilCountDesc> silCountDescH_;
+    size_t silCountDesc_ = 0;
+    DevBuf silSepK_, silCount_, silBlobBuf_;
+    Blob silBlob_;                                 // tables of the current SIL node set
+    std::vector<int> silPlanSet_;
+    bool silPlanned_ = false;
+    size_t silLeafCopyDesc_ = 0, silLeafCopyTiles_ = 0, silSepCopyDesc_ = 0, silSepCopyTiles_ = 0;
+    int silLeafCopyNTiles_ = 0, silSepCopyNTiles_ = 0;
     std::vector<SilNode> sil_;
     std::vector<int> silOf_;                       // node -> index into sil_ (-1)
     std::vector<int32_t> silMRowH_, silMColH_;

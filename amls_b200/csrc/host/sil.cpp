@@ -62,24 +62,42 @@ void tiles32(std::vector<TileRef>& t, int desc, int64_t r, int64_t c) {
 
 void Engine::silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc) {
     const int N = static_cast<int>(nodes_.size());
+    silSep_.clear();
+    silLeafCand_.clear();
+    silMPat_.assign(static_cast<size_t>(N), {});
     sil_.clear();
     silOf_.assign(static_cast<size_t>(N), -1);
-    silMRowH_.clear();
-    silMColH_.clear();
-    silMOffH_.clear();
-    silMatTotal_ = silVecTotal_ = silInvTotal_ = 0;
+    silPlanSet_.clear();
+    silPlanned_ = false;
+    silSepTotal_ = 0;
     if (opt_.silMode < 0) return;
     std::vector<char> mark;
     for (int i : order_) {
         const Node& nd = nodes_[static_cast<size_t>(i)];
         const int64_t n = nd.n;
         if (n == 0) continue;
+        if (nd.level == 0) {
+            // leaves: decided per solve from the nonzero values of K_ii (the
+            // reference counts the nonzero entries of the dense block,
+            // eigenpair_solver.hpp:73-81); the pattern of M_ii for the products
+            if (opt_.silMode == 0 && n < 200) continue;
+            auto& pat = silMPat_[static_cast<size_t>(i)];
+            for (int64_t lr = 0; lr < n; ++lr) {
+                const int64_t old = perm_[static_cast<size_t>(nd.off + lr)];
+                for (int64_t e = mp[old]; e < mp[old + 1]; ++e) {
+                    const int64_t c = inv_[static_cast<size_t>(mc[e])];
+                    if (owner_[static_cast<size_t>(c)] == i)
+                        pat.push_back(static_cast<int32_t>(lr * n + (c - nd.off)));   // row-major key
+                }
+            }
+            silLeafCand_.push_back(i);
+            continue;
+        }
         bool use = opt_.silMode > 0;
         if (!use && n >= 200) {
-            // structural nonzeros of K^_ii (the reference counts the nonzero
-            // entries of the dense K^_ii, eigenpair_solver.hpp:73-81): the
-            // pattern of K_ii and the fill of every descendant's update,
-            // which is dense over its coupling rows inside node i
+            // separators: K^_ii carries the updates of its descendants, dense
+            // over each descendant's coupling rows inside the node; counted
+            // from that structure (exact cancellation to zero is not modelled)
             const double lim = 0.15 * static_cast<double>(n) * static_cast<double>(n);
             mark.assign(static_cast<size_t>(n * n), 0);
             int64_t cnt = 0;
@@ -102,12 +120,105 @@ void Engine::silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp,
                 if (std::find(D.anc.begin(), D.anc.end(), i) == D.anc.end()) continue;
                 auto lo = std::lower_bound(D.S.begin(), D.S.end(), static_cast<int32_t>(nd.off));
                 auto hi = std::lower_bound(D.S.begin(), D.S.end(), static_cast<int32_t>(nd.off + n));
-                for (auto a = lo; a != hi; ++a)
-                    for (auto b = lo; b != hi; ++b) put(*a - nd.off, *b - nd.off);
+                for (auto x = lo; x != hi; ++x)
+                    for (auto y = lo; y != hi; ++y) put(*x - nd.off, *y - nd.off);
             }
             use = static_cast<double>(cnt) < lim;
         }
         if (!use) continue;
+        silSep_.push_back(i);
+        silSepOff_[i] = silSepTotal_;
+        silSepTotal_ += n * n;
+    }
+    if (!silSep_.empty()) silSepK_.ensure(sizeof(double) * static_cast<size_t>(silSepTotal_));
+    if (!silLeafCand_.empty()) {
+        // count descriptors over the candidate leaves' K front diagonal blocks
+        std::vector<SilCountDesc> cd;
+        for (size_t q = 0; q < silLeafCand_.size(); ++q) {
+            const Node& nd = nodes_[static_cast<size_t>(silLeafCand_[q])];
+            cd.push_back(SilCountDesc{nullptr, nd.ld, static_cast<int32_t>(nd.n), 0});
+        }
+        silCountDescH_ = cd;
+        silCount_.ensure(sizeof(unsigned long long) * silLeafCand_.size());
+    }
+}
+
+void Engine::silBuildStatic() {
+    silCopy_.assign(static_cast<size_t>(maxLevel_) + 1, SilLevelCopy());
+    // separators: K^_ii copied before the level's in-place Cholesky (inside
+    // the elimination graph)
+    std::vector<std::vector<SilCopyDesc>> cd(static_cast<size_t>(maxLevel_) + 1);
+    std::vector<std::vector<TileRef>> ct(static_cast<size_t>(maxLevel_) + 1);
+    for (int i : silSep_) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        auto& d = cd[static_cast<size_t>(nd.level)];
+        tiles32(ct[static_cast<size_t>(nd.level)], static_cast<int>(d.size()), nd.n, nd.n);
+        d.push_back(SilCopyDesc{kPool_.as<double>() + nd.frontOff, nd.ld, silSepK_.as<double>() + silSepOff_.at(i),
+                                static_cast<int32_t>(nd.n), 0});
+    }
+    for (int l = 0; l <= maxLevel_; ++l) {
+        SilLevelCopy& c = silCopy_[static_cast<size_t>(l)];
+        c.desc = sblob_.add(cd[static_cast<size_t>(l)]);
+        c.tiles = sblob_.add(ct[static_cast<size_t>(l)]);
+        c.nTiles = static_cast<int>(ct[static_cast<size_t>(l)].size());
+    }
+    for (SilCountDesc& d : silCountDescH_) d.F = nullptr;
+    for (size_t q = 0; q < silLeafCand_.size(); ++q)
+        silCountDescH_[q].F = kPool_.as<double>() + nodes_[static_cast<size_t>(silLeafCand_[q])].frontOff;
+    silCountDesc_ = sblob_.add(silCountDescH_);
+}
+
+// the SIL nodes of this solve: the separators picked at analysis and the
+// leaves whose K_ii has fewer than 0.15 n^2 nonzero values (silMode 0) or
+// every leaf (silMode 1); a new set rebuilds the node plan
+void Engine::silChoose(cudaStream_t s) {
+    if (opt_.silMode < 0) return;
+    std::vector<int> set(silSep_.begin(), silSep_.end());
+    if (!silLeafCand_.empty()) {
+        const int nc = static_cast<int>(silLeafCand_.size());
+        if (opt_.silMode > 0) {
+            set.insert(set.end(), silLeafCand_.begin(), silLeafCand_.end());
+        } else {
+            LAUNCH(launchSilCountNonzero(sblob_.dev<SilCountDesc>(silCountDesc_), nc,
+                                         silCount_.as<unsigned long long>(), s));
+            std::vector<unsigned long long> cnt(static_cast<size_t>(nc));
+            cudaCheck(cudaMemcpyAsync(cnt.data(), silCount_.as<unsigned long long>(), sizeof(unsigned long long) * nc,
+                                      cudaMemcpyDeviceToHost, s), "SIL counts");
+            cudaCheck(cudaStreamSynchronize(s), "SIL counts");
+            for (int q = 0; q < nc; ++q) {
+                const double nn = static_cast<double>(nodes_[static_cast<size_t>(silLeafCand_[static_cast<size_t>(q)])].n);
+                if (static_cast<double>(cnt[static_cast<size_t>(q)]) < 0.15 * nn * nn)
+                    set.push_back(silLeafCand_[static_cast<size_t>(q)]);
+            }
+        }
+    }
+    std::sort(set.begin(), set.end(), [&](int x, int y) {
+        return nodes_[static_cast<size_t>(x)].off < nodes_[static_cast<size_t>(y)].off;
+    });
+    if (!silPlanned_ || set != silPlanSet_) silPlan(set);
+    // leaves: K_ii = K^_ii straight from the assembled front (before the
+    // elimination factors it in place)
+    if (silLeafCopyNTiles_ > 0)
+        LAUNCH(launchSilSymCopy(silBlob_.dev<SilCopyDesc>(silLeafCopyDesc_), silBlob_.dev<TileRef>(silLeafCopyTiles_),
+                                silLeafCopyNTiles_, s));
+}
+
+void Engine::silPlan(const std::vector<int>& set) {
+    const int N = static_cast<int>(nodes_.size());
+    sil_.clear();
+    silOf_.assign(static_cast<size_t>(N), -1);
+    silMRowH_.clear();
+    silMColH_.clear();
+    silMOffH_.clear();
+    silMatTotal_ = silVecTotal_ = silInvTotal_ = 0;
+    silPlanSet_ = set;
+    silPlanned_ = true;
+    silLeafCopyNTiles_ = silSepCopyNTiles_ = 0;
+    silBlob_.clear();
+    if (set.empty()) return;
+    for (int i : set) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        const int64_t n = nd.n;
         SilNode sn;
         sn.node = i;
         sn.mat = silMatTotal_;
@@ -125,15 +236,15 @@ void Engine::silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp,
         auto lowerOff = [&](int64_t r, int64_t c) {
             return r >= c ? nd.frontOff + r + c * nd.ld : nd.frontOff + c + r * nd.ld;
         };
+        const auto& pat = silMPat_[static_cast<size_t>(i)];
+        size_t q = 0;
         for (int64_t lr = 0; lr < n; ++lr) {
             silMRowH_.push_back(static_cast<int32_t>(static_cast<int64_t>(silMColH_.size()) - e0));
             if (nd.level == 0) {
-                const int64_t old = perm_[static_cast<size_t>(nd.off + lr)];
-                for (int64_t e = mp[old]; e < mp[old + 1]; ++e) {
-                    const int64_t c = inv_[static_cast<size_t>(mc[e])];
-                    if (owner_[static_cast<size_t>(c)] != i) continue;
-                    silMColH_.push_back(static_cast<int32_t>(c - nd.off));
-                    silMOffH_.push_back(lowerOff(lr, c - nd.off));
+                for (; q < pat.size() && pat[q] / n == lr; ++q) {
+                    const int64_t lc = pat[q] % n;
+                    silMColH_.push_back(static_cast<int32_t>(lc));
+                    silMOffH_.push_back(lowerOff(lr, lc));
                 }
             } else {
                 for (int64_t lc = 0; lc < n; ++lc) {
@@ -146,7 +257,6 @@ void Engine::silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp,
         silOf_[static_cast<size_t>(i)] = static_cast<int>(sil_.size());
         sil_.push_back(sn);
     }
-    if (sil_.empty()) return;
     const size_t nS = sil_.size();
     const size_t mat = static_cast<size_t>(std::max<int64_t>(silMatTotal_, 1));
     silA_.ensure(sizeof(double) * mat);
@@ -174,28 +284,27 @@ void Engine::silAnalyze(const int64_t* kp, const int32_t* kc, const int64_t* mp,
                               cudaMemcpyHostToDevice, stream_), "upload");
     // L^-1 of A is written below the diagonal only
     cudaCheck(cudaMemsetAsync(silLinv_.as<double>(), 0, sizeof(double) * mat, stream_), "zero");
-    cudaCheck(cudaStreamSynchronize(stream_), "upload");
-}
 
-void Engine::silBuildStatic() {
-    silCopy_.assign(static_cast<size_t>(maxLevel_) + 1, SilLevelCopy());
-    if (sil_.empty()) return;
+    // node tables
     double* A = silA_.as<double>();
-    std::vector<std::vector<SilCopyDesc>> cd(static_cast<size_t>(maxLevel_) + 1);
-    std::vector<std::vector<TileRef>> ct(static_cast<size_t>(maxLevel_) + 1);
-    std::vector<SilCopyDesc> low;
-    std::vector<TileRef> lowT;
+    std::vector<SilCopyDesc> leafCp, sepCp, low;
+    std::vector<TileRef> leafT, sepT, lowT;
     std::vector<SilShiftDesc> sh;
     std::vector<CholItem> items;
     std::vector<GemmDesc> bd;
     std::vector<TileRef> bt;
-    for (size_t b = 0; b < sil_.size(); ++b) {
+    for (size_t b = 0; b < nS; ++b) {
         const SilNode& sn = sil_[b];
         const Node& nd = nodes_[static_cast<size_t>(sn.node)];
         const int64_t n = nd.n;
-        auto& d = cd[static_cast<size_t>(nd.level)];
-        tiles32(ct[static_cast<size_t>(nd.level)], static_cast<int>(d.size()), n, n);
-        d.push_back(SilCopyDesc{kPool_.as<double>() + nd.frontOff, nd.ld, A + sn.mat, static_cast<int32_t>(n), 0});
+        if (nd.level == 0) {
+            tiles32(leafT, static_cast<int>(leafCp.size()), n, n);
+            leafCp.push_back(SilCopyDesc{kPool_.as<double>() + nd.frontOff, nd.ld, A + sn.mat, static_cast<int32_t>(n), 0});
+        } else {
+            tiles32(sepT, static_cast<int>(sepCp.size()), n, n);
+            sepCp.push_back(SilCopyDesc{silSepK_.as<double>() + silSepOff_.at(sn.node), n, A + sn.mat,
+                                        static_cast<int32_t>(n), 0});
+        }
         tiles32(lowT, static_cast<int>(low.size()), n, n);
         low.push_back(SilCopyDesc{kPool_.as<double>() + nd.frontOff, nd.ld, silL_.as<double>() + sn.mat,
                                   static_cast<int32_t>(n), 1});
@@ -208,28 +317,33 @@ void Engine::silBuildStatic() {
         bd.push_back(gemmS(n, n, n, kTransA | kTriKFrom, silLinv_.as<double>() + sn.mat, n,
                            silLinv_.as<double>() + sn.mat, n, silB_.as<double>() + sn.mat, n));
     }
-    for (int l = 0; l <= maxLevel_; ++l) {
-        SilLevelCopy& c = silCopy_[static_cast<size_t>(l)];
-        c.desc = sblob_.add(cd[static_cast<size_t>(l)]);
-        c.tiles = sblob_.add(ct[static_cast<size_t>(l)]);
-        c.nTiles = static_cast<int>(ct[static_cast<size_t>(l)].size());
-    }
-    silLowerDesc_ = sblob_.add(low);
-    silLowerTiles_ = sblob_.add(lowT);
+    silLeafCopyDesc_ = silBlob_.add(leafCp);
+    silLeafCopyTiles_ = silBlob_.add(leafT);
+    silLeafCopyNTiles_ = static_cast<int>(leafT.size());
+    silSepCopyDesc_ = silBlob_.add(sepCp);
+    silSepCopyTiles_ = silBlob_.add(sepT);
+    silSepCopyNTiles_ = static_cast<int>(sepT.size());
+    silLowerDesc_ = silBlob_.add(low);
+    silLowerTiles_ = silBlob_.add(lowT);
     silLowerNTiles_ = static_cast<int>(lowT.size());
-    silShiftDesc_ = sblob_.add(sh);
-    silChol_ = buildCholPlan(sblob_, items);
-    silBGemm_ = addBatch(sblob_, bd, bt);
+    silShiftDesc_ = silBlob_.add(sh);
+    silChol_ = buildCholPlan(silBlob_, items);
+    silBGemm_ = addBatch(silBlob_, bd, bt);
+    silBlob_.upload(silBlobBuf_, stream_);
+    cudaCheck(cudaStreamSynchronize(stream_), "SIL plan");
 }
 
 void Engine::silPrepare(cudaStream_t s) {
     if (sil_.empty()) return;
     const int nS = static_cast<int>(sil_.size());
-    LAUNCH(launchSilShift(sblob_.dev<SilShiftDesc>(silShiftDesc_), nS, s));
-    LAUNCH(launchSilSymCopy(sblob_.dev<SilCopyDesc>(silLowerDesc_), sblob_.dev<TileRef>(silLowerTiles_),
+    if (silSepCopyNTiles_ > 0)
+        LAUNCH(launchSilSymCopy(silBlob_.dev<SilCopyDesc>(silSepCopyDesc_), silBlob_.dev<TileRef>(silSepCopyTiles_),
+                                silSepCopyNTiles_, s));
+    LAUNCH(launchSilShift(silBlob_.dev<SilShiftDesc>(silShiftDesc_), nS, s));
+    LAUNCH(launchSilSymCopy(silBlob_.dev<SilCopyDesc>(silLowerDesc_), silBlob_.dev<TileRef>(silLowerTiles_),
                             silLowerNTiles_, s));
-    runCholPlan(sblob_, silChol_, s);
-    LAUNCH(launchGemmBatched(sblob_.dev<GemmDesc>(silBGemm_.desc), sblob_.dev<TileRef>(silBGemm_.tiles),
+    runCholPlan(silBlob_, silChol_, s);
+    LAUNCH(launchGemmBatched(silBlob_.dev<GemmDesc>(silBGemm_.desc), silBlob_.dev<TileRef>(silBGemm_.tiles),
                              silBGemm_.nTiles, s));
     cudaCheck(cudaMemsetAsync(silState_.as<int32_t>(), 0, sizeof(int32_t) * 2 * nS, s), "SIL state");
     checkStatus("shift-invert factorisation");

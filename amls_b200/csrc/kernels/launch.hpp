@@ -202,6 +202,13 @@ struct SilCopyDesc {
     int32_t n, mode;
 };
 cudaError_t launchSilSymCopy(const SilCopyDesc* d, const TileRef* tiles, int nTiles, cudaStream_t s);
+// count[b] = number of nonzero values of the n x n block F (ld) of descriptor b
+struct SilCountDesc {
+    const double* F;
+    int64_t ld;
+    int32_t n, pad;
+};
+cudaError_t launchSilCountNonzero(const SilCountDesc* d, int nDesc, unsigned long long* count, cudaStream_t s);
 // sigma = -max(1e-10, 1e-9 max_j |A_jj|), then A <- A - sigma M (M: lower
 // triangle of the M front's diagonal block, ld ldm).  One CTA per node.
 struct SilShiftDesc {

@@ -93,6 +93,28 @@ cudaError_t launchSilSymCopy(const SilCopyDesc* d, const TileRef* tiles, int nTi
     return cudaGetLastError();
 }
 
+// nonzero values of each block (one CTA per block; integer sums, exact)
+__global__ void __launch_bounds__(256) silCountKernel(const SilCountDesc* __restrict__ d,
+                                                      unsigned long long* __restrict__ count) {
+    const SilCountDesc D = d[blockIdx.x];
+    const int64_t nn = (int64_t)D.n * D.n;
+    unsigned long long c = 0;
+    for (int64_t q = threadIdx.x; q < nn; q += blockDim.x) {
+        const int r = (int)(q % D.n), col = (int)(q / D.n);
+        c += D.F[r + (int64_t)col * D.ld] != 0.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(count + blockIdx.x, c);
+}
+
+cudaError_t launchSilCountNonzero(const SilCountDesc* d, int nDesc, unsigned long long* count, cudaStream_t s) {
+    if (nDesc <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long) * (size_t)nDesc, s);
+    if (e != cudaSuccess) return e;
+    silCountKernel<<<nDesc, 256, 0, s>>>(d, count);
+    return cudaGetLastError();
+}
+
 // One CTA per node: sigma from the largest |K^_jj| (A holds K^), then
 // A <- A - sigma M^ (M^ from the M front's lower triangle).
 __global__ void __launch_bounds__(256) silShiftKernel(const SilShiftDesc* __restrict__ d) {

@@ -89,6 +89,27 @@ def _csr_arrays(A):
     return rp, ci, v
 
 
+def read_matrix_market(path: str) -> sp.csr_matrix:
+    """readMatrixMarket (src/io/matrix_market.cpp:48-97) through the C ABI."""
+    n = C.c_int64(0)
+    nnz = C.c_int64(0)
+    _lib.check(_lib.lib().amls_mm_read(str(path).encode(), C.byref(n), C.byref(nnz), None, None, None))
+    rp = np.zeros(n.value + 1, np.int64)
+    ci = np.zeros(max(nnz.value, 1), np.int32)
+    v = np.zeros(max(nnz.value, 1), np.float64)
+    _lib.check(_lib.lib().amls_mm_read(str(path).encode(), C.byref(n), C.byref(nnz), _lib.ptr(rp),
+                                       _lib.ptr(ci), _lib.ptr(v)))
+    return sp.csr_matrix((v[:nnz.value], ci[:nnz.value], rp), shape=(n.value, n.value))
+
+
+def write_matrix_market(path: str, A) -> None:
+    """writeMatrixMarket (src/io/matrix_market.cpp:99-115): lower triangle,
+    real symmetric."""
+    rp, ci, v = _csr_arrays(A)
+    _lib.check(_lib.lib().amls_mm_write(str(path).encode(), A.shape[0], _lib.ptr(rp), _lib.ptr(ci),
+                                        _lib.ptr(v)))
+
+
 def recursive_bisection(K, M, nLevels: int, leafSize: int):
     """Partition of |K| + |M|: returns (perm, tree arrays dict)."""
     kp, kc, _ = _csr_arrays(K)

@@ -129,6 +129,22 @@ int amls_partition(int64_t n, const int64_t* k_rowptr, const int32_t* k_col,
                    int32_t* role, int64_t* left, int64_t* right, int64_t* idx_ptr,
                    int64_t* idx);
 
+/* Matrix Market input (host only).  Replaces readMatrixMarket
+ * (src/io/matrix_market.cpp:48-97): coordinate format, real / double /
+ * integer / pattern fields (pattern entries 1.0), general or symmetric
+ * (mirrored), comments and empty lines skipped, duplicates summed.  The
+ * matrix must be square.  Two calls: with rowptr/col/val NULL it sets *n and
+ * *nnz; then with arrays of n+1 / nnz / nnz entries it fills the CSR (sorted
+ * columns). */
+int amls_mm_read(const char* path, int64_t* n, int64_t* nnz, int64_t* rowptr, int32_t* col,
+                 double* val);
+/* Matrix Market output of a symmetric CSR matrix: the lower triangle as
+ * "real symmetric" with 17 significant digits (writeMatrixMarket,
+ * src/io/matrix_market.cpp:99-115; the size line counts the entries
+ * written). */
+int amls_mm_write(const char* path, int64_t n, const int64_t* rowptr, const int32_t* col,
+                  const double* val);
+
 /* Whole AMLS solve from host CSR arrays.  Replaces AmlsSolver::solve
  * (src/amls/solver.cpp:100-319): optional shift, partition + permutation,
  * two-pass truncation (k0 = max(4, ceil(3 nev / N)), lambda_cut = eta *
