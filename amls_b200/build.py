@@ -3,7 +3,9 @@
 Compiles every ``csrc/**/*.cu`` with nvcc for ``arch=compute_100a,code=sm_100a``
 and every ``csrc/**/*.cpp`` with g++ (C++17), then links them with the CUDA
 runtime and the METIS library shipped with the CUDA toolkit into
-``amls_b200/libamls_b200.so`` (in-tree, next to this file).  Objects go to
+``amls_b200/libamls_b200.so`` (in-tree, next to this file), and the
+command-line programs ``amls_solve`` / ``amls_verify`` (csrc/apps) linked
+against it.  Objects go to
 ``amls_b200/_build/``; a source is recompiled only when it or a header under
 ``csrc/`` or ``include/`` is newer than its object.
 """
@@ -58,7 +60,7 @@ def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "**", "*.cu"), recursive=True)
                   + glob.glob(os.path.join(CSRC, "**", "*.cpp"), recursive=True))
-    srcs = [s for s in srcs if os.sep + "worker" + os.sep not in s]
+    srcs = [s for s in srcs if os.sep + "worker" + os.sep not in s and os.sep + "apps" + os.sep not in s]
     hm = _headers_mtime()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         results = list(ex.map(lambda s: _compile(s, hm, verbose), srcs))
@@ -83,6 +85,18 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"worker build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    # command-line programs over the C ABI (amls_solve, amls_verify)
+    for app in ("amls_solve", "amls_verify"):
+        asrc = os.path.join(CSRC, "apps", app + ".cpp")
+        exe = os.path.join(HERE, app)
+        dep = max(os.path.getmtime(asrc), os.path.getmtime(os.path.join(CSRC, "apps", "app_common.hpp")),
+                  os.path.getmtime(LIB))
+        if not os.path.exists(exe) or os.path.getmtime(exe) < dep:
+            cmd = ["g++", *CXX_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC, asrc, "-o", exe,
+                   "-L", HERE, "-l:libamls_b200.so", "-Wl,-rpath,$ORIGIN"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"{app} build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     return LIB
 
 
