@@ -146,6 +146,65 @@ extern "C" int amls_solve_batch(amls_handle h, int32_t batch, const int64_t* pen
     });
 }
 
+extern "C" int amls_eliminate(amls_handle h, const double* kv, const double* mv, int32_t values_on_device) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!kv || !mv) return fail(AMLS_ERR_INVALID_ARGUMENT, "null values");
+        h->eng->stageEliminate(kv, mv, values_on_device != 0);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_condense(amls_handle h, int32_t mode, int64_t k, double lambda_cut, int64_t* p) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->stageCondense(mode, static_cast<int>(k), lambda_cut, p);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_pass_modes(amls_handle h, int32_t* k_node, double* mu) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->stageModes(k_node, mu);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_reduced_eig(amls_handle h, int64_t want, int32_t vectors, double* theta, int64_t* m) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->stageReduced(static_cast<int>(want), vectors != 0, theta, m);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_backtransform(amls_handle h, double* Z, int32_t outputs_on_device, int64_t* m) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->stageBacktransform(Z, outputs_on_device != 0, m);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_refine(amls_handle h, int64_t nev, double* theta, double* Z, int32_t outputs_on_device,
+                           int64_t* iters) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        h->eng->stageRefine(static_cast<int>(nev), theta, Z, outputs_on_device != 0, iters);
+        return AMLS_OK;
+    });
+}
+
+extern "C" int amls_tree(amls_handle h, int64_t* n_nodes, int64_t* parent, int64_t* size, int32_t* level) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!h->eng->analyzed()) return fail(AMLS_ERR_INVALID_ARGUMENT, "no analysis on the handle");
+        h->eng->tree(n_nodes, parent, size, level);
+        return AMLS_OK;
+    });
+}
+
 extern "C" int amls_info(amls_handle h, int64_t* info) {
     return guarded([&]() -> int {
         if (int e = checkHandle(h)) return e;

@@ -194,6 +194,7 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
     cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
     analyzed_ = false;
     tridiagDone_ = false;
+    stageLevel_ = 0;
     dropGraphs();              // the tables (and buffers) they replay are rebuilt
     if (n <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty matrix");
     for (int64_t r = 0; r < n; ++r) {
@@ -1375,26 +1376,11 @@ void Engine::backtransform(const Pass& P, int m, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // numeric solve
 // ---------------------------------------------------------------------------
-void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
-                         double* Z, bool outputsOnDevice, int64_t* pOut, double* timing, int64_t* mOut) {
-    if (!analyzed_) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_solve_values before amls_analyze");
-    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
-    if (opt_.nev <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
-    const int64_t nev = std::min<int64_t>(opt_.nev, n_);
-    cudaStream_t s = stream_;
-    launches_ = 0;
-    for (int t = 2; t < AMLS_WORK_SLOTS; ++t) work_[t] = 0;
-    for (int c = 0; c < kProfCats; ++c) {
-        catF_[c] = elimCatF_[c];
-        catB_[c] = elimCatB_[c];
-    }
-    tridiagDone_ = false;
-    const auto t0 = Clock::now();
-    if (!evSolve0_) {
-        cudaCheck(cudaEventCreate(&evSolve0_), "cudaEventCreate");
-        cudaCheck(cudaEventCreate(&evSolve1_), "cudaEventCreate");
-    }
-    cudaCheck(cudaEventRecord(evSolve0_, s), "cudaEventRecord");
+// values in, fronts assembled, shift-invert nodes chosen, elimination
+// (replayed graph) and the shift-invert factorisations; returns the time
+// after the value upload
+Engine::Clock::time_point Engine::numericElimination(const double* kv, const double* mv, bool valuesOnDevice,
+                                                     cudaStream_t s) {
     cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
     if (valuesOnDevice) {
         cudaCheck(cudaMemcpyAsync(kVal_.as<double>(), kv, sizeof(double) * nnzK_, cudaMemcpyDeviceToDevice, s), "values");
@@ -1418,6 +1404,31 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     eliminate(s);
     checkStatus("elimination");
     silPrepare(s);
+    return t1;
+}
+
+void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
+                         double* Z, bool outputsOnDevice, int64_t* pOut, double* timing, int64_t* mOut) {
+    if (!analyzed_) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_solve_values before amls_analyze");
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    if (opt_.nev <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "nev must be positive");
+    const int64_t nev = std::min<int64_t>(opt_.nev, n_);
+    cudaStream_t s = stream_;
+    stageLevel_ = 0;
+    launches_ = 0;
+    for (int t = 2; t < AMLS_WORK_SLOTS; ++t) work_[t] = 0;
+    for (int c = 0; c < kProfCats; ++c) {
+        catF_[c] = elimCatF_[c];
+        catB_[c] = elimCatB_[c];
+    }
+    tridiagDone_ = false;
+    const auto t0 = Clock::now();
+    if (!evSolve0_) {
+        cudaCheck(cudaEventCreate(&evSolve0_), "cudaEventCreate");
+        cudaCheck(cudaEventCreate(&evSolve1_), "cudaEventCreate");
+    }
+    cudaCheck(cudaEventRecord(evSolve0_, s), "cudaEventRecord");
+    const auto t1 = numericElimination(kv, mv, valuesOnDevice, s);
     const auto t2 = Clock::now();
     double tRed = 0;
     Pass P;
@@ -1719,6 +1730,100 @@ void Engine::sygvxBatched(int batch, const int64_t* n, const int64_t* matOff, co
                              cudaMemcpyDeviceToHost), "V");
     }
     (void)ko;
+}
+
+// ---------------------------------------------------------------------------
+// stage-by-stage solve (one pencil)
+// ---------------------------------------------------------------------------
+void Engine::stageEliminate(const double* kv, const double* mv, bool onDevice) {
+    if (!analyzed_) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_eliminate before amls_analyze");
+    if (nPencils_ != 1) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "stage calls need a single pencil");
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    launches_ = 0;
+    for (int t = 2; t < AMLS_WORK_SLOTS; ++t) work_[t] = 0;
+    for (int c = 0; c < kProfCats; ++c) {
+        catF_[c] = elimCatF_[c];
+        catB_[c] = elimCatB_[c];
+    }
+    tridiagDone_ = false;
+    stageLevel_ = 0;
+    numericElimination(kv, mv, onDevice, stream_);
+    stageLevel_ = 1;
+}
+
+void Engine::stageCondense(int mode, int k, double lambdaCut, int64_t* pOut) {
+    if (stageLevel_ < 1) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_condense before amls_eliminate");
+    if (mode != 0 && mode != 1) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "mode must be 0 (fixed count) or 1 (threshold)");
+    if (mode == 0 && k <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "fixed count must be positive");
+    stage_ = Pass();
+    const double thr = lambdaCut > 0 ? 1.0 / lambdaCut : 1e300;
+    condense(mode, {mode == 0 ? k : 0}, {mode == 0 ? 0.0 : thr}, {mode == 0 ? 0.0 : lambdaCut}, stage_, stream_);
+    stageLevel_ = 2;
+    if (pOut) *pOut = stage_.p;
+}
+
+void Engine::stageModes(int32_t* kNode, double* mu) const {
+    if (stageLevel_ < 2) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "no condensed pass on the handle");
+    if (kNode) std::copy(stage_.k.begin(), stage_.k.end(), kNode);
+    if (mu) {
+        std::vector<double> nu(static_cast<size_t>(stage_.p));
+        cudaCheck(cudaMemcpy(nu.data(), wPool_.as<double>(), sizeof(double) * stage_.p, cudaMemcpyDeviceToHost), "modes");
+        for (int64_t j = 0; j < stage_.p; ++j) mu[j] = 1.0 / nu[static_cast<size_t>(j)];
+    }
+}
+
+void Engine::stageReduced(int want, bool vectors, double* theta, int64_t* mOut) {
+    if (stageLevel_ < 2) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_reduced_eig before amls_condense");
+    if (want <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "want must be positive");
+    reducedSolve(stage_, {want}, stream_, vectors);
+    const auto& th = stage_.theta[0];
+    if (theta) std::copy(th.begin(), th.end(), theta);
+    if (mOut) *mOut = static_cast<int64_t>(th.size());
+    stageLevel_ = vectors ? 4 : 3;
+}
+
+void Engine::stageBacktransform(double* Z, bool onDevice, int64_t* mOut) {
+    if (stageLevel_ < 4) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_backtransform needs amls_reduced_eig with vectors");
+    const int m = stage_.got[0];
+    backtransform(stage_, m, stream_);
+    finalizeVectors(ztPool_.as<double>(), m, m, stream_);
+    if (Z)
+        cudaCheck(cudaMemcpy(Z, zOut_.as<double>(), sizeof(double) * m * n_,
+                             onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost), "Z");
+    if (mOut) *mOut = m;
+    stageLevel_ = 5;
+}
+
+void Engine::stageRefine(int nev, double* theta, double* Z, bool onDevice, int64_t* iters) {
+    if (stageLevel_ < 5) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_refine needs amls_backtransform first");
+    if (opt_.refine < 1)
+        throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "amls_refine needs an analysis with refine >= 1 (applications per step)");
+    const int m = stage_.got[0];
+    if (nev <= 0 || nev > m) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "nev must be 1 .. the back-transformed count");
+    std::vector<double> th = stage_.theta[0];
+    const int it = refine(ztPool_.as<double>(), m, nev, th, Z != nullptr, stream_);
+    th.resize(static_cast<size_t>(nev));
+    if (theta) std::copy(th.begin(), th.end(), theta);
+    if (Z) {
+        finalizeVectors(ztPool_.as<double>(), m, nev, stream_);
+        cudaCheck(cudaMemcpy(Z, zOut_.as<double>(), sizeof(double) * nev * n_,
+                             onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost), "Z");
+    }
+    if (iters) *iters = it;
+    lastTheta_ = th;
+    lastHasVectors_ = Z != nullptr;
+    stageLevel_ = 1;          // the basis in ztPool_ is consumed
+}
+
+void Engine::tree(int64_t* nNodes, int64_t* parent, int64_t* size, int32_t* level) const {
+    const int N = static_cast<int>(nodes_.size());
+    if (nNodes) *nNodes = N;
+    for (int i = 0; i < N; ++i) {
+        const Node& nd = nodes_[static_cast<size_t>(i)];
+        if (parent) parent[i] = nd.parent;
+        if (size) size[i] = nd.n;
+        if (level) level[i] = nd.level;
+    }
 }
 
 void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, int32_t ntypes,

@@ -22,6 +22,7 @@
 //   back-transform z = L^-T S q (subspace_condensation.cpp:263-319),
 //     un-permutation and M-normalisation (solver.cpp:302-311).
 #pragma once
+#include <chrono>
 #include <cstdint>
 #include <map>
 #include <string>
@@ -48,6 +49,18 @@ public:
     void analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const int32_t* kc,
                       const int64_t* mp, const int32_t* mc, const amls_options& opt);
     int pencils() const { return nPencils_; }
+    // stage-by-stage numeric solve of one analysed pencil, at the reference's
+    // seams: GaussianElimination::run, SubspaceCondensation::run with
+    // FixedCount(k) (mode 0) or Threshold(lambda_cut) (mode 1),
+    // solveProjected, backtransform + un-permute + M-normalise, and the FP64
+    // refinement
+    void stageEliminate(const double* kv, const double* mv, bool onDevice);
+    void stageCondense(int mode, int k, double lambdaCut, int64_t* pOut);
+    void stageModes(int32_t* kNode, double* mu) const;
+    void stageReduced(int want, bool vectors, double* theta, int64_t* mOut);
+    void stageBacktransform(double* Z, bool onDevice, int64_t* mOut);
+    void stageRefine(int nev, double* theta, double* Z, bool onDevice, int64_t* iters);
+    void tree(int64_t* nNodes, int64_t* parent, int64_t* size, int32_t* level) const;
     // theta: one pencil theta[nev]; a batch theta[q * nev + j] with
     // mOut[q] values per pencil.  Z: n x (nev or fewer for one pencil).
     void solveValues(const double* kv, const double* mv, bool valuesOnDevice, double* theta,
@@ -110,6 +123,8 @@ private:
         int mMax = 0;                   // largest got
     };
 
+    using Clock = std::chrono::steady_clock;
+    Clock::time_point numericElimination(const double* kv, const double* mv, bool valuesOnDevice, cudaStream_t s);
     void buildStatic();
     void eliminate(cudaStream_t s);
     void eliminateLaunches(cudaStream_t s);
@@ -257,6 +272,9 @@ private:
     bool silPlanned_ = false;
     size_t silLeafCopyDesc_ = 0, silLeafCopyTiles_ = 0, silSepCopyDesc_ = 0, silSepCopyTiles_ = 0;
     int silLeafCopyNTiles_ = 0, silSepCopyNTiles_ = 0;
+    // stage-by-stage state
+    Pass stage_;
+    int stageLevel_ = 0;          // 1 eliminated, 2 condensed, 3 reduced (with vectors: 4), 5 back-transformed
     std::vector<SilNode> sil_;
     std::vector<int> silOf_;                       // node -> index into sil_ (-1)
     std::vector<int32_t> silMRowH_, silMColH_;

@@ -251,6 +251,64 @@ class AmlsSolver:
         out["p"] = int(p.value)
         return out
 
+    # ---- stage by stage (the reference's pipeline seams) ----
+    def eliminate(self, K, M) -> None:
+        """GaussianElimination::run on the analysed pattern with these values."""
+        _, _, kv = _csr_arrays(K)
+        _, _, mv = _csr_arrays(M)
+        _lib.check(_lib.lib().amls_eliminate(self._h, _lib.ptr(kv), _lib.ptr(mv), 0))
+
+    def condense(self, mode: str, k: int = 0, lambda_cut: float = 0.0) -> int:
+        """SubspaceCondensation::run with FixedCountTruncation(k) ("fixed") or
+        ThresholdTruncation(lambda_cut) ("threshold"); returns p."""
+        p = C.c_int64(0)
+        _lib.check(_lib.lib().amls_condense(self._h, 0 if mode == "fixed" else 1, int(k), float(lambda_cut),
+                                            C.byref(p)))
+        self._p = p.value
+        return p.value
+
+    def pass_modes(self):
+        """(kept count per tree node, local eigenvalues mu in node-id order)."""
+        t = self.tree()
+        k = np.zeros(len(t["parent"]), np.int32)
+        mu = np.zeros(max(self._p, 1))
+        _lib.check(_lib.lib().amls_pass_modes(self._h, _lib.ptr(k), _lib.ptr(mu)))
+        return k, mu[:self._p]
+
+    def reduced_eig(self, want: int, vectors: bool = True) -> np.ndarray:
+        theta = np.zeros(max(int(want), 1))
+        m = C.c_int64(0)
+        _lib.check(_lib.lib().amls_reduced_eig(self._h, int(want), 1 if vectors else 0, _lib.ptr(theta),
+                                               C.byref(m)))
+        self._m = m.value
+        return theta[:m.value].copy()
+
+    def backtransform(self) -> np.ndarray:
+        n = self.info()["n"]
+        Z = np.zeros((self._m, n))
+        m = C.c_int64(0)
+        _lib.check(_lib.lib().amls_backtransform(self._h, _lib.ptr(Z), 0, C.byref(m)))
+        return Z[:m.value].T.copy()
+
+    def refine(self, nev: int):
+        n = self.info()["n"]
+        theta = np.zeros(int(nev))
+        Z = np.zeros((int(nev), n))
+        it = C.c_int64(0)
+        _lib.check(_lib.lib().amls_refine(self._h, int(nev), _lib.ptr(theta), _lib.ptr(Z), 0, C.byref(it)))
+        self._last_nev = int(nev)
+        return theta, Z.T.copy(), int(it.value)
+
+    def tree(self) -> dict:
+        nn = C.c_int64(0)
+        _lib.check(_lib.lib().amls_tree(self._h, C.byref(nn), None, None, None))
+        N = nn.value
+        parent = np.zeros(N, np.int64)
+        size = np.zeros(N, np.int64)
+        level = np.zeros(N, np.int32)
+        _lib.check(_lib.lib().amls_tree(self._h, C.byref(nn), _lib.ptr(parent), _lib.ptr(size), _lib.ptr(level)))
+        return dict(parent=parent, size=size, level=level)
+
     def sensitivities(self, pencil, weights=None, per_mode: bool = False, gap_tol: float = 1e-6,
                       elem_type=None):
         """Per-element eigenvalue sensitivities of the last solve's eigenpairs

@@ -204,6 +204,42 @@ int amls_solve_values_batch(amls_handle h, const double* k_val, const double* m_
                             int32_t values_on_device, double* theta, int64_t* m, double* Z,
                             int32_t outputs_on_device, double* timing);
 
+/* Stage-by-stage numeric solve of an analysed single pencil, at the seams
+ * of the reference's pipeline, so that a caller can drive its own
+ * truncation policy (every stage runs on the GPU; state stays on the
+ * handle):
+ *   amls_eliminate      GaussianElimination::run (gaussian_elimination.cpp:
+ *                       828-1088): values in (host or device arrays of
+ *                       nnz(K), nnz(M)), fronts assembled, elimination and
+ *                       congruence updates, shift-invert factorisations
+ *   amls_condense       SubspaceCondensation::run (subspace_condensation.cpp:
+ *                       18-36) with FixedCountTruncation(k) (mode 0) or
+ *                       ThresholdTruncation(lambda_cut) (mode 1,
+ *                       spectral_truncation.hpp:35-88): local eigensolves of
+ *                       every node (dense or shift-invert by silMode) and the
+ *                       projection; *p = reduced size
+ *   amls_pass_modes     the pass's kept count per tree node k_node[N] and
+ *                       local eigenvalues mu[p] (node-id order)
+ *   amls_reduced_eig    solveProjected (solver.cpp:145-161): the lowest
+ *                       min(want, p) theta of the reduced pencil; vectors = 1
+ *                       keeps its eigenvectors for the back-transform
+ *   amls_backtransform  backtransform + un-permute + M-normalise
+ *                       (subspace_condensation.cpp:263-319, solver.cpp:
+ *                       302-311): Z (n x m, column-major, m = *m)
+ *   amls_refine         FP64 refinement of the back-transformed basis
+ *                       (amls_options.refine / refineTol / refineMaxIter of
+ *                       the analysis) to the lowest nev eigenpairs
+ * amls_tree gives the analysed forest's node count, parents, sizes and
+ * levels (node ids as in k_node; arrays NULL to skip). */
+int amls_eliminate(amls_handle h, const double* k_val, const double* m_val, int32_t values_on_device);
+int amls_condense(amls_handle h, int32_t mode, int64_t k, double lambda_cut, int64_t* p);
+int amls_pass_modes(amls_handle h, int32_t* k_node, double* mu);
+int amls_reduced_eig(amls_handle h, int64_t want, int32_t vectors, double* theta, int64_t* m);
+int amls_backtransform(amls_handle h, double* Z, int32_t outputs_on_device, int64_t* m);
+int amls_refine(amls_handle h, int64_t nev, double* theta, double* Z, int32_t outputs_on_device,
+                int64_t* iters);
+int amls_tree(amls_handle h, int64_t* n_nodes, int64_t* parent, int64_t* size, int32_t* level);
+
 /* Diagnostics of the last analysis/solve on the handle:
  *   info[0] tree nodes, [1] levels, [2] p of pass A, [3] p of the final pass,
  *   [4] sum of front sizes (doubles), [5] device bytes in use,
