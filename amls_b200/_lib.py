@@ -40,7 +40,7 @@ EXPORTS = [
     "amls_sygvx_lowest_noalloc", "amls_sensitivities", "amls_permutation", "amls_solve_batch",
     "amls_analyze_batch", "amls_solve_values_batch", "amls_mm_read", "amls_mm_write",
     "amls_eliminate", "amls_condense", "amls_pass_modes", "amls_reduced_eig", "amls_backtransform",
-    "amls_refine", "amls_tree",
+    "amls_refine", "amls_tree", "amls_element_pattern", "amls_hex_assemble",
 ]
 NOALLOC_MAX_N = 128
 
@@ -97,6 +97,9 @@ def lib() -> C.CDLL:
         L.amls_backtransform.argtypes = [P, P, C.c_int32, C.POINTER(C.c_int64)]
         L.amls_refine.argtypes = [P, C.c_int64, P, P, C.c_int32, C.POINTER(C.c_int64)]
         L.amls_tree.argtypes = [P, C.POINTER(C.c_int64), P, P, P]
+        L.amls_element_pattern.argtypes = [C.c_int64, C.c_int64, C.c_int32, P, C.POINTER(C.c_int64), P, P]
+        L.amls_hex_assemble.argtypes = [P, C.c_int32, C.c_int64, C.c_int64, P, P, P, P, P, C.c_double, C.c_int64,
+                                        P, P, P, P, C.c_int32]
         L.amls_mm_read.argtypes = [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P]
         L.amls_mm_write.argtypes = [C.c_char_p, C.c_int64, P, P, P]
         L.amls_solve_batch.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, C.POINTER(Options), P, P, P, P]

@@ -42,6 +42,11 @@ class Pencil:
     E: np.ndarray | None = None        # (nelem,) element moduli
     rho: np.ndarray | None = None      # (nelem,) element densities
     name: str = ""
+    # mesh geometry (hex pencils only): node coordinates, element node ids
+    coords: np.ndarray | None = None   # (nnodes, 3)
+    enodes: np.ndarray | None = None   # (nelem, (order+1)^3) int64
+    order: int = 0
+    nu: float = 0.3
 
     @property
     def n(self) -> int:
@@ -244,6 +249,12 @@ def hex_pencil(ex: int, ey: int, ez: int, order: int, seed: int = 0,
     gj = p * eY[:, None] + loc_b[None, :]
     gk = p * eZ[:, None] + loc_c[None, :]
     enodes = gi + nx * (gj + ny * gk)                      # (nelem, nn)
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    coords = np.zeros((nx * ny * nz, 3))
+    gid = (ii + nx * (jj + ny * kk)).ravel()
+    coords[gid, 0] = ii.ravel() * (h / p)
+    coords[gid, 1] = jj.ravel() * (h / p)
+    coords[gid, 2] = kk.ravel() * (h / p)
     fn = fidx[enodes]                                       # -1 where clamped
     dofmap = np.where(fn[:, :, None] >= 0, 3 * fn[:, :, None] + np.arange(3)[None, None, :], -1)
     dofmap = dofmap.reshape(fn.shape[0], -1)                # DOF = 3*local_node + comp
@@ -257,7 +268,8 @@ def hex_pencil(ex: int, ey: int, ez: int, order: int, seed: int = 0,
     K = _assemble(dofmap, Kbar, E, n)
     M = _assemble(dofmap, Mbar, rho, n)
     name = f"hex{8 if order == 1 else 27}:{ex}x{ey}x{ez}:seed{seed}"
-    return Pencil(K, M, dofmap=dofmap, Kbar=Kbar, Mbar=Mbar, E=E, rho=rho, name=name)
+    return Pencil(K, M, dofmap=dofmap, Kbar=Kbar, Mbar=Mbar, E=E, rho=rho, name=name, coords=coords,
+                  enodes=enodes.astype(np.int64), order=order, nu=nu)
 
 
 def _assemble(dofmap: np.ndarray, Ae: np.ndarray, scale: np.ndarray, n: int) -> sp.csr_matrix:

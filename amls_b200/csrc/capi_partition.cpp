@@ -1,5 +1,7 @@
 // C ABI: host-only entry points (options, errors, partition).
+#include <algorithm>
 #include <cstring>
+#include <vector>
 #include <exception>
 #include <stdexcept>
 #include <string>
@@ -65,6 +67,43 @@ extern "C" int amls_partition(int64_t n, const int64_t* kp, const int32_t* kc, c
             for (int64_t v : nd.indices) idx[acc++] = v;
         }
         idx_ptr[N] = acc;
+        return AMLS_OK;
+    });
+}
+
+// CSR pattern of an element mesh: the union of the element DOF cliques
+// (free DOFs only), columns sorted.  Two calls: rowptr / col NULL sets *nnz.
+extern "C" int amls_element_pattern(int64_t n, int64_t nelem, int32_t ndofe, const int64_t* dofmap, int64_t* nnz,
+                                    int64_t* rowptr, int32_t* col) {
+    return guarded([&]() -> int {
+        if (n <= 0 || nelem < 0 || ndofe <= 0 || !dofmap || !nnz)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "amls_element_pattern: bad argument");
+        std::vector<std::vector<int32_t>> rows(static_cast<size_t>(n));
+        for (int64_t e = 0; e < nelem; ++e) {
+            const int64_t* d = dofmap + e * ndofe;
+            for (int32_t a = 0; a < ndofe; ++a) {
+                if (d[a] < 0) continue;
+                if (d[a] >= n) return fail(AMLS_ERR_INVALID_ARGUMENT, "amls_element_pattern: DOF out of range");
+                auto& r = rows[static_cast<size_t>(d[a])];
+                for (int32_t b = 0; b < ndofe; ++b)
+                    if (d[b] >= 0) r.push_back(static_cast<int32_t>(d[b]));
+            }
+        }
+        int64_t tot = 0;
+        for (auto& r : rows) {
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
+            tot += static_cast<int64_t>(r.size());
+        }
+        *nnz = tot;
+        if (rowptr && col) {
+            int64_t q = 0;
+            rowptr[0] = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                for (int32_t c : rows[static_cast<size_t>(i)]) col[q++] = c;
+                rowptr[i + 1] = q;
+            }
+        }
         return AMLS_OK;
     });
 }

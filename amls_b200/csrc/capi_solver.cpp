@@ -205,6 +205,20 @@ extern "C" int amls_tree(amls_handle h, int64_t* n_nodes, int64_t* parent, int64
     });
 }
 
+extern "C" int amls_hex_assemble(amls_handle h, int32_t order, int64_t nelem, int64_t nnodes, const double* coords,
+                                 const int64_t* enodes, const int64_t* dofmap, const double* E, const double* rho,
+                                 double nu, int64_t n, const int64_t* rowptr, const int32_t* col, double* k_val,
+                                 double* m_val, int32_t outputs_on_device) {
+    return guarded([&]() -> int {
+        if (int e = checkHandle(h)) return e;
+        if (!coords || !enodes || !dofmap || !E || !rho || !rowptr || !col || !k_val || !m_val)
+            return fail(AMLS_ERR_INVALID_ARGUMENT, "null argument");
+        h->eng->assembleHex(order, nelem, nnodes, coords, enodes, dofmap, E, rho, nu, n, rowptr, col, k_val, m_val,
+                            outputs_on_device != 0);
+        return AMLS_OK;
+    });
+}
+
 extern "C" int amls_info(amls_handle h, int64_t* info) {
     return guarded([&]() -> int {
         if (int e = checkHandle(h)) return e;

@@ -1888,6 +1888,61 @@ void Engine::sensitivities(int64_t nelem, int nd, const int64_t* dofmap, int32_t
 }
 
 
+void Engine::assembleHex(int order, int64_t nelem, int64_t nnodes, const double* coords, const int64_t* enodes,
+                         const int64_t* dofmap, const double* E, const double* rho, double nu, int64_t n,
+                         const int64_t* rowptr, const int32_t* col, double* kval, double* mval,
+                         bool outputsOnDevice) {
+    if (order != 1 && order != 2) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element order must be 1 or 2");
+    if (nelem <= 0 || nnodes <= 0 || n <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty mesh");
+    const int nn = (order + 1) * (order + 1) * (order + 1), nd = 3 * nn;
+    for (int64_t q = 0; q < nelem * nn; ++q)
+        if (enodes[q] < 0 || enodes[q] >= nnodes) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element node id out of range");
+    for (int64_t q = 0; q < nelem * nd; ++q)
+        if (dofmap[q] < -1 || dofmap[q] >= n) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "dofmap entry out of range");
+    const int64_t nnz = rowptr[n];
+    cudaCheck(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t s = stream_;
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+        b.ensure(bytes);
+        cudaCheck(cudaMemcpyAsync(b.as<char>(), src, bytes, cudaMemcpyHostToDevice, s), "assembly upload");
+    };
+    up(asmCoords_, coords, sizeof(double) * nnodes * 3);
+    up(asmEnodes_, enodes, sizeof(int64_t) * nelem * nn);
+    up(asmDof_, dofmap, sizeof(int64_t) * nelem * nd);
+    up(asmE_, E, sizeof(double) * nelem);
+    up(asmRho_, rho, sizeof(double) * nelem);
+    up(asmRp_, rowptr, sizeof(int64_t) * (n + 1));
+    up(asmCol_, col, sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+    double* kd = outputsOnDevice ? kval : static_cast<double*>(asmK_.ensure(sizeof(double) * std::max<int64_t>(nnz, 1)));
+    double* md = outputsOnDevice ? mval : static_cast<double*>(asmM_.ensure(sizeof(double) * std::max<int64_t>(nnz, 1)));
+    cudaCheck(cudaMemsetAsync(status_.as<int>(), 0, 2 * sizeof(int), s), "status");
+    HexAssembleArgs a{};
+    a.order = order;
+    a.nelem = nelem;
+    a.coords = asmCoords_.as<double>();
+    a.enodes = asmEnodes_.as<int64_t>();
+    a.dofmap = asmDof_.as<int64_t>();
+    a.E = asmE_.as<double>();
+    a.rho = asmRho_.as<double>();
+    a.nu = nu;
+    a.rowptr = asmRp_.as<int64_t>();
+    a.col = asmCol_.as<int32_t>();
+    a.nnz = nnz;
+    a.kval = kd;
+    a.mval = md;
+    a.status = status_.as<int>();
+    LAUNCH(launchHexAssemble(a, s));
+    int h[2] = {0, 0};
+    cudaCheck(cudaMemcpyAsync(h, status_.as<int>(), sizeof(h), cudaMemcpyDeviceToHost, s), "status");
+    if (!outputsOnDevice) {
+        cudaCheck(cudaMemcpyAsync(kval, kd, sizeof(double) * nnz, cudaMemcpyDeviceToHost, s), "K values");
+        cudaCheck(cudaMemcpyAsync(mval, md, sizeof(double) * nnz, cudaMemcpyDeviceToHost, s), "M values");
+    }
+    cudaCheck(cudaStreamSynchronize(s), "assembly");
+    if (h[0] == kDevBadPattern)
+        throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "element " + std::to_string(h[1]) + " couples DOFs the CSR pattern lacks");
+}
+
 void Engine::finalizeVectors(const double* zt, int64_t ldz, int m, cudaStream_t s) {
     norms_.ensure(sizeof(double) * static_cast<size_t>(m) * nPencils_);
     zOut_.ensure(sizeof(double) * static_cast<size_t>(m * n_));

@@ -77,6 +77,10 @@ public:
                        const int32_t* elemType, const double* Kbar,
                        const double* Mbar, const double* weights, double gapTol, double* gE,
                        double* gRho, double* dE, double* dRho, int32_t* simple);
+    // hex elasticity pencil values assembled on the GPU (assemble.cu)
+    void assembleHex(int order, int64_t nelem, int64_t nnodes, const double* coords, const int64_t* enodes,
+                     const int64_t* dofmap, const double* E, const double* rho, double nu, int64_t n,
+                     const int64_t* rowptr, const int32_t* col, double* kval, double* mval, bool outputsOnDevice);
     void info(int64_t* out) const;
     // permutation of the last analysis (perm[new] = old, n entries)
     void permutation(int64_t* out) const;
@@ -312,6 +316,7 @@ private:
     std::vector<double> lastTheta_;                // eigenvalues of the last solve
     bool lastHasVectors_ = false;
     DevBuf senDof_, senEl_, senOut_, senType_;
+    DevBuf asmCoords_, asmEnodes_, asmDof_, asmE_, asmRho_, asmRp_, asmCol_, asmK_, asmM_;
 
     // kernel profiling
     bool profiling_ = false;

@@ -14,6 +14,7 @@ enum DevStatus : int {
     kDevNotSpd = 1,      // non-positive or NaN pivot
     kDevIterCap = 2,     // iteration cap reached
     kDevTimeout = 3,     // a bounded wait on the tensor cores ran out
+    kDevBadPattern = 4,  // an element entry missing from the given CSR pattern
 };
 
 // ---------------------------------------------------------------- GEMM --
@@ -311,6 +312,28 @@ cudaError_t launchSensitivity(int64_t nelem, int nd, const int64_t* dofmap, cons
                               const double* Mbar, const double* X, int64_t n, int nmodes,
                               const double* lambda, const double* weight, double* gE,
                               double* gRho, double* dE, double* dRho, cudaStream_t s);
+// Hex elasticity assembly on the GPU (assemble.cu): element matrices of
+// isoparametric 8-node (order 1) or 27-node (order 2) hexahedra scaled by
+// E[e] / rho[e] and summed into the CSR values kval / mval (nnz each, zeroed
+// first) of the pattern rowptr / col (device arrays, sorted columns).
+struct HexAssembleArgs {
+    int32_t order, pad;
+    int64_t nelem;
+    const double* coords;      // node coordinates (3 per node)
+    const int64_t* enodes;     // nelem x nn node ids
+    const int64_t* dofmap;     // nelem x 3 nn global DOFs (-1 constrained)
+    const double* E;
+    const double* rho;
+    double nu;
+    const int64_t* rowptr;
+    const int32_t* col;
+    int64_t nnz;
+    double* kval;
+    double* mval;
+    int* status;               // kDevBadPattern when an entry is missing
+};
+cudaError_t launchHexAssemble(const HexAssembleArgs& a, cudaStream_t s);
+
 // out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
 cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
                          double c, const double* z, double* out, cudaStream_t s);

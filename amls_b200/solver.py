@@ -110,6 +110,19 @@ def write_matrix_market(path: str, A) -> None:
                                         _lib.ptr(v)))
 
 
+def element_pattern(n: int, dofmap: np.ndarray):
+    """CSR pattern (rowptr, col) of an element mesh (amls_element_pattern)."""
+    dm = np.ascontiguousarray(dofmap, dtype=np.int64)
+    nnz = C.c_int64(0)
+    _lib.check(_lib.lib().amls_element_pattern(int(n), dm.shape[0], dm.shape[1], _lib.ptr(dm), C.byref(nnz),
+                                               None, None))
+    rp = np.zeros(n + 1, np.int64)
+    ci = np.zeros(max(nnz.value, 1), np.int32)
+    _lib.check(_lib.lib().amls_element_pattern(int(n), dm.shape[0], dm.shape[1], _lib.ptr(dm), C.byref(nnz),
+                                               _lib.ptr(rp), _lib.ptr(ci)))
+    return rp, ci[:nnz.value]
+
+
 def recursive_bisection(K, M, nLevels: int, leafSize: int):
     """Partition of |K| + |M|: returns (perm, tree arrays dict)."""
     kp, kc, _ = _csr_arrays(K)
@@ -308,6 +321,33 @@ class AmlsSolver:
         level = np.zeros(N, np.int32)
         _lib.check(_lib.lib().amls_tree(self._h, C.byref(nn), _lib.ptr(parent), _lib.ptr(size), _lib.ptr(level)))
         return dict(parent=parent, size=size, level=level)
+
+    def assemble_hex(self, pencil, rowptr, col, on_device: bool = False, k_ptr: int = 0, m_ptr: int = 0):
+        """K and M values of a hex pencil's mesh assembled on the GPU in the
+        pattern (rowptr, col): host arrays returned, or written to the device
+        pointers k_ptr / m_ptr with on_device."""
+        coords = np.ascontiguousarray(pencil.coords, dtype=np.float64)
+        en = np.ascontiguousarray(pencil.enodes, dtype=np.int64)
+        dm = np.ascontiguousarray(pencil.dofmap, dtype=np.int64)
+        E = np.ascontiguousarray(pencil.E, dtype=np.float64)
+        rho = np.ascontiguousarray(pencil.rho, dtype=np.float64)
+        rp = np.ascontiguousarray(rowptr, dtype=np.int64)
+        ci = np.ascontiguousarray(col, dtype=np.int32)
+        n = rp.size - 1
+        if on_device:
+            kv, mv = C.c_void_p(k_ptr), C.c_void_p(m_ptr)
+        else:
+            kh = np.zeros(max(ci.size, 1))
+            mh = np.zeros(max(ci.size, 1))
+            kv, mv = _lib.ptr(kh), _lib.ptr(mh)
+        _lib.check(_lib.lib().amls_hex_assemble(self._h, int(pencil.order), en.shape[0], coords.shape[0],
+                                                _lib.ptr(coords), _lib.ptr(en), _lib.ptr(dm), _lib.ptr(E),
+                                                _lib.ptr(rho), float(pencil.nu), n, _lib.ptr(rp), _lib.ptr(ci),
+                                                kv, mv, 1 if on_device else 0))
+        if on_device:
+            return None
+        return (sp.csr_matrix((kh[:ci.size], ci, rp), shape=(n, n)),
+                sp.csr_matrix((mh[:ci.size], ci, rp), shape=(n, n)))
 
     def sensitivities(self, pencil, weights=None, per_mode: bool = False, gap_tol: float = 1e-6,
                       elem_type=None):

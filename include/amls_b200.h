@@ -145,6 +145,30 @@ int amls_mm_read(const char* path, int64_t* n, int64_t* nnz, int64_t* rowptr, in
 int amls_mm_write(const char* path, int64_t n, const int64_t* rowptr, const int32_t* col,
                   const double* val);
 
+/* CSR pattern of an element mesh (host only): the union over elements of
+ * the cliques of their free DOFs (dofmap[nelem * ndofe], -1 constrained),
+ * columns sorted.  Two calls: with rowptr / col NULL it sets *nnz; then with
+ * arrays of n+1 / nnz entries it fills them. */
+int amls_element_pattern(int64_t n, int64_t nelem, int32_t ndofe, const int64_t* dofmap, int64_t* nnz,
+                         int64_t* rowptr, int32_t* col);
+
+/* Hex elasticity pencil assembled on the GPU (no counterpart in the
+ * reference, whose pencils come from files or graph-Laplacian generators):
+ * isoparametric 8-node (order 1) or 27-node (order 2) hexahedra with nodal
+ * coordinates coords[nnodes * 3] and node ids enodes[nelem * (order+1)^3]
+ * (local node a0 + (order+1)(a1 + (order+1) a2) along x, y, z), isotropic
+ * elasticity with modulus E[e] and Poisson ratio nu, consistent mass with
+ * density rho[e], Gauss-Legendre quadrature with order + 1 points per
+ * direction; DOF 3 a + component mapped by dofmap[nelem * 3 nn] (-1
+ * constrained).  The values of K and M in the CSR pattern rowptr / col (host
+ * arrays, e.g. from amls_element_pattern) are written to k_val / m_val:
+ * device arrays of nnz doubles with outputs_on_device = 1 (ready for
+ * amls_solve_values), host arrays otherwise. */
+int amls_hex_assemble(amls_handle h, int32_t order, int64_t nelem, int64_t nnodes, const double* coords,
+                      const int64_t* enodes, const int64_t* dofmap, const double* E, const double* rho,
+                      double nu, int64_t n, const int64_t* rowptr, const int32_t* col, double* k_val,
+                      double* m_val, int32_t outputs_on_device);
+
 /* Whole AMLS solve from host CSR arrays.  Replaces AmlsSolver::solve
  * (src/amls/solver.cpp:100-319): optional shift, partition + permutation,
  * two-pass truncation (k0 = max(4, ceil(3 nev / N)), lambda_cut = eta *
