@@ -227,7 +227,10 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
         if (nb <= 0) throw AmlsError(AMLS_ERR_INVALID_ARGUMENT, "empty pencil in the batch");
         PartitionResult pr;
         if (P == 1) {
-            pr = recursiveBisection(n, kp, kc, mp, mc, opt.nLevels, opt.leafSize, opt.numThreads);
+            // the graph of |K| + |M| extracted on the GPU, METIS on the host
+            std::vector<int64_t> xadj, adj;
+            extractGraphDevice(n, kp, kc, mp, mc, xadj, adj);
+            pr = recursiveBisectionGraph(n, std::move(xadj), std::move(adj), opt.nLevels, opt.leafSize, opt.numThreads);
         } else {
             // the pencil's diagonal block with local indices
             std::vector<int64_t> bkp(static_cast<size_t>(nb + 1)), bmp(static_cast<size_t>(nb + 1));
@@ -523,6 +526,40 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
                      "[amls_b200] analyze: partition %.3f s, symbolic + layout %.3f s, CSR maps %.3f s, "
                      "uploads %.3f s, launch tables %.3f s\n",
                      secs(ta0, ta1), secs(ta1, ta2), secs(ta2, ta3), secs(ta3, ta4), secs(ta4, Clock::now()));
+}
+
+// adjacency of |K| + |M| without self loops, neighbour lists sorted (the
+// partition's input graph), built on the GPU from the CSR patterns
+void Engine::extractGraphDevice(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
+                                const int32_t* mc, std::vector<int64_t>& xadj, std::vector<int64_t>& adj) {
+    cudaStream_t s = stream_;
+    DevBuf dkp, dkc, dmp, dmc, dcnt, dadj;
+    const int64_t nk = kp[n], nm = mp[n];
+    dkp.ensure(sizeof(int64_t) * (n + 1));
+    dmp.ensure(sizeof(int64_t) * (n + 1));
+    dkc.ensure(sizeof(int32_t) * std::max<int64_t>(nk, 1));
+    dmc.ensure(sizeof(int32_t) * std::max<int64_t>(nm, 1));
+    dcnt.ensure(sizeof(int64_t) * (n + 1));
+    cudaCheck(cudaMemcpyAsync(dkp.as<int64_t>(), kp, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s), "graph");
+    cudaCheck(cudaMemcpyAsync(dmp.as<int64_t>(), mp, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s), "graph");
+    cudaCheck(cudaMemcpyAsync(dkc.as<int32_t>(), kc, sizeof(int32_t) * nk, cudaMemcpyHostToDevice, s), "graph");
+    cudaCheck(cudaMemcpyAsync(dmc.as<int32_t>(), mc, sizeof(int32_t) * nm, cudaMemcpyHostToDevice, s), "graph");
+    LAUNCH(launchGraphCount(n, dkp.as<int64_t>(), dkc.as<int32_t>(), dmp.as<int64_t>(), dmc.as<int32_t>(),
+                            dcnt.as<int64_t>(), s));
+    std::vector<int64_t> cnt(static_cast<size_t>(n));
+    cudaCheck(cudaMemcpyAsync(cnt.data(), dcnt.as<int64_t>(), sizeof(int64_t) * n, cudaMemcpyDeviceToHost, s), "graph");
+    cudaCheck(cudaStreamSynchronize(s), "graph");
+    xadj.assign(static_cast<size_t>(n) + 1, 0);
+    for (int64_t v = 0; v < n; ++v) xadj[static_cast<size_t>(v) + 1] = xadj[static_cast<size_t>(v)] + cnt[static_cast<size_t>(v)];
+    cudaCheck(cudaMemcpyAsync(dcnt.as<int64_t>(), xadj.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s),
+              "graph");
+    dadj.ensure(sizeof(int64_t) * std::max<int64_t>(xadj.back(), 1));
+    LAUNCH(launchGraphFill(n, dkp.as<int64_t>(), dkc.as<int32_t>(), dmp.as<int64_t>(), dmc.as<int32_t>(),
+                           dcnt.as<int64_t>(), dadj.as<int64_t>(), s));
+    adj.resize(static_cast<size_t>(xadj.back()));
+    cudaCheck(cudaMemcpyAsync(adj.data(), dadj.as<int64_t>(), sizeof(int64_t) * adj.size(), cudaMemcpyDeviceToHost, s),
+              "graph");
+    cudaCheck(cudaStreamSynchronize(s), "graph");
 }
 
 void Engine::buildStatic() {

@@ -129,6 +129,8 @@ private:
 
     using Clock = std::chrono::steady_clock;
     Clock::time_point numericElimination(const double* kv, const double* mv, bool valuesOnDevice, cudaStream_t s);
+    void extractGraphDevice(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc,
+                            std::vector<int64_t>& xadj, std::vector<int64_t>& adj);
     void buildStatic();
     void eliminate(cudaStream_t s);
     void eliminateLaunches(cudaStream_t s);

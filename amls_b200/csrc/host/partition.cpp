@@ -418,9 +418,18 @@ int64_t buildTree(SeparatorTree& tree, Split& s) {
 PartitionResult recursiveBisection(int64_t n, const int64_t* kRowPtr, const int32_t* kCol,
                                    const int64_t* mRowPtr, const int32_t* mCol, int nLevels,
                                    int64_t leafSize, int numThreads) {
+    if (n == 0) return PartitionResult();
+    Csr g = extractGraph(n, kRowPtr, kCol, mRowPtr, mCol);
+    return recursiveBisectionGraph(n, std::move(g.xadj), std::move(g.adjncy), nLevels, leafSize, numThreads);
+}
+
+PartitionResult recursiveBisectionGraph(int64_t n, std::vector<int64_t>&& xadj, std::vector<int64_t>&& adjncy,
+                                        int nLevels, int64_t leafSize, int numThreads) {
     PartitionResult res;
     if (n == 0) return res;
-    const Csr g = extractGraph(n, kRowPtr, kCol, mRowPtr, mCol);
+    Csr g;
+    g.xadj = std::move(xadj);
+    g.adjncy = std::move(adjncy);
     std::vector<int64_t> all(static_cast<size_t>(n));
     std::iota(all.begin(), all.end(), 0);
     int threads = numThreads > 0 ? numThreads : static_cast<int>(std::thread::hardware_concurrency());

@@ -56,5 +56,9 @@ PartitionResult recursiveBisection(int64_t n,
                                    const int64_t* kRowPtr, const int32_t* kCol,
                                    const int64_t* mRowPtr, const int32_t* mCol,
                                    int nLevels, int64_t leafSize, int numThreads = 0);
+// The same from the graph of |K| + |M| without self loops (neighbour lists
+// sorted), e.g. extracted on the GPU.
+PartitionResult recursiveBisectionGraph(int64_t n, std::vector<int64_t>&& xadj, std::vector<int64_t>&& adjncy,
+                                        int nLevels, int64_t leafSize, int numThreads = 0);
 
 }  // namespace amls_b200

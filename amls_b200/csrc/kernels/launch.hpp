@@ -334,6 +334,13 @@ struct HexAssembleArgs {
 };
 cudaError_t launchHexAssemble(const HexAssembleArgs& a, cudaStream_t s);
 
+// Graph of |K| + |M| without self loops (graph.cu), neighbour lists sorted:
+// cnt[v] = degree, then with xadj = prefix sums of cnt, the lists in adj.
+cudaError_t launchGraphCount(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc,
+                             int64_t* cnt, cudaStream_t s);
+cudaError_t launchGraphFill(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp, const int32_t* mc,
+                            const int64_t* xadj, int64_t* adj, cudaStream_t s);
+
 // out = a*x + b*y + c*z (z may be null), elementwise over n doubles.
 cudaError_t launchAxpby3(int64_t n, double a, const double* x, double b, const double* y,
                          double c, const double* z, double* out, cudaStream_t s);

@@ -335,3 +335,14 @@ def test_c2_per_eigenvalue_error_against_exact(solver, precision):
     assert residuals(p.K, p.M, ref.theta, ref.Z).max() < 1e-6
     mn = np.einsum("ij,ij->j", ref.Z, p.M @ ref.Z)
     assert np.allclose(mn, 1.0, atol=1e-12)
+
+
+def test_device_graph_partition_equals_host_partition(solver):
+    """The engine builds the graph of |K| + |M| on the GPU for METIS; the
+    permutation equals the host partitioner's on the same pencil."""
+    from amls_b200.solver import recursive_bisection
+    for p, L, leaf in ((cases.config_pencil("C1"), 4, 500), (cases.grid_graph_2d(40, 30), 4, 150),
+                       (cases.hex_pencil(5, 6, 4, 2, seed=2), 5, 300)):
+        perm, _ = recursive_bisection(p.K, p.M, L, leaf)
+        solver.analyze(p.K, p.M, AmlsOptions(nev=5, nLevels=L, leafSize=leaf))
+        assert np.array_equal(solver.permutation(), perm)
