@@ -21,14 +21,22 @@ import scipy.sparse as sp
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "amls_cpu.cpp")
 LIB = os.path.join(HERE, "libamls_cpu.so")
+METIS_SRC = os.path.join(HERE, "metis_seq.cpp")
+METIS_LIB = os.path.join(HERE, "libmetis_seq.so")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+METIS_A = os.path.join(CUDA, "targets", "x86_64-linux", "lib", "libmetis_static.a")
 
 
 def build() -> str:
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
-        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", SRC, "-o", LIB, "-ldl", "-lpthread"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"oracle build failed: {' '.join(cmd)}\n{r.stderr}")
+    """Both oracle libraries: the C++ restatement of the AMLS algorithm and
+    the sequential restatement of the reference's nested dissection (linked
+    with the METIS library of the CUDA toolkit)."""
+    for src, lib, extra in ((SRC, LIB, ["-ldl", "-lpthread"]), (METIS_SRC, METIS_LIB, [METIS_A, "-lm"])):
+        if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(src):
+            cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", src, "-o", lib, *extra]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"oracle build failed: {' '.join(cmd)}\n{r.stderr}")
     return LIB
 
 
@@ -87,3 +95,38 @@ def solve(K, M, tree: dict, nev: int, eta: float = 2.0, fixed_keep: int = 0, vec
         raise RuntimeError(err.value.decode())
     keys = ["permutation", "elimination", "condensation", "reduced", "backtransform", "total"]
     return theta, (None if Z is None else Z.T.copy()), int(p.value), int(pa.value), dict(zip(keys, tm.tolist()))
+
+
+def sequential_partition(K, M, n_levels: int, leaf_size: int):
+    """The reference's MetisPartitioner::recursiveBisection restated
+    sequentially (oracle/metis_seq.cpp, with its METIS_PartGraphRecursive
+    call): (perm, tree arrays) as amls_b200.solver.recursive_bisection."""
+    build()
+    L = C.CDLL(METIS_LIB)
+    P = C.c_void_p
+    L.metis_seq_partition.argtypes = [C.c_int64, P, P, P, P, C.c_int, C.c_int64, P, P, P, P, P, P, P, P]
+    K = sp.csr_matrix(K)
+    M = sp.csr_matrix(M)
+    K.sort_indices()
+    M.sort_indices()
+    n = K.shape[0]
+    kp = np.ascontiguousarray(K.indptr, np.int64)
+    kc = np.ascontiguousarray(K.indices, np.int32)
+    mp = np.ascontiguousarray(M.indptr, np.int64)
+    mc = np.ascontiguousarray(M.indices, np.int32)
+    perm = np.zeros(n, np.int64)
+    nn = C.c_int64(0)
+    parent = np.zeros(n, np.int64)
+    role = np.zeros(n, np.int32)
+    left = np.zeros(n, np.int64)
+    right = np.zeros(n, np.int64)
+    ip = np.zeros(n + 1, np.int64)
+    ix = np.zeros(n, np.int64)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)   # noqa: E731
+    rc = L.metis_seq_partition(n, ptr(kp), ptr(kc), ptr(mp), ptr(mc), int(n_levels), int(leaf_size), ptr(perm),
+                               C.byref(nn), ptr(parent), ptr(role), ptr(left), ptr(right), ptr(ip), ptr(ix))
+    if rc != 0:
+        raise RuntimeError("METIS failed")
+    N = nn.value
+    return perm, dict(parent=parent[:N].copy(), role=role[:N].copy(), left=left[:N].copy(),
+                      right=right[:N].copy(), idx_ptr=ip[:N + 1].copy(), idx=ix.copy())

@@ -5,6 +5,7 @@ with 2-8 leaves at 3 levels, perm[new] = old with post-order segments,
 permuted diagonal blocks equal the original ones; plus determinism.
 """
 import numpy as np
+import pytest
 
 from amls_b200 import cases, recursive_bisection
 from oracle import amls_ref as R
@@ -78,3 +79,26 @@ def test_partition_deterministic_and_leaf_rule():
     assert len(t["parent"]) == 1 and np.array_equal(perm, np.arange(40))
     tree = Tree.from_arrays(**t)
     assert tree.role[0] == LEAF
+
+
+@pytest.mark.parametrize("case", ["C1", "C2", "grid", "hexbox"])
+def test_parallel_partition_equals_sequential_restatement(case):
+    """The parallel partitioner (adjacency built per vertex in parallel, the
+    unread METIS_PartGraphRecursive call dropped, concurrent subtrees in
+    worker processes) returns the same permutation and tree as a literal
+    sequential restatement of metis_partitioner.cpp that keeps every call
+    (oracle/metis_seq.cpp)."""
+    from amls_b200 import cases
+    from amls_b200.solver import recursive_bisection
+    from oracle import cpu
+    p, L, leaf = {
+        "C1": (cases.config_pencil("C1"), 4, 500),
+        "C2": (cases.config_pencil("C2"), 6, 500),
+        "grid": (cases.grid_graph_2d(64, 64), 4, 1000),
+        "hexbox": (cases.hex_pencil(9, 5, 7, 1, seed=3), 6, 200),
+    }[case]
+    perm, t = recursive_bisection(p.K, p.M, L, leaf)
+    perm_s, t_s = cpu.sequential_partition(p.K, p.M, L, leaf)
+    assert np.array_equal(perm, perm_s)
+    for k in ("parent", "role", "left", "right", "idx_ptr", "idx"):
+        assert np.array_equal(t[k], t_s[k]), k
