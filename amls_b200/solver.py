@@ -89,6 +89,26 @@ def _csr_arrays(A):
     return rp, ci, v
 
 
+def _block_diag(As) -> sp.csr_matrix:
+    """Block-diagonal CSR of square matrices (sorted indices, int64 row
+    pointers, int32 columns), assembled from the blocks' CSR arrays."""
+    parts = [_csr_arrays(a) for a in As]
+    n = sum(len(rp) - 1 for rp, _, _ in parts)
+    nnz = sum(int(rp[-1]) for rp, _, _ in parts)
+    rp = np.zeros(n + 1, np.int64)
+    ci = np.empty(nnz, np.int32)
+    v = np.empty(nnz, np.float64)
+    r0 = z0 = 0
+    for prp, pci, pv in parts:
+        nb, zb = len(prp) - 1, int(prp[-1])
+        rp[r0 + 1:r0 + nb + 1] = prp[1:] + z0
+        ci[z0:z0 + zb] = pci[:zb] + r0
+        v[z0:z0 + zb] = pv[:zb]
+        r0 += nb
+        z0 += zb
+    return sp.csr_matrix((v, ci, rp), shape=(n, n))
+
+
 def read_matrix_market(path: str) -> sp.csr_matrix:
     """readMatrixMarket (src/io/matrix_market.cpp:48-97) through the C ABI."""
     n = C.c_int64(0)
@@ -186,8 +206,8 @@ class AmlsSolver:
         partition and two-pass truncation), all of them level-batched on the
         GPU.  Returns a list of Solution (theta, Z per pencil; p and timing of
         the whole batch)."""
-        K = sp.block_diag([sp.csr_matrix(k) for k in Ks], format="csr")
-        M = sp.block_diag([sp.csr_matrix(m) for m in Ms], format="csr")
+        K = _block_diag(Ks)
+        M = _block_diag(Ms)
         off = np.zeros(len(Ks) + 1, np.int64)
         off[1:] = np.cumsum([k.shape[0] for k in Ks])
         kp, kc, kv = _csr_arrays(K)
@@ -216,10 +236,8 @@ class AmlsSolver:
     def analyze_batch(self, Ks, Ms, opt: AmlsOptions):
         """Pattern analysis of a batch; returns the block-diagonal (K, M) whose
         .data arrays are the value order of solve_values_batch."""
-        K = sp.block_diag([sp.csr_matrix(k) for k in Ks], format="csr")
-        M = sp.block_diag([sp.csr_matrix(m) for m in Ms], format="csr")
-        K.sort_indices()
-        M.sort_indices()
+        K = _block_diag(Ks)
+        M = _block_diag(Ms)
         off = np.zeros(len(Ks) + 1, np.int64)
         off[1:] = np.cumsum([k.shape[0] for k in Ks])
         kp, kc, _ = _csr_arrays(K)
