@@ -294,6 +294,15 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
         T.fgT = b.add(fgT); T.nfg = static_cast<int>(fgT.size());
         T.bgT = b.add(bgT); T.nbg = static_cast<int>(bgT.size());
         T.btT = b.add(btT); T.nbt = static_cast<int>(btT.size());
+        if (opt_.verbosity >= 3) {   // sweep plan: descriptors and 64 x 64 tiles per launch
+            double fTri = 0, fOff = 0;
+            for (const GemmDesc& g : ft) fTri += 1.0 * g.M * g.N * g.K;
+            for (const GemmDesc& g : fg) fOff += 2.0 * g.M * g.N * g.K;
+            std::fprintf(stderr,
+                         "[amls_b200] sweep level %d: nodes %zu tri tiles %d (%.3g flop) off-diagonal "
+                         "descs %zu tiles %d/%d (%.3g flop)\n",
+                         l, ft.size(), T.nft, fTri, fg.size(), T.nfg, T.nbg, fOff);
+        }
     }
     const size_t oSweep = b.add(sweep);
     // Rayleigh-Ritz products: Kc = X R^T, Mc = X MX^T (split-K over n), Q = Vc^T X

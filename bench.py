@@ -214,14 +214,12 @@ def run_ours(args, rank, world, dist):
 
     # accuracy of the timed solve's eigenvalues against the exact golden
     accuracy = {}
-    gold = os.path.join(ROOT, "tests", "golden", "c5_exact.npz")
     th = theta.cpu().numpy()
-    if args.config == "C5" and os.path.exists(gold):
-        ex = np.load(gold)["theta"][:nev]
+    ex, gname = exact_eigenvalues(args.config, nev)
+    if ex is not None:
         accuracy["max_rel_err_vs_exact"] = float(np.max(np.abs(th - ex) / ex))
         accuracy["median_rel_err_vs_exact"] = float(np.median(np.abs(th - ex) / ex))
-        accuracy["exact_reference"] = ("shift-invert Lanczos (scipy ARPACK, sigma 0, tol 1e-13), "
-                                       "tests/golden/c5_exact.npz")
+        accuracy["exact_reference"] = f"shift-invert Lanczos (scipy ARPACK, sigma 0), tests/golden/{gname}"
     # the other precision arm, same protocol (the metric compares the two)
     other = None
     if not args.no_compare:
@@ -241,7 +239,7 @@ def run_ours(args, rank, world, dist):
             t3.append(step3()["device"])
         o_step = max_over_ranks(float(np.mean(t3)), dist)
         other = {"precision": oprec, "s": o_step}
-        if args.config == "C5" and os.path.exists(gold):
+        if ex is not None:
             th3 = theta.cpu().numpy()
             other["max_rel_err_vs_exact"] = float(np.max(np.abs(th3 - ex) / ex))
         other["speedup_of_" + args.precision] = o_step / t_step
@@ -328,7 +326,7 @@ def run_ours(args, rank, world, dist):
     }
     if not args.no_batch:
         line["batch_c3"] = run_batch(args, rank, world, dist)
-    if rank == 0 and world == 1 and not args.no_cpu and args.config == "C5":
+    if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(args)
     return line
 
@@ -392,6 +390,16 @@ def run_batch(args, rank, world, dist):
     return out
 
 
+def exact_eigenvalues(config, nev):
+    """Exact lowest eigenvalues of a workload from its golden file."""
+    name, key = {"C1": ("c1_exact.npz", "theta"), "C2": ("c2_exact.npz", "theta"),
+                 "C4": ("c4_grad.npz", "lam"), "C5": ("c5_exact.npz", "theta")}[config]
+    path = os.path.join(ROOT, "tests", "golden", name)
+    if not os.path.exists(path):
+        return None, name
+    return np.load(path)[key][:nev], name
+
+
 def fp64_gemm_peak():
     """cuBLAS DGEMM throughput on this GPU now (8192^3, best of 3), TFLOP/s."""
     import torch
@@ -444,18 +452,18 @@ def c5_tree():
     return {k: g[k].astype(np.int64) for k in ("parent", "left", "right", "idx_ptr", "idx")}
 
 
-def cpu_full_solve(p, tree, threads):
-    """One full C5 AMLS solve (nev 500, eta 2, elimination per pass, vectors)
-    by the C++ restatement of the reference algorithm, timed on the host."""
+def cpu_full_solve(p, tree, threads, nev=500):
+    """One full AMLS solve (eta 2, elimination per pass, vectors) by the C++
+    restatement of the reference algorithm, timed on the host."""
     from oracle import cpu
     t0 = time.perf_counter()
-    th, _, pp, pa, tm = cpu.solve(p.K, p.M, tree, 500, eta=2.0, vectors=True, threads=threads)
+    th, _, pp, pa, tm = cpu.solve(p.K, p.M, tree, nev, eta=2.0, vectors=True, threads=threads)
     return time.perf_counter() - t0, pp, pa, tm
 
 
-def cpu_baseline_line(t, cores, pp, pa, tm, runs):
+def cpu_baseline_line(t, cores, pp, pa, tm, runs, config="C5"):
     return {"value": t, "unit": "s", "cores": cores, "kind": "port",
-            "sample": (f"the full C5 workload ({runs} run{'s' if runs > 1 else ''}, no scaling): the "
+            "sample": (f"the full {config} workload ({runs} run{'s' if runs > 1 else ''}, no scaling): the "
                        f"reference algorithm restated in C++ (oracle/amls_cpu.cpp: elimination re-run "
                        f"per pass, dense local dsygvx, projection, reduced dsygvx, back-transform, "
                        f"M-normalisation), OpenBLAS single-threaded per call and {cores} host threads "
@@ -464,12 +472,20 @@ def cpu_baseline_line(t, cores, pp, pa, tm, runs):
 
 
 def cpu_sample(args):
-    """cpu_baseline of our arm: one full C5 run."""
+    """cpu_baseline of our arm: one full run of the workload (C5 on its
+    fixture tree; the smaller workloads on the tree of the sequential
+    restatement of the reference's partitioner, the same tree)."""
     from amls_b200 import cases
     cores = os.cpu_count() or 1
-    p = cases.config_pencil("C5", seed=0)
-    t, pp, pa, tm = cpu_full_solve(p, c5_tree(), cores)
-    return cpu_baseline_line(t, cores, pp, pa, tm, 1)
+    cfg = CONFIGS[args.config]
+    p = cases.config_pencil(args.config, seed=0)
+    if args.config == "C5":
+        tree = c5_tree()
+    else:
+        from oracle import cpu
+        tree = cpu.sequential_partition(p.K, p.M, cfg["nLevels"], 500)[1]
+    t, pp, pa, tm = cpu_full_solve(p, tree, cores, cfg["nev"])
+    return cpu_baseline_line(t, cores, pp, pa, tm, 1, args.config)
 
 
 def run_reference(args, rank, world):
@@ -506,6 +522,8 @@ def run_reference(args, rank, world):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
         "data": "synthetic (seeded hex-elasticity pencil)",
         "config": dict(workload("C5", False),
+                       precision="fp64 (the reference algorithm: LAPACK/BLAS on the host cores)",
+                       l2="not applicable (host run)",
                        steps_requested=args.steps, warmup_requested=args.warmup,
                        budget_s=budget,
                        note=("the reference algorithm stops at the AMLS Ritz values (4-13 % error "

@@ -1,7 +1,10 @@
 """Golden vectors for the precision workload (27-node hex 7^3, 9,450 DOF,
-nev 100) and the differentiation workload (27-node hex 10^3, 26,460 DOF,
-2,000 element parameters, nev 50), generated on the CPU:
+nev 100), the differentiation workload (27-node hex 10^3, 26,460 DOF,
+2,000 element parameters, nev 50) and the small workload (8-node hex 12^3,
+6,084 DOF, nev 20), generated on the CPU:
 
+  c1_exact.npz   the 20 smallest exact eigenvalues of the small workload
+                 (scipy ARPACK, sigma = 0, tol 1e-14);
   c2_oracle.npz  the oracle's AMLS output (theta, p, p of pass A, perm) with
                  the reference's default local eigensolver choice (silMode 0)
                  at nLevels 6, leafSize 500, eta 2;
@@ -30,7 +33,7 @@ difference quotient (f(+h) - f(-h)) / 2h is then evaluated two ways:
           d = x_-^T Mbar_e x_+).  Both use only the perturbed eigenpairs.
 
 Run from the repository root (takes tens of minutes):
-  python tests/golden/make_c2c4_golden.py [c2|c4|both]
+  python tests/golden/make_c2c4_golden.py [c1|c2|c4|both]
 """
 import os
 import sys
@@ -82,6 +85,13 @@ def cross_form(p, e, A, Xm, Xp):
     b = Xp[d[keep]]
     Ak = A[np.ix_(keep, keep)]
     return np.einsum("ik,ij,jk->k", a, Ak, b)
+
+
+def c1():
+    p = cases.config_pencil("C1", seed=0)
+    w, _ = _eigsh(p.K, p.M, 20)
+    print("c1 exact", w[:3], flush=True)
+    np.savez(os.path.join(HERE, "c1_exact.npz"), theta=w)
 
 
 def c2():
@@ -146,6 +156,8 @@ def c4():
 
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "both"
+    if which == "c1":
+        c1()
     if which in ("c2", "both"):
         c2()
     if which in ("c4", "both"):
