@@ -22,10 +22,16 @@ constexpr int kFJ = 4;             // n8 fragments per warp (warp tile 32 x 8 kF
 constexpr int kBM = kGemmTile, kBN = kGemmTile;   // 64 x 64
 constexpr int kKs = 16;                            // K slice
 constexpr int kStages = 3;
-constexpr int kLdA = kBM + 4, kLdB = kBN + 4;      // = 4 mod 16 doubles
-constexpr int kStage = kKs * (kLdA + kLdB);        // doubles per stage
+// An operand slice is stored in shared memory in the order it is contiguous
+// in global memory, so that consecutive cp.async writes land in consecutive
+// banks: k-major ([k][row], row pitch kLdA / kLdB) when rows are contiguous,
+// row-major ([row][k], pitch kLdK) when k is.  Both pitches are 4 mod 16
+// doubles, which keeps the fragment loads at two wavefronts per warp.
+constexpr int kLdA = kBM + 4, kLdB = kBN + 4;
+constexpr int kLdK = kKs + 4;
+constexpr int kOpSlot = (kKs * kLdA > kBM * kLdK) ? kKs * kLdA : kBM * kLdK;   // doubles per operand
+constexpr int kStage = 2 * kOpSlot;                // doubles per stage
 constexpr size_t kGemmSmem = sizeof(double) * kStages * kStage;
-constexpr int kLA = kBM * kKs / kGemmThreads, kLB = kBN * kKs / kGemmThreads;
 
 __device__ __forceinline__ void dmma16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
     asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
@@ -35,61 +41,144 @@ __device__ __forceinline__ void dmma16x8x16(double (&c)[4], const double (&a)[8]
           "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-// 8-byte asynchronous copy; src_size 0 writes zeros and reads nothing
-__device__ __forceinline__ void cpAsync8(double* dst, const double* src, bool valid) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+// Asynchronous copies to a shared-space address; a source size below the
+// copy size zero-fills the rest (0: nothing is read).
+__device__ __forceinline__ void cpAsync8(unsigned dst, const double* src, int bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cpAsync16(unsigned dst, const double* src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes));
 }
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;"); }
 template <int N>
 __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
-// one K slice of op(A) (kBM x kKs) and op(B) (kKs x kBN) into shared memory,
-// stored k-major: As[k][i], Bs[k][j]; global reads coalesced on the
-// contiguous side of each layout
-// Gathered A (GA): the column indices aMap[gk] of a slice, loaded one slice
-// ahead into registers so that the address of a gathered copy never waits
-// on the map.
-template <bool GA>
-__device__ __forceinline__ void loadMap(const GemmDesc& D, int k0, int kEnd, int32_t (&am)[kLA]) {
-    if constexpr (GA) {
+// Copy plan of one operand of a tile.  A K slice of the operand (64 rows x
+// 16 k) is stored in shared memory in the order it is contiguous in global
+// memory:
+//   row layout ([k][row], pitch kLdA; rows contiguous, or gathered columns
+//   whose rows are contiguous): 8-byte copies, thread t copies row t % 64 of
+//   k = t / 64 + 2u (u < 8); 16-byte copies, rows 2 (t % 32) and the next of
+//   k = t / 32 + 4u (u < 4);
+//   k layout ([row][k], pitch kLdK; k contiguous): 8-byte copies, thread t
+//   copies k = t % 16 of rows t / 16 + 8u (u < 8); 16-byte copies, k =
+//   2 (t % 8) and the next of rows t / 8 + 16u (u < 4).
+// A thread's copies in a slice differ by a constant source step, and the
+// next slice is a constant step further, so a copy costs one address add, a
+// size select and the copy.  16-byte copies need a 16-byte aligned operand
+// with an even leading dimension (and an even first k for the k layout);
+// otherwise the plan uses 8-byte copies.
+struct CopyPlan {
+    const double* p;    // source of copy u = 0 in the next slice (gathered: row base)
+    const double* safe; // operand base: the source of copies that read nothing
+    int64_t stepU;      // source step between copies u
+    int64_t ld;
+    int rowsLeft;       // row layout: valid rows from the thread's first row
+    int rq;             // k layout: the thread's first row
+    int rows;           // k layout: valid rows of the tile
+    int sub;            // row layout: the thread's first k; k layout: the thread's k
+    unsigned dst;       // shared offset (bytes) of copy u = 0 within the operand slot
+    bool vec;
+};
+
+__device__ __forceinline__ bool aligned16(const double* p) {
+    return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
+__device__ __forceinline__ CopyPlan planRow(const double* base, int64_t ld, int row0, int rows, int kBeg,
+                                            bool gather) {
+    CopyPlan c;
+    const int t = threadIdx.x;
+    c.vec = aligned16(base) && (ld & 1) == 0;
+    const int r = c.vec ? 2 * (t & 31) : (t & 63);
+    c.sub = c.vec ? (t >> 5) : (t >> 6);
+    c.rowsLeft = rows - r;
+    c.ld = ld;
+    c.stepU = (c.vec ? 4 : 2) * ld;
+    c.safe = base;
+    c.p = gather ? base + row0 + r : base + row0 + r + (int64_t)(kBeg + c.sub) * ld;
+    c.dst = 8u * static_cast<unsigned>(c.sub * kLdA + r);
+    return c;
+}
+
+__device__ __forceinline__ CopyPlan planK(const double* base, int64_t ld, int row0, int rows, int kBeg) {
+    CopyPlan c;
+    const int t = threadIdx.x;
+    c.vec = aligned16(base) && (ld & 1) == 0 && (kBeg & 1) == 0;
+    c.sub = c.vec ? 2 * (t & 7) : (t & 15);
+    c.rq = c.vec ? (t >> 3) : (t >> 4);
+    c.rows = rows;
+    c.ld = ld;
+    c.stepU = (c.vec ? 16 : 8) * ld;
+    c.safe = base;
+    c.p = base + (int64_t)(row0 + c.rq) * ld + kBeg + c.sub;
+    c.dst = 8u * static_cast<unsigned>(c.rq * kLdK + c.sub);
+    return c;
+}
+
+// one slice of a row-layout operand; kLeft = valid k from the slice start;
+// map (gathered columns) = the column indices of the thread's copies
+template <bool GATHER>
+__device__ __forceinline__ void issueRow(CopyPlan& c, unsigned slot, int kLeft, const int32_t (&map)[8]) {
+    if (c.vec) {
+        const int rb = c.rowsLeft >= 2 ? 16 : (c.rowsLeft == 1 ? 8 : 0);
 #pragma unroll
-        for (int u = 0; u < kLA; ++u) {
-            const int gk = k0 + (threadIdx.x + kGemmThreads * u) / kBM;
-            am[u] = gk < kEnd ? D.aMap[gk] : 0;
+        for (int u = 0; u < 4; ++u) {
+            const int b = c.sub + 4 * u < kLeft ? rb : 0;
+            const double* src = GATHER ? c.p + (int64_t)map[u] * c.ld : c.p + u * c.stepU;
+            cpAsync16(slot + c.dst + 8u * 4 * kLdA * u, b ? src : c.safe, b);
         }
+    } else {
+        const int rb = c.rowsLeft > 0 ? 8 : 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int b = c.sub + 2 * u < kLeft ? rb : 0;
+            const double* src = GATHER ? c.p + (int64_t)map[u] * c.ld : c.p + u * c.stepU;
+            cpAsync8(slot + c.dst + 8u * 2 * kLdA * u, b ? src : c.safe, b);
+        }
+    }
+    if (!GATHER) c.p += kKs * c.ld;
+}
+
+__device__ __forceinline__ void issueK(CopyPlan& c, unsigned slot, int kLeft) {
+    if (c.vec) {
+        const int kb = c.sub + 1 < kLeft ? 16 : (c.sub < kLeft ? 8 : 0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int b = c.rq + 16 * u < c.rows ? kb : 0;
+            cpAsync16(slot + c.dst + 8u * 16 * kLdK * u, b ? c.p + u * c.stepU : c.safe, b);
+        }
+    } else {
+        const int kb = c.sub < kLeft ? 8 : 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int b = c.rq + 8 * u < c.rows ? kb : 0;
+            cpAsync8(slot + c.dst + 8u * 8 * kLdK * u, b ? c.p + u * c.stepU : c.safe, b);
+        }
+    }
+    c.p += kKs;
+}
+
+// Gathered A: the column indices of the thread's copies of slice k0, loaded
+// one slice ahead so that the address of a gathered copy never waits on the
+// map (out-of-range k read index 0: their copies are zero-filled).
+__device__ __forceinline__ void loadMap(const GemmDesc& D, const CopyPlan& c, int k0, int kEnd,
+                                        int32_t (&am)[8]) {
+    const int ks = c.vec ? 4 : 2;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int gk = k0 + c.sub + ks * u;
+        am[u] = (u < (c.vec ? 4 : 8) && gk < kEnd) ? D.aMap[gk] : 0;
     }
 }
 
 template <bool TA, bool TB, bool GA>
-__device__ __forceinline__ void issueSlice(const GemmDesc& D, int m0, int n0, int k0, int kEnd,
-                                           double* As, double* Bs, const int32_t (&am)[kLA]) {
-#pragma unroll
-    for (int u = 0; u < kLA; ++u) {
-        const int idx = threadIdx.x + kGemmThreads * u;
-        const int i = TA ? idx / kKs : idx % kBM;
-        const int k = TA ? idx % kKs : idx / kBM;
-        const int gi = m0 + i, gk = k0 + k;
-        const bool ok = gi < D.M && gk < kEnd;
-        const double* src = D.A;
-        if (ok) {
-            if (TA) src = D.A + gk + (int64_t)gi * D.lda;
-            else if (GA) src = D.A + gi + (int64_t)am[u] * D.lda;
-            else src = D.A + gi + (int64_t)gk * D.lda;
-        }
-        cpAsync8(As + k * kLdA + i, src, ok);
-    }
-#pragma unroll
-    for (int u = 0; u < kLB; ++u) {
-        const int idx = threadIdx.x + kGemmThreads * u;
-        const int j = TB ? idx % kBN : idx / kKs;
-        const int k = TB ? idx / kBN : idx % kKs;
-        const int gj = n0 + j, gk = k0 + k;
-        const bool ok = gj < D.N && gk < kEnd;
-        const double* src = D.B;
-        if (ok) src = TB ? D.B + gj + (int64_t)gk * D.ldb : D.B + gk + (int64_t)gj * D.ldb;
-        cpAsync8(Bs + k * kLdB + j, src, ok);
-    }
+__device__ __forceinline__ void issueSlice(CopyPlan& pa, CopyPlan& pb, unsigned slot, int kLeft,
+                                           const int32_t (&am)[8]) {
+    if (TA) issueK(pa, slot, kLeft);
+    else issueRow<GA>(pa, slot, kLeft, am);
+    if (TB) issueRow<false>(pb, slot + 8u * kOpSlot, kLeft, am);
+    else issueK(pb, slot + 8u * kOpSlot, kLeft);
 }
 
 template <bool TA, bool TB, bool GA>
@@ -114,45 +203,67 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
     if (D.flags & kTriKFrom) kBeg = max(kBeg, n0);
     if (D.flags & kTriAUpTo) kEnd = min(kEnd, m0 + kBM);
     const int nSlices = kEnd > kBeg ? (kEnd - kBeg + kKs - 1) / kKs : 0;
-    int32_t am[kLA];
+    const int mRows = min(kBM, D.M - m0), nRows = min(kBN, D.N - n0);
+    CopyPlan pa = TA ? planK(D.A, D.lda, m0, mRows, kBeg) : planRow(D.A, D.lda, m0, mRows, kBeg, GA);
+    CopyPlan pb = TB ? planRow(D.B, D.ldb, n0, nRows, kBeg, false) : planK(D.B, D.ldb, n0, nRows, kBeg);
+    const unsigned sm0 = static_cast<unsigned>(__cvta_generic_to_shared(sm));
+    int32_t am[8];
 #pragma unroll
     for (int st = 0; st < kStages - 1; ++st) {
         if (st < nSlices) {
-            double* base = sm + st * kStage;
-            loadMap<GA>(D, kBeg + st * kKs, kEnd, am);
-            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + st * kKs, kEnd, base, base + kKs * kLdA, am);
+            if (GA) loadMap(D, pa, kBeg + st * kKs, kEnd, am);
+            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * st * kStage, kEnd - kBeg - st * kKs, am);
         }
         cpAsyncCommit();
     }
-    if (kStages - 1 < nSlices) loadMap<GA>(D, kBeg + (kStages - 1) * kKs, kEnd, am);
+    if (GA && kStages - 1 < nSlices) loadMap(D, pa, kBeg + (kStages - 1) * kKs, kEnd, am);
     for (int sl = 0; sl < nSlices; ++sl) {
         cpAsyncWait<kStages - 2>();
         __syncthreads();
         const int nx = sl + kStages - 1;
         if (nx < nSlices) {
-            double* base = sm + (nx % kStages) * kStage;
-            issueSlice<TA, TB, GA>(D, m0, n0, kBeg + nx * kKs, kEnd, base, base + kKs * kLdA, am);
-            if (nx + 1 < nSlices) loadMap<GA>(D, kBeg + (nx + 1) * kKs, kEnd, am);
+            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * (nx % kStages) * kStage, kEnd - kBeg - nx * kKs, am);
+            if (GA && nx + 1 < nSlices) loadMap(D, pa, kBeg + (nx + 1) * kKs, kEnd, am);
         }
         cpAsyncCommit();
         const double* As = sm + (sl % kStages) * kStage;
-        const double* Bs = As + kKs * kLdA;
-        // fragments: A element (row g (+8), k tg + 4 q), B element (k tg + 4 q, col g)
+        const double* Bs = As + kOpSlot;
+        // fragments: A element (MMA row g (+8), k tg + 4 q), B element (k tg + 4 q,
+        // MMA col g).  An operand in the row layout is read two rows at a time
+        // (16-byte loads): MMA rows g and g + 8 of a 16-row block are tile rows
+        // 2g and 2g + 1, and MMA col g of n8 fragments 2p and 2p + 1 are tile
+        // cols 16p + 2g and 16p + 2g + 1; the epilogue maps the accumulators back.
         double a[2][8], b[kFJ][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-            const int r = wm + 16 * i + g;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                a[i][2 * q] = As[(tg + 4 * q) * kLdA + r];
-                a[i][2 * q + 1] = As[(tg + 4 * q) * kLdA + r + 8];
+                const int k = tg + 4 * q;
+                if (TA) {
+                    const int r = wm + 16 * i + g;
+                    a[i][2 * q] = As[r * kLdK + k];
+                    a[i][2 * q + 1] = As[(r + 8) * kLdK + k];
+                } else {
+                    const double2 v = *reinterpret_cast<const double2*>(As + k * kLdA + wm + 16 * i + 2 * g);
+                    a[i][2 * q] = v.x;
+                    a[i][2 * q + 1] = v.y;
+                }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kFJ; ++j) {
-            const int c = wn + 8 * j + g;
+        for (int q = 0; q < 4; ++q) {
+            const int k = tg + 4 * q;
+            if (TB) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) b[j][q] = Bs[(tg + 4 * q) * kLdB + c];
+                for (int jp = 0; jp < kFJ / 2; ++jp) {
+                    const double2 v = *reinterpret_cast<const double2*>(Bs + k * kLdB + wn + 16 * jp + 2 * g);
+                    b[2 * jp][q] = v.x;
+                    b[2 * jp + 1][q] = v.y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < kFJ; ++j) b[j][q] = Bs[(wn + 8 * j + g) * kLdK + k];
+            }
         }
 #pragma unroll
         for (int i = 0; i < 2; ++i)
@@ -160,20 +271,22 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
             for (int j = 0; j < kFJ; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
     }
     cpAsyncWait<0>();
-    // epilogue: fragment (i, j) element q sits at row wm + 16 i + g + 8 (q / 2),
-    // column wn + 8 j + 2 tg + (q % 2)
+    // epilogue: fragment (i, j) element q sits at MMA row wm + 16 i + g + 8 (q / 2),
+    // MMA column wn + 8 j + 2 tg + (q % 2); tile row and column as the
+    // fragment loads relabelled them
 #pragma unroll
     for (int j = 0; j < kFJ; ++j)
 #pragma unroll
         for (int q2 = 0; q2 < 2; ++q2) {
-            const int col = n0 + wn + 8 * j + 2 * tg + q2;
+            const int col = TB ? n0 + wn + 16 * (j / 2) + 4 * tg + 2 * q2 + (j % 2)
+                               : n0 + wn + 8 * j + 2 * tg + q2;
             if (col >= D.N) continue;
             const double cs = (D.flags & kColScale) ? D.colScale[col] : 1.0;
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int row = m0 + wm + 16 * i + g + 8 * h;
+                    const int row = TA ? m0 + wm + 16 * i + g + 8 * h : m0 + wm + 16 * i + 2 * g + h;
                     if (row >= D.M) continue;
                     double v = D.alpha * acc[i][j][2 * h + q2] * cs;
                     if (D.flags & kRowScale) v *= D.rowScale[row];
@@ -251,7 +364,8 @@ __device__ __forceinline__ void fuIssueSlice(const FrontUpdDesc& D, int p0, int 
         const bool ok = gr < D.s && gk < D.n;
         const double* base = (op == 0 || op == 2) ? D.A : D.B;
         const double* src = ok ? base + gr + (int64_t)gk * D.ld : D.A;
-        cpAsync8(st + op * kKs * kLdA + k * kLdA + r, src, ok);
+        cpAsync8(static_cast<unsigned>(__cvta_generic_to_shared(st + op * kKs * kLdA + k * kLdA + r)), src,
+                 ok ? 8 : 0);
     }
 }
 }  // namespace
