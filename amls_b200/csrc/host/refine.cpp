@@ -29,6 +29,22 @@ namespace {
 constexpr int kT = kGemmTile;
 constexpr int kTB = kGemmTile;
 int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// Tiles by decreasing work (K extent x rows x columns), ties in table order:
+// CTAs start in table order, so the heavy tiles go first and the light ones
+// fill the last wave.
+void sortByWork(std::vector<TileRef>& t, const std::vector<GemmDesc>& d) {
+    auto work = [&](const TileRef& r) {
+        const GemmDesc& g = d[static_cast<size_t>(r.desc)];
+        int64_t kb = 0, ke = g.K;
+        if (g.flags & kTriKUpTo) ke = std::min<int64_t>(ke, r.n0 + kGemmTile);
+        if (g.flags & kTriKFrom) kb = std::max<int64_t>(kb, r.n0);
+        const int64_t rows = std::min<int64_t>(kGemmTile, g.M - r.m0);
+        const int64_t cols = std::min<int64_t>(kGemmTile, g.N - r.n0);
+        return std::max<int64_t>(0, ke - kb) * rows * cols;
+    };
+    std::stable_sort(t.begin(), t.end(), [&](const TileRef& a, const TileRef& b) { return work(a) > work(b); });
+}
 }  // namespace
 
 #define LAUNCH(call)                                   \
@@ -285,6 +301,10 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
             sweep.insert(sweep.end(), d.begin(), d.end());
             for (TileRef& r : t) r.desc += base;
         };
+        sortByWork(ftT, ft);
+        sortByWork(fgT, fg);
+        sortByWork(bgT, bg);
+        sortByWork(btT, bt);
         append(ft, ftT);
         append(fg, fgT);
         append(bg, bgT);
@@ -520,7 +540,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
         }
         if (!last || vectors) {
             LAUNCH(launchGemmBatched(b.dev<GemmDesc>(oUP), b.dev<TileRef>(oUPT),
-                                     last ? nUp1 : static_cast<int>(upT.size()), s));
+                                    last ? nUp1 : static_cast<int>(upT.size()), s));
             catF_[2] += (last ? static_cast<double>(nev) / dq : 2.0 + static_cast<double>(nextLock) / dq) *
                         2.0 * dn * dq * dq;
             catB_[2] += 8.0 * (last ? 2.0 : 4.0) * dn * dq;

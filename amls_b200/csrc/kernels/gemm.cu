@@ -86,9 +86,8 @@ __device__ __forceinline__ bool aligned16(const double* p) {
 }
 
 __device__ __forceinline__ CopyPlan planRow(const double* base, int64_t ld, int row0, int rows, int kBeg,
-                                            bool gather) {
+                                            bool gather, int t = threadIdx.x) {
     CopyPlan c;
-    const int t = threadIdx.x;
     c.vec = aligned16(base) && (ld & 1) == 0;
     const int r = c.vec ? 2 * (t & 31) : (t & 63);
     c.sub = c.vec ? (t >> 5) : (t >> 6);
@@ -181,99 +180,89 @@ __device__ __forceinline__ void issueSlice(CopyPlan& pa, CopyPlan& pb, unsigned 
     else issueK(pb, slot + 8u * kOpSlot, kLeft);
 }
 
-template <bool TA, bool TB, bool GA>
-__device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, double* sm) {
-    const int m0 = t.m0, n0 = t.n0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, tg = lane & 3;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-    double acc[2][kFJ][4];
+// K range of a tile: split-K chunk; triangular B restricts k to <= the
+// tile's last column (kTriKUpTo) or >= its first column (kTriKFrom),
+// triangular A to <= the tile's last row (kTriAUpTo)
+struct TileRange {
+    int kBeg, kEnd, nSlices;
+};
+__device__ __forceinline__ TileRange tileRange(const GemmDesc& D, const TileRef& t) {
+    TileRange r;
+    r.kBeg = D.kChunk > 0 ? t.pad * D.kChunk : 0;
+    r.kEnd = D.kChunk > 0 ? min(D.K, r.kBeg + D.kChunk) : D.K;
+    if (D.flags & kTriKUpTo) r.kEnd = min(r.kEnd, t.n0 + kBN);
+    if (D.flags & kTriKFrom) r.kBeg = max(r.kBeg, t.n0);
+    if (D.flags & kTriAUpTo) r.kEnd = min(r.kEnd, t.m0 + kBM);
+    r.nSlices = r.kEnd > r.kBeg ? (r.kEnd - r.kBeg + kKs - 1) / kKs : 0;
+    return r;
+}
+
+__device__ __forceinline__ void zeroAcc(double (&acc)[2][kFJ][4]) {
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < kFJ; ++j)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
-    // split-K range; triangular B restricts k to <= the tile's last column
-    // (kTriKUpTo) or >= its first column (kTriKFrom), triangular A to <= the
-    // tile's last row (kTriAUpTo)
-    int kBeg = D.kChunk > 0 ? t.pad * D.kChunk : 0;
-    int kEnd = D.kChunk > 0 ? min(D.K, kBeg + D.kChunk) : D.K;
-    if (D.flags & kTriKUpTo) kEnd = min(kEnd, n0 + kBN);
-    if (D.flags & kTriKFrom) kBeg = max(kBeg, n0);
-    if (D.flags & kTriAUpTo) kEnd = min(kEnd, m0 + kBM);
-    const int nSlices = kEnd > kBeg ? (kEnd - kBeg + kKs - 1) / kKs : 0;
-    const int mRows = min(kBM, D.M - m0), nRows = min(kBN, D.N - n0);
-    CopyPlan pa = TA ? planK(D.A, D.lda, m0, mRows, kBeg) : planRow(D.A, D.lda, m0, mRows, kBeg, GA);
-    CopyPlan pb = TB ? planRow(D.B, D.ldb, n0, nRows, kBeg, false) : planK(D.B, D.ldb, n0, nRows, kBeg);
-    const unsigned sm0 = static_cast<unsigned>(__cvta_generic_to_shared(sm));
-    int32_t am[8];
+}
+
+// One K slice from shared memory into the accumulators.  Fragments: A
+// element (MMA row g (+8), k tg + 4 q), B element (k tg + 4 q, MMA col g).
+// An operand in the row layout is read two rows at a time (16-byte loads):
+// MMA rows g and g + 8 of a 16-row block are tile rows 2g and 2g + 1, and MMA
+// col g of n8 fragments 2p and 2p + 1 are tile cols 16p + 2g and 16p + 2g + 1;
+// the epilogue maps the accumulators back.
+template <bool TA, bool TB>
+__device__ __forceinline__ void computeSlice(double (&acc)[2][kFJ][4], const double* As, const double* Bs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    double a[2][8], b[kFJ][4];
 #pragma unroll
-    for (int st = 0; st < kStages - 1; ++st) {
-        if (st < nSlices) {
-            if (GA) loadMap(D, pa, kBeg + st * kKs, kEnd, am);
-            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * st * kStage, kEnd - kBeg - st * kKs, am);
-        }
-        cpAsyncCommit();
-    }
-    if (GA && kStages - 1 < nSlices) loadMap(D, pa, kBeg + (kStages - 1) * kKs, kEnd, am);
-    for (int sl = 0; sl < nSlices; ++sl) {
-        cpAsyncWait<kStages - 2>();
-        __syncthreads();
-        const int nx = sl + kStages - 1;
-        if (nx < nSlices) {
-            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * (nx % kStages) * kStage, kEnd - kBeg - nx * kKs, am);
-            if (GA && nx + 1 < nSlices) loadMap(D, pa, kBeg + (nx + 1) * kKs, kEnd, am);
-        }
-        cpAsyncCommit();
-        const double* As = sm + (sl % kStages) * kStage;
-        const double* Bs = As + kOpSlot;
-        // fragments: A element (MMA row g (+8), k tg + 4 q), B element (k tg + 4 q,
-        // MMA col g).  An operand in the row layout is read two rows at a time
-        // (16-byte loads): MMA rows g and g + 8 of a 16-row block are tile rows
-        // 2g and 2g + 1, and MMA col g of n8 fragments 2p and 2p + 1 are tile
-        // cols 16p + 2g and 16p + 2g + 1; the epilogue maps the accumulators back.
-        double a[2][8], b[kFJ][4];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int k = tg + 4 * q;
-                if (TA) {
-                    const int r = wm + 16 * i + g;
-                    a[i][2 * q] = As[r * kLdK + k];
-                    a[i][2 * q + 1] = As[(r + 8) * kLdK + k];
-                } else {
-                    const double2 v = *reinterpret_cast<const double2*>(As + k * kLdA + wm + 16 * i + 2 * g);
-                    a[i][2 * q] = v.x;
-                    a[i][2 * q + 1] = v.y;
-                }
-            }
-        }
+    for (int i = 0; i < 2; ++i) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int k = tg + 4 * q;
-            if (TB) {
-#pragma unroll
-                for (int jp = 0; jp < kFJ / 2; ++jp) {
-                    const double2 v = *reinterpret_cast<const double2*>(Bs + k * kLdB + wn + 16 * jp + 2 * g);
-                    b[2 * jp][q] = v.x;
-                    b[2 * jp + 1][q] = v.y;
-                }
+            if (TA) {
+                const int r = wm + 16 * i + g;
+                a[i][2 * q] = As[r * kLdK + k];
+                a[i][2 * q + 1] = As[(r + 8) * kLdK + k];
             } else {
-#pragma unroll
-                for (int j = 0; j < kFJ; ++j) b[j][q] = Bs[(wn + 8 * j + g) * kLdK + k];
+                const double2 v = *reinterpret_cast<const double2*>(As + k * kLdA + wm + 16 * i + 2 * g);
+                a[i][2 * q] = v.x;
+                a[i][2 * q + 1] = v.y;
             }
         }
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < kFJ; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
     }
-    cpAsyncWait<0>();
-    // epilogue: fragment (i, j) element q sits at MMA row wm + 16 i + g + 8 (q / 2),
-    // MMA column wn + 8 j + 2 tg + (q % 2); tile row and column as the
-    // fragment loads relabelled them
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = tg + 4 * q;
+        if (TB) {
+#pragma unroll
+            for (int jp = 0; jp < kFJ / 2; ++jp) {
+                const double2 v = *reinterpret_cast<const double2*>(Bs + k * kLdB + wn + 16 * jp + 2 * g);
+                b[2 * jp][q] = v.x;
+                b[2 * jp + 1][q] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kFJ; ++j) b[j][q] = Bs[(wn + 8 * j + g) * kLdK + k];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < kFJ; ++j) dmma16x8x16(acc[i][j], a[i], b[j]);
+}
+
+// Epilogue: fragment (i, j) element q sits at MMA row wm + 16 i + g + 8 (q / 2),
+// MMA column wn + 8 j + 2 tg + (q % 2); tile row and column as the fragment
+// loads relabelled them.
+template <bool TA, bool TB>
+__device__ __forceinline__ void storeTile(const GemmDesc& D, int m0, int n0, const double (&acc)[2][kFJ][4]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
 #pragma unroll
     for (int j = 0; j < kFJ; ++j)
 #pragma unroll
@@ -303,6 +292,43 @@ __device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, do
                     }
                 }
         }
+}
+
+template <bool TA, bool TB, bool GA>
+__device__ __forceinline__ void gemmTile(const GemmDesc& D, const TileRef& t, double* sm) {
+    double acc[2][kFJ][4];
+    zeroAcc(acc);
+    const TileRange R = tileRange(D, t);
+    const int kBeg = R.kBeg, kEnd = R.kEnd, nSlices = R.nSlices;
+    const int m0 = t.m0, n0 = t.n0;
+    const int mRows = min(kBM, D.M - m0), nRows = min(kBN, D.N - n0);
+    CopyPlan pa = TA ? planK(D.A, D.lda, m0, mRows, kBeg) : planRow(D.A, D.lda, m0, mRows, kBeg, GA);
+    CopyPlan pb = TB ? planRow(D.B, D.ldb, n0, nRows, kBeg, false) : planK(D.B, D.ldb, n0, nRows, kBeg);
+    const unsigned sm0 = static_cast<unsigned>(__cvta_generic_to_shared(sm));
+    int32_t am[8];
+#pragma unroll
+    for (int st = 0; st < kStages - 1; ++st) {
+        if (st < nSlices) {
+            if (GA) loadMap(D, pa, kBeg + st * kKs, kEnd, am);
+            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * st * kStage, kEnd - kBeg - st * kKs, am);
+        }
+        cpAsyncCommit();
+    }
+    if (GA && kStages - 1 < nSlices) loadMap(D, pa, kBeg + (kStages - 1) * kKs, kEnd, am);
+    for (int sl = 0; sl < nSlices; ++sl) {
+        cpAsyncWait<kStages - 2>();
+        __syncthreads();
+        const int nx = sl + kStages - 1;
+        if (nx < nSlices) {
+            issueSlice<TA, TB, GA>(pa, pb, sm0 + 8u * (nx % kStages) * kStage, kEnd - kBeg - nx * kKs, am);
+            if (GA && nx + 1 < nSlices) loadMap(D, pa, kBeg + (nx + 1) * kKs, kEnd, am);
+        }
+        cpAsyncCommit();
+        const double* As = sm + (sl % kStages) * kStage;
+        computeSlice<TA, TB>(acc, As, As + kOpSlot);
+    }
+    cpAsyncWait<0>();
+    storeTile<TA, TB>(D, m0, n0, acc);
 }
 }  // namespace
 
@@ -352,21 +378,15 @@ namespace {
 constexpr int kFuStage = 4 * kKs * kLdA;   // Ap, Bp, Aq, Bq slices
 constexpr size_t kFuSmem = sizeof(double) * kStages * kFuStage;
 
-__device__ __forceinline__ void fuIssueSlice(const FrontUpdDesc& D, int p0, int q0, int k0, double* st) {
-    // 4 operands x 64 rows x 16 k = 4096 elements, 16 per thread
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int idx = threadIdx.x + NT * u;
-        const int op = idx >> 10, e = idx & 1023;
-        const int r = e % 64, k = e / 64;
-        const int gk = k0 + k;
-        const int gr = (op < 2 ? p0 : q0) + r;
-        const bool ok = gr < D.s && gk < D.n;
-        const double* base = (op == 0 || op == 2) ? D.A : D.B;
-        const double* src = ok ? base + gr + (int64_t)gk * D.ld : D.A;
-        cpAsync8(static_cast<unsigned>(__cvta_generic_to_shared(st + op * kKs * kLdA + k * kLdA + r)), src,
-                 ok ? 8 : 0);
-    }
+// Operand slots of a stage: Ap, Bp, Aq, Bq (64 rows x 16 k each, [k][row]).
+// Threads 0..127 copy the A slices (rows p, rows q), threads 128..255 the B
+// slices, each through the GEMM's row-layout copy plans.
+constexpr unsigned kFuOpBytes = 8u * kKs * kLdA;
+__device__ __forceinline__ void fuIssueSlice(CopyPlan& cp, CopyPlan& cq, unsigned st, int kLeft) {
+    const int32_t none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const unsigned opB = threadIdx.x >= 128 ? 1u : 0u;
+    issueRow<false>(cp, st + opB * kFuOpBytes, kLeft, none);
+    issueRow<false>(cq, st + (2u + opB) * kFuOpBytes, kLeft, none);
 }
 }  // namespace
 
@@ -389,16 +409,21 @@ __global__ void __launch_bounds__(NT) frontUpdateKernel(const FrontUpdDesc* __re
 #pragma unroll
             for (int q = 0; q < 4; ++q) aK[i][j][q] = aM[i][j][q] = 0.0;
     const int nSlices = (D.n + kKs - 1) / kKs;
+    const double* src = threadIdx.x < 128 ? D.A : D.B;
+    const int ct = threadIdx.x & 127;
+    CopyPlan cp = planRow(src, D.ld, p0, min(64, D.s - p0), 0, false, ct);
+    CopyPlan cq = planRow(src, D.ld, q0, min(64, D.s - q0), 0, false, ct);
+    const unsigned sm0 = static_cast<unsigned>(__cvta_generic_to_shared(fuSmem));
 #pragma unroll
     for (int st = 0; st < kStages - 1; ++st) {
-        if (st < nSlices) fuIssueSlice(D, p0, q0, st * kKs, fuSmem + st * kFuStage);
+        if (st < nSlices) fuIssueSlice(cp, cq, sm0 + 8u * st * kFuStage, D.n - st * kKs);
         cpAsyncCommit();
     }
     for (int sl = 0; sl < nSlices; ++sl) {
         cpAsyncWait<kStages - 2>();
         __syncthreads();
         const int nx = sl + kStages - 1;
-        if (nx < nSlices) fuIssueSlice(D, p0, q0, nx * kKs, fuSmem + (nx % kStages) * kFuStage);
+        if (nx < nSlices) fuIssueSlice(cp, cq, sm0 + 8u * (nx % kStages) * kFuStage, D.n - nx * kKs);
         cpAsyncCommit();
         const double* Ap = fuSmem + (sl % kStages) * kFuStage;
         const double* Bp = Ap + kKs * kLdA;
