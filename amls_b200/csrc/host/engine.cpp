@@ -815,19 +815,26 @@ void Engine::checkStatus(const char* phase) {
 // ---------------------------------------------------------------------------
 // eigen driver
 // ---------------------------------------------------------------------------
-// Cooperative tridiagonalisation of the matrices in `large`, in launches of at
-// most tridiagLargeMaxCtas(maxN) matrices (one CTA per SM), each matrix given
-// CTAs in proportion to n^2 (measured faster than n^3 on the benchmark tree).  The stream is synchronised before returning
-// (the launch tables live in `blob`).
-void Engine::tridiagLargeAll(const std::vector<EigDesc>& large, DevBuf& pbuf, DevBuf& blob,
+// Cooperative tridiagonalisation of the matrices in `large`.  A launch runs
+// as many column steps as its largest matrix has, each ending in a grid
+// barrier, so the matrices go largest first into launches of similar
+// orders: a launch takes the next matrices down to 0.4 x its largest order
+// (at most tridiagLargeMaxCtas(maxN), one CTA per SM), each matrix given CTAs
+// in proportion to n^2 (measured faster than n^3 on the benchmark tree).  The
+// stream is synchronised before returning (the launch tables live in `blob`).
+void Engine::tridiagLargeAll(const std::vector<EigDesc>& largeIn, DevBuf& pbuf, DevBuf& blob,
                              cudaStream_t s) {
+    std::vector<EigDesc> large(largeIn);
+    std::stable_sort(large.begin(), large.end(), [](const EigDesc& a, const EigDesc& b) { return a.n > b.n; });
     size_t g0 = 0;
     while (g0 < large.size()) {
-        int maxN = 0;
-        for (size_t g = g0; g < large.size(); ++g) maxN = std::max<int>(maxN, large[g].n);
+        const int maxN = large[g0].n;
         const int maxCta = tridiagLargeMaxCtas(maxN);
         if (maxCta < 1) throw AmlsError(AMLS_ERR_CUDA, "cooperative tridiagonalisation does not fit");
-        const size_t g1 = std::min(large.size(), g0 + static_cast<size_t>(maxCta));
+        size_t g1 = g0 + 1;
+        while (g1 < large.size() && g1 - g0 < static_cast<size_t>(maxCta) &&
+               10 * static_cast<int64_t>(large[g1].n) >= 4 * static_cast<int64_t>(maxN))
+            ++g1;
         const int cnt = static_cast<int>(g1 - g0);
         std::vector<EigDesc> part(large.begin() + static_cast<std::ptrdiff_t>(g0),
                                   large.begin() + static_cast<std::ptrdiff_t>(g1));

@@ -299,7 +299,7 @@ def run_ours(args, rank, world, dist):
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     dom_ms, dom_launches = ktimes[dom]
     roof = dominant_roofline(dom, dom_ms / max(args.steps, 1), dom_launches / max(args.steps, 1),
-                             work, info, pk, src, s)
+                             work, info, pk, src, s, args.config)
     line = {
         "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
@@ -417,7 +417,17 @@ def fp64_gemm_peak():
     return best
 
 
-def dominant_roofline(cat, ms, launches, work, info, pk, src, s):
+def gemm_traffic():
+    """DRAM bytes per launch of the DMMA GEMM kernel from the committed ncu
+    capture of one C5 solve (profiles/gemm_dram_c5.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "gemm_dram_c5.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def dominant_roofline(cat, ms, launches, work, info, pk, src, s, config="C5"):
     """Roofline of the dominant kernel category from the engine's ledger."""
     from amls_b200 import _lib
     led = s.category_work()
@@ -429,9 +439,16 @@ def dominant_roofline(cat, ms, launches, work, info, pk, src, s):
         psrc = ("measured in this run: cuBLAS DGEMM 8192^3 (the FP64 products run on the DMMA "
                 "tensor path; FP64 has no tcgen05 kind)")
         ach = flops / t / 1e12 if t > 0 else 0.0
-        return {"bound": "tensor", "kernel": cat, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "traffic": None, "peak_source": psrc,
-                "launches_per_step": launches, "ms_per_step": ms}
+        tr = gemm_traffic() if (cat == "gemm" and config == "C5") else None
+        out = {"bound": "tensor", "kernel": cat, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+               "frac": ach / peak, "traffic": tr["traffic_bytes_per_launch"] if tr else None,
+               "peak_source": psrc, "launches_per_step": launches, "ms_per_step": ms}
+        if tr:
+            out["traffic_note"] = ("DRAM bytes per DMMA GEMM launch (read + write), mean over the "
+                                   f"{tr['launches']} launches of one C5 solve in profiles/gemm_dram_c5.json; "
+                                   f"{tr['traffic_bytes_per_step'] / 1e9:.1f} GB per solve, against "
+                                   f"{byts / 1e9:.1f} GB algorithmic bytes of the category")
+        return out
     peak = pk.get("hbm_gbs", 6650.0)
     ach = byts / t / 1e9 if t > 0 else 0.0
     del _lib, work, info
