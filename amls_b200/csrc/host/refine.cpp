@@ -36,7 +36,8 @@ int cdiv2(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 void sortByWork(std::vector<TileRef>& t, const std::vector<GemmDesc>& d) {
     auto work = [&](const TileRef& r) {
         const GemmDesc& g = d[static_cast<size_t>(r.desc)];
-        int64_t kb = 0, ke = g.K;
+        int64_t kb = g.kChunk > 0 ? static_cast<int64_t>(r.pad) * g.kChunk : 0;
+        int64_t ke = g.kChunk > 0 ? std::min<int64_t>(g.K, kb + g.kChunk) : g.K;
         if (g.flags & kTriKUpTo) ke = std::min<int64_t>(ke, r.n0 + kGemmTile);
         if (g.flags & kTriKFrom) kb = std::max<int64_t>(kb, r.n0);
         const int64_t rows = std::min<int64_t>(kGemmTile, g.M - r.m0);
@@ -301,6 +302,30 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
             sweep.insert(sweep.end(), d.begin(), d.end());
             for (TileRef& r : t) r.desc += base;
         };
+        // The backward products T_i -= X_S^T-gathered L_Si of the upper
+        // levels have few 64 x 64 tiles (N = n_i is small) and long K = s_i:
+        // below four waves of three CTAs per SM, split K into chunks of at
+        // least 256 (the kernel accumulates chunks with atomics; beta is 1).
+        {
+            constexpr int kWaveTiles = 4 * 3 * 148;
+            if (!bg.empty() && static_cast<int>(bgT.size()) < kWaveTiles) {
+                const int want = cdiv2(kWaveTiles, static_cast<int64_t>(bgT.size()));
+                bgT.clear();
+                for (size_t q = 0; q < bg.size(); ++q) {
+                    GemmDesc& h = bg[q];
+                    const int split = std::min(want, h.K / 256);
+                    int chunks = 1;
+                    if (split >= 2) {
+                        h.kChunk = (cdiv2(h.K, split) + 15) / 16 * 16;
+                        chunks = cdiv2(h.K, h.kChunk);
+                    }
+                    for (int kc = 0; kc < chunks; ++kc)
+                        for (int jt = 0; jt < cdiv2(h.N, kTB); ++jt)
+                            for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                                bgT.push_back({static_cast<int32_t>(q), it * kTB, jt * kTB, kc});
+                }
+            }
+        }
         sortByWork(ftT, ft);
         sortByWork(fgT, fg);
         sortByWork(bgT, bg);

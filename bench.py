@@ -180,6 +180,13 @@ def run_ours(args, rank, world, dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    if args.profile_range:
+        # one solve inside a profiler range (ncu --profile-from-start off), nothing else
+        torch.cuda.profiler.start()
+        step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        return None
     if dist:
         dist.barrier()
     # timed steps: uninstrumented (value); then the same number of steps with
@@ -565,6 +572,9 @@ def main():
                     help="arm timed as `value` (the other one is timed beside it)")
     ap.add_argument("--no-compare", action="store_true", help="skip the other precision arm")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch (C3) measurement")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="after the warm-up, run one solve inside a CUDA profiler range and exit "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--no-refine", action="store_true",
                     help="time the AMLS solve alone (not at the metric's accuracy)")
     args = ap.parse_args()
@@ -584,7 +594,7 @@ def main():
         d.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = d
     line = run_ours(args, rank, world, dist)
-    if rank == 0:
+    if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
