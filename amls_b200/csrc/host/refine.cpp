@@ -208,6 +208,10 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
     struct Tabs {
         size_t ftT, fgT, bgT, btT;
         int nft, nfg, nbg, nbt;
+        // outputs of the split-K triangular products (cleared before the
+        // launch, the chunks accumulate with atomics): first element and
+        // columns of each node's block of T (forward) and X (backward)
+        std::vector<std::pair<double*, int64_t>> ftZero, btZero;
     };
     std::vector<Tabs> tabs(static_cast<size_t>(maxLevel_) + 1);
     std::vector<GemmDesc> sweep;
@@ -325,6 +329,46 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
                                 bgT.push_back({static_cast<int32_t>(q), it * kTB, jt * kTB, kc});
                 }
             }
+        }
+        // The triangular products of the upper levels (n_i of hundreds to
+        // thousands, few nodes) have few tiles of very unequal K (k up to the
+        // tile's column, or from it): below four waves, split K into chunks
+        // of at least 256 as well, clearing the outputs first.
+        {
+            constexpr int kWaveTiles = 4 * 3 * 148;
+            auto splitTri = [&](std::vector<GemmDesc>& d, std::vector<TileRef>& t, bool upTo,
+                                std::vector<std::pair<double*, int64_t>>& zero) {
+                if (d.empty() || static_cast<int>(t.size()) >= kWaveTiles) return;
+                const int want = cdiv2(kWaveTiles, static_cast<int64_t>(t.size()));
+                bool any = false;
+                for (GemmDesc& g : d) {
+                    const int split = std::min(want, g.K / 256);
+                    if (split >= 2) {
+                        g.kChunk = (cdiv2(g.K, split) + 15) / 16 * 16;
+                        any = true;
+                    }
+                }
+                if (!any) return;
+                t.clear();
+                for (size_t q = 0; q < d.size(); ++q) {
+                    const GemmDesc& g = d[q];
+                    const int chunks = g.kChunk > 0 ? cdiv2(g.K, g.kChunk) : 1;
+                    if (g.kChunk > 0) zero.push_back({g.C, g.N});
+                    for (int jt = 0; jt < cdiv2(g.N, kTB); ++jt) {
+                        // K range of the tile's columns: [0, 64 (jt + 1)) or [64 jt, K)
+                        const int kLo = upTo ? 0 : jt * kTB, kHi = upTo ? std::min(g.K, (jt + 1) * kTB) : g.K;
+                        for (int kc = 0; kc < chunks; ++kc) {
+                            const int c0 = g.kChunk > 0 ? kc * g.kChunk : 0;
+                            const int c1 = g.kChunk > 0 ? std::min(g.K, c0 + g.kChunk) : g.K;
+                            if (c1 <= kLo || c0 >= kHi) continue;
+                            for (int it = 0; it < cdiv2(nq, kTB); ++it)
+                                t.push_back({static_cast<int32_t>(q), it * kTB, jt * kTB, kc});
+                        }
+                    }
+                }
+            };
+            splitTri(ft, ftT, true, tabs[static_cast<size_t>(l)].ftZero);
+            splitTri(bt, btT, false, tabs[static_cast<size_t>(l)].btZero);
         }
         sortByWork(ftT, ft);
         sortByWork(fgT, fg);
@@ -445,14 +489,23 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
             spmm(Y, X, keepR ? R : nullptr);
         }
         const GemmDesc* sw = b.dev<GemmDesc>(oSweep);
+        // clears the active rows [lock, nq) of split-K outputs (nq x cols blocks)
+        auto clearRows = [&](const std::vector<std::pair<double*, int64_t>>& z) {
+            for (const auto& [p0, cols] : z)
+                cudaCheck(cudaMemset2DAsync(p0 + lock, sizeof(double) * static_cast<size_t>(nq), 0,
+                                            sizeof(double) * static_cast<size_t>(nq - lock),
+                                            static_cast<size_t>(cols), s), "clear");
+        };
         for (int l = 0; l <= maxLevel_; ++l) {          // forward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
+            clearRows(T.ftZero);
             LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.ftT), T.nft, s));
             LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.fgT), T.nfg, s));
         }
         for (int l = maxLevel_; l >= 0; --l) {          // backward sweep
             const Tabs& T = tabs[static_cast<size_t>(l)];
             LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.bgT), T.nbg, s));
+            clearRows(T.btZero);
             LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.btT), T.nbt, s));
         }
         catF_[2] += fsolve * (nq - lock) / dq;
