@@ -216,8 +216,11 @@ public:
                     if (!s.busy) return true;
                 return false;
             });
+            // this process first (the call needs no copy of the graph; the
+            // root's separator, the largest call, always runs here), then
+            // the workers
             k = slots_.size();
-            for (size_t i = slots_.size(); i-- > 0;)   // workers first
+            for (size_t i = 0; i < slots_.size(); ++i)
                 if (!slots_[i].busy) {
                     k = i;
                     break;
