@@ -101,7 +101,7 @@ def test_sensitivities_two_element_types(solver):
 
 
 def test_c4_gradient_matches_golden_and_finite_differences(solver):
-    """Differentiation workload (BASELINE configuration: 27-node hex 10^3,
+    """Differentiation workload (27-node hex 10^3,
     26,460 DOF, 2,000 element parameters, nev 50, w_k ~ U[0, 1], simple modes
     with relative gap > 1e-6): the adjoint gradient of sum_k w_k lambda_k
     over all E_e and rho_e equals the gradient from the reference (ARPACK)
