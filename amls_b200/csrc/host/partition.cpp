@@ -95,36 +95,68 @@ Csr extractGraph(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t*
     return g;
 }
 
+// Subgraph induced by `verts` (ascending, as every vertex set of the
+// recursion is: the root's is 0..n-1 and a split keeps the order), vertices
+// renumbered by their position in `verts`.  The renumbering is increasing,
+// so each neighbour list stays sorted.  Large sets are counted and filled in
+// parallel over host threads (the top levels of the recursion, whose calls
+// are on its critical path while few other threads run).
 Csr inducedSubgraph(const Csr& g, const std::vector<int64_t>& verts, std::vector<int64_t>& localOf) {
     const int64_t m = static_cast<int64_t>(verts.size());
     localOf.assign(g.xadj.size() - 1, -1);
     for (int64_t i = 0; i < m; ++i) localOf[static_cast<size_t>(verts[static_cast<size_t>(i)])] = i;
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt == 0) nt = 1;
+    if (nt > 16) nt = 16;
+    if (m < 16384) nt = 1;
+    auto forRange = [&](auto&& fn) {
+        if (nt == 1) {
+            fn(int64_t{0}, m);
+            return;
+        }
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] { fn(m * t / nt, m * (t + 1) / nt); });
+        for (auto& x : th) x.join();
+    };
     Csr sub;
     sub.xadj.assign(static_cast<size_t>(m) + 1, 0);
-    std::vector<int64_t> tmp;
-    for (int64_t i = 0; i < m; ++i) {
-        const int64_t v = verts[static_cast<size_t>(i)];
-        tmp.clear();
-        for (int64_t p = g.xadj[static_cast<size_t>(v)]; p < g.xadj[static_cast<size_t>(v) + 1]; ++p) {
-            const int64_t u = g.adjncy[static_cast<size_t>(p)];
-            if (localOf[static_cast<size_t>(u)] >= 0) tmp.push_back(localOf[static_cast<size_t>(u)]);
+    forRange([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            const int64_t v = verts[static_cast<size_t>(i)];
+            int64_t c = 0;
+            for (int64_t p = g.xadj[static_cast<size_t>(v)]; p < g.xadj[static_cast<size_t>(v) + 1]; ++p)
+                c += localOf[static_cast<size_t>(g.adjncy[static_cast<size_t>(p)])] >= 0;
+            sub.xadj[static_cast<size_t>(i) + 1] = c;
         }
-        std::sort(tmp.begin(), tmp.end());
-        sub.xadj[static_cast<size_t>(i) + 1] = sub.xadj[static_cast<size_t>(i)] + static_cast<int64_t>(tmp.size());
-        sub.adjncy.insert(sub.adjncy.end(), tmp.begin(), tmp.end());
-    }
+    });
+    for (int64_t i = 0; i < m; ++i) sub.xadj[static_cast<size_t>(i) + 1] += sub.xadj[static_cast<size_t>(i)];
+    sub.adjncy.resize(static_cast<size_t>(sub.xadj.back()));
+    forRange([&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            const int64_t v = verts[static_cast<size_t>(i)];
+            int64_t o = sub.xadj[static_cast<size_t>(i)];
+            for (int64_t p = g.xadj[static_cast<size_t>(v)]; p < g.xadj[static_cast<size_t>(v) + 1]; ++p) {
+                const int64_t u = localOf[static_cast<size_t>(g.adjncy[static_cast<size_t>(p)])];
+                if (u >= 0) sub.adjncy[static_cast<size_t>(o++)] = u;
+            }
+        }
+    });
     return sub;
 }
 
 // In-process separator (serialised); part[v] in {0, 1, 2}, 2 = separator.
-std::vector<int64_t> bisectInProcess(Csr& g) {
+// METIS reads the graph arrays only (its coarsening builds new graphs), so
+// the caller's graph is passed as it is, without a copy.
+std::vector<int64_t> bisectInProcess(const Csr& g) {
     const int64_t n = static_cast<int64_t>(g.xadj.size()) - 1;
     std::vector<int64_t> part(static_cast<size_t>(n), 0);
     if (n == 0) return part;
     int rc;
     {
         std::lock_guard<std::mutex> lock(gMetisMutex);
-        rc = metisSeparator(n, g.xadj.data(), g.adjncy.data(), part.data());
+        rc = metisSeparator(n, const_cast<int64_t*>(g.xadj.data()), const_cast<int64_t*>(g.adjncy.data()),
+                            part.data());
     }
     if (rc != kMetisOk) throw std::runtime_error("METIS_ComputeVertexSeparator failed");
     return part;
@@ -207,7 +239,7 @@ public:
     SeparatorPool(const SeparatorPool&) = delete;
     SeparatorPool& operator=(const SeparatorPool&) = delete;
 
-    std::vector<int64_t> separator(Csr g) {
+    std::vector<int64_t> separator(const Csr& g) {
         size_t k;
         {
             std::unique_lock<std::mutex> lock(m_);
@@ -366,8 +398,8 @@ std::unique_ptr<Split> splitRec(const Csr& g, std::vector<int64_t> verts, int de
     }
     // the root's vertex set is all of g in order: its induced subgraph is g
     std::vector<int64_t> localOf;
-    Csr sub = depth == 0 ? g : inducedSubgraph(g, verts, localOf);
-    const std::vector<int64_t> part = pool.separator(std::move(sub));
+    const std::vector<int64_t> part =
+        depth == 0 ? pool.separator(g) : pool.separator(inducedSubgraph(g, verts, localOf));
     std::vector<int64_t> side[2], sep;
     for (int64_t i = 0; i < m; ++i) {
         const int64_t p = part[static_cast<size_t>(i)];
