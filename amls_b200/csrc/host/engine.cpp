@@ -4,6 +4,7 @@
 #include <chrono>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -308,10 +309,15 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
         subStart[static_cast<size_t>(i)] = s;
     }
 
-    // symbolic fill: S_i = ancestor DOFs coupled to node i after elimination
+    // symbolic fill: S_i = ancestor DOFs coupled to node i after elimination.
+    // A node's set needs the sets its descendants push up, so the nodes go
+    // level by level, those of one level in parallel over host threads; the
+    // pushes of a level are appended after it (S is sorted and deduplicated,
+    // so the order of the pushed entries does not matter).
     std::vector<std::vector<int32_t>> push(static_cast<size_t>(N));
-    std::vector<char> isAnc(static_cast<size_t>(N), 0);
-    for (int i : order_) {
+    std::vector<std::vector<int32_t>> up(static_cast<size_t>(N));     // node i's push to its first ancestor owner
+    std::vector<int> upTo(static_cast<size_t>(N), -1);
+    auto symbolic = [&](int i, std::vector<char>& isAnc) {
         Node& nd = nodes_[static_cast<size_t>(i)];
         for (int a : nd.anc) isAnc[static_cast<size_t>(a)] = 1;
         std::vector<int32_t> S = std::move(push[static_cast<size_t>(i)]);
@@ -340,12 +346,48 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
         if (!S.empty()) {
             const int a0 = owner_[static_cast<size_t>(S[0])];
             const Node& A0 = nodes_[static_cast<size_t>(a0)];
-            auto& dst = push[static_cast<size_t>(a0)];
+            auto& dst = up[static_cast<size_t>(i)];
             for (int32_t c : S)
                 if (c >= A0.off + A0.n) dst.push_back(c);
+            upTo[static_cast<size_t>(i)] = a0;
         }
         nd.S = std::move(S);
         for (int a : nd.anc) isAnc[static_cast<size_t>(a)] = 0;
+    };
+    {
+        unsigned nt = std::thread::hardware_concurrency();
+        nt = std::max(1u, std::min(nt, 32u));
+        for (int l = 0; l <= maxLevel_; ++l) {
+            const std::vector<int>& lv = byLevel_[static_cast<size_t>(l)];
+            const unsigned tn = std::min<unsigned>(nt, static_cast<unsigned>(lv.size()));
+            std::exception_ptr err;
+            std::mutex errMu;
+            std::atomic<size_t> next{0};
+            auto work = [&] {
+                std::vector<char> isAnc(static_cast<size_t>(N), 0);
+                try {
+                    for (size_t q = next++; q < lv.size(); q = next++) symbolic(lv[q], isAnc);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lk(errMu);
+                    if (!err) err = std::current_exception();
+                }
+            };
+            if (tn <= 1) {
+                work();
+            } else {
+                std::vector<std::thread> th;
+                for (unsigned t = 0; t < tn; ++t) th.emplace_back(work);
+                for (auto& x : th) x.join();
+            }
+            if (err) std::rethrow_exception(err);
+            for (int i : lv)
+                if (upTo[static_cast<size_t>(i)] >= 0) {
+                    auto& dst = push[static_cast<size_t>(upTo[static_cast<size_t>(i)])];
+                    const auto& src = up[static_cast<size_t>(i)];
+                    dst.insert(dst.end(), src.begin(), src.end());
+                    std::vector<int32_t>().swap(up[static_cast<size_t>(i)]);
+                }
+        }
     }
     // layout
     frontTotal_ = eigTotal_ = vecTotal_ = invTotal_ = 0;
@@ -426,6 +468,7 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
         std::vector<int32_t> ucols;
         std::vector<int64_t> dst(static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
         std::vector<int32_t> uni, tmp, pat;
+        std::vector<int32_t> posOf(static_cast<size_t>(n), -1);   // column -> position in the current union
         int64_t valOff = 0;
         auto groupEnd = [&](int64_t r) {
             const int64_t len = mp[r + 1] - mp[r];
@@ -436,7 +479,7 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
         };
         auto sortedPattern = [&](int64_t r, std::vector<int32_t>& out) {
             out.assign(mc + mp[r], mc + mp[r + 1]);
-            std::sort(out.begin(), out.end());
+            if (!std::is_sorted(out.begin(), out.end())) std::sort(out.begin(), out.end());
             out.erase(std::unique(out.begin(), out.end()), out.end());
         };
         int64_t r = 0;
@@ -460,9 +503,11 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
             S.colOff = static_cast<int64_t>(ucols.size());
             S.len = static_cast<int32_t>(uni.size());
             S.valOff = valOff;
+            // every column of rows r..e is in the union, so posOf is fresh for them
+            for (size_t t = 0; t < uni.size(); ++t) posOf[static_cast<size_t>(uni[t])] = static_cast<int32_t>(t);
             for (int64_t d = r; d < e; ++d)
                 for (int64_t q = mp[d]; q < mp[d + 1]; ++q) {
-                    const int64_t t = std::lower_bound(uni.begin(), uni.end(), mc[q]) - uni.begin();
+                    const int64_t t = posOf[static_cast<size_t>(mc[q])];
                     dst[static_cast<size_t>(q)] = valOff + t * kSpmmSuperRows + (d - r);
                 }
             ucols.insert(ucols.end(), uni.begin(), uni.end());

@@ -81,8 +81,14 @@ class Solution:
 
 
 def _csr_arrays(A):
-    A = sp.csr_matrix(A)
-    A.sort_indices()
+    """Row pointers (int64), columns (int32, sorted within rows) and values
+    of A as CSR; a CSR input with sorted indices is used as it is (no copy),
+    anything else is converted (the caller's matrix is never modified)."""
+    if not (sp.issparse(A) and A.format == "csr"):
+        A = sp.csr_matrix(A)
+    if not A.has_sorted_indices:
+        A = A.copy()
+        A.sort_indices()
     rp = np.ascontiguousarray(A.indptr, dtype=np.int64)
     ci = np.ascontiguousarray(A.indices, dtype=np.int32)
     v = np.ascontiguousarray(A.data, dtype=np.float64)
