@@ -785,8 +785,12 @@ void Engine::buildStatic() {
 // captured once into a CUDA graph and replayed by every later numeric solve
 // (the per-launch event instrumentation, when on, runs it eagerly).
 void Engine::eliminate(cudaStream_t s) {
-    if (profiling_) {
+    // The first numeric solve of an analysis launches eagerly (a one-shot
+    // solve, such as amls_solve, gains nothing from capturing); the second
+    // captures the fixed schedule into a graph that later solves replay.
+    if (profiling_ || (!elimExec_ && elimEagerRuns_ == 0)) {
         eliminateLaunches(s);
+        ++elimEagerRuns_;
         return;
     }
     if (!elimExec_) {
@@ -815,6 +819,7 @@ void Engine::dropGraphs() {
     if (elimExec_) cudaGraphExecDestroy(elimExec_);
     elimExec_ = nullptr;
     elimLaunches_ = 0;
+    elimEagerRuns_ = 0;
 }
 
 void Engine::eliminateLaunches(cudaStream_t s) {

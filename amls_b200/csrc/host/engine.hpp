@@ -324,6 +324,7 @@ private:
     bool profiling_ = false;
     cudaGraphExec_t elimExec_ = nullptr;            // captured elimination schedule
     int64_t elimLaunches_ = 0;                      // kernels in it
+    int elimEagerRuns_ = 0;                         // eager eliminations since the analysis
     std::vector<cudaEvent_t> evPool_;
     size_t evUsed_ = 0;
     std::vector<int> evCat_;

@@ -284,7 +284,7 @@ def test_elimination_graph_replay_matches_eager(solver):
     th = [np.zeros(40) for _ in range(3)]
     solver.set_profiling(True)           # eager launches, an event pair around each
     solver.solve_values(kv.ctypes.data, mv.ctypes.data, False, th[0].ctypes.data, None, False)
-    solver.set_profiling(False)          # captured on first use, then replayed
+    solver.set_profiling(False)          # captured at the second solve, then replayed
     for t in th[1:]:
         solver.solve_values(kv.ctypes.data, mv.ctypes.data, False, t.ctypes.data, None, False)
     assert rel_err(th[1], th[0]) < 1e-12
