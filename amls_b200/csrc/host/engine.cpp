@@ -10,6 +10,7 @@
 #include <cstring>
 #include <exception>
 #include <functional>
+#include <future>
 #include <iterator>
 #include <mutex>
 #include <thread>
@@ -91,6 +92,16 @@ Engine::Engine(int device) : device_(device) {
     cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device);
     status_.ensure(4 * sizeof(int));
+    // the result copy's pinned double buffer; without it copies go direct
+    void* pin = nullptr;
+    if (cudaHostAlloc(&pin, 2 * kPinChunk, cudaHostAllocDefault) == cudaSuccess &&
+        cudaEventCreateWithFlags(&pinEv_[0], cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&pinEv_[1], cudaEventDisableTiming) == cudaSuccess) {
+        pinRing_ = static_cast<char*>(pin);
+    } else {
+        cudaGetLastError();
+        if (pin) cudaFreeHost(pin);
+    }
 }
 
 Engine::~Engine() {
@@ -102,6 +113,49 @@ Engine::~Engine() {
     if (stream_) {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
+    }
+    for (cudaEvent_t e : pinEv_)
+        if (e) cudaEventDestroy(e);
+    if (pinRing_) cudaFreeHost(pinRing_);
+}
+
+// Device -> pageable host copy of a large result through the pinned double
+// buffer: chunk c + 1 is copied by the DMA engine while host threads move
+// chunk c into the destination (whose first touch also costs page faults,
+// spread over the threads).  Returns when dst holds the data.
+void Engine::copyToHost(double* dst, const double* src, size_t count, cudaStream_t s) {
+    const size_t bytes = count * sizeof(double);
+    if (!pinRing_ || bytes < 2 * kPinChunk) {
+        cudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "copy out");
+        cudaCheck(cudaStreamSynchronize(s), "copy out");
+        return;
+    }
+    const size_t nChunks = (bytes + kPinChunk - 1) / kPinChunk;
+    char* ring[2] = {pinRing_, pinRing_ + kPinChunk};
+    auto issue = [&](size_t c) {
+        const size_t off = c * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        cudaCheck(cudaMemcpyAsync(ring[c & 1], reinterpret_cast<const char*>(src) + off, len,
+                                  cudaMemcpyDeviceToHost, s), "copy out");
+        cudaCheck(cudaEventRecord(pinEv_[c & 1], s), "copy out");
+    };
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 4u));
+    issue(0);
+    for (size_t c = 0; c < nChunks; ++c) {
+        // the other buffer held chunk c - 1, already moved out below
+        if (c + 1 < nChunks) issue(c + 1);
+        cudaCheck(cudaEventSynchronize(pinEv_[c & 1]), "copy out");
+        const size_t off = c * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        char* d = reinterpret_cast<char*>(dst) + off;
+        const char* from = ring[c & 1];
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; ++t)
+            th.emplace_back([=] {
+                const size_t b = len * t / nt, e = len * (t + 1) / nt;
+                std::memcpy(d + b, from + b, e - b);
+            });
+        std::memcpy(d, from, len / nt);
+        for (auto& x : th) x.join();
     }
 }
 
@@ -220,6 +274,73 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
     std::vector<int64_t> post;
     nPencils_ = P;
     pOff_.assign(pOff, pOff + P + 1);
+    // super-rows for the products with M (they depend on M's pattern only):
+    // built on a host thread while the partition runs, uploaded below
+    struct SuperRows {
+        std::vector<SpmmSuper> sup;
+        std::vector<int32_t> ucols;
+        std::vector<int64_t> dst;
+        int64_t valOff = 0;
+    };
+    std::future<SuperRows> superRows = std::async(std::launch::async, [this, n, mp, mc]() {
+        std::vector<SpmmSuper> sup;
+        std::vector<int32_t> ucols;
+        std::vector<int64_t> dst(static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
+        std::vector<int32_t> uni, tmp, pat;
+        std::vector<int32_t> posOf(static_cast<size_t>(n), -1);   // column -> position in the current union
+        int64_t valOff = 0;
+        auto groupEnd = [&](int64_t r) {
+            const int64_t len = mp[r + 1] - mp[r];
+            int64_t e = r + 1;
+            while (e < n && e - r < kSpmmSuperRows && mp[e + 1] - mp[e] == len && std::equal(mc + mp[r], mc + mp[r + 1], mc + mp[e]))
+                ++e;
+            return e;
+        };
+        auto sortedPattern = [&](int64_t r, std::vector<int32_t>& out) {
+            out.assign(mc + mp[r], mc + mp[r + 1]);
+            if (!std::is_sorted(out.begin(), out.end())) std::sort(out.begin(), out.end());
+            out.erase(std::unique(out.begin(), out.end()), out.end());
+        };
+        int64_t r = 0;
+        while (r < n) {
+            int64_t e = groupEnd(r);
+            sortedPattern(r, uni);
+            while (e < n) {
+                const int64_t e2 = groupEnd(e);
+                if (e2 - r > kSpmmSuperRows) break;
+                sortedPattern(e, pat);
+                tmp.clear();
+                std::set_union(uni.begin(), uni.end(), pat.begin(), pat.end(), std::back_inserter(tmp));
+                if (static_cast<double>(tmp.size() - uni.size()) > 0.8 * static_cast<double>(pat.size())) break;
+                uni.swap(tmp);
+                e = e2;
+            }
+            SpmmSuper S{};
+            S.row0 = r;
+            S.pencil = static_cast<int32_t>(std::upper_bound(pOff_.begin(), pOff_.end(), r) - pOff_.begin() - 1);
+            S.rows = static_cast<int32_t>(e - r);
+            S.colOff = static_cast<int64_t>(ucols.size());
+            S.len = static_cast<int32_t>(uni.size());
+            S.valOff = valOff;
+            // every column of rows r..e is in the union, so posOf is fresh for them
+            for (size_t t = 0; t < uni.size(); ++t) posOf[static_cast<size_t>(uni[t])] = static_cast<int32_t>(t);
+            for (int64_t d = r; d < e; ++d)
+                for (int64_t q = mp[d]; q < mp[d + 1]; ++q) {
+                    const int64_t t = posOf[static_cast<size_t>(mc[q])];
+                    dst[static_cast<size_t>(q)] = valOff + t * kSpmmSuperRows + (d - r);
+                }
+            ucols.insert(ucols.end(), uni.begin(), uni.end());
+            valOff += static_cast<int64_t>(uni.size()) * kSpmmSuperRows;
+            sup.push_back(S);
+            r = e;
+        }
+        SuperRows out;
+        out.sup = std::move(sup);
+        out.ucols = std::move(ucols);
+        out.dst = std::move(dst);
+        out.valOff = valOff;
+        return out;
+    });
     pencilOf_.clear();
     pNodes_.assign(static_cast<size_t>(P), 0);
     perm_.clear();
@@ -464,57 +585,11 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
     // the union pattern, filled from the CSR values at each numeric solve
     // through supDst (CSR entry -> block position)
     {
-        std::vector<SpmmSuper> sup;
-        std::vector<int32_t> ucols;
-        std::vector<int64_t> dst(static_cast<size_t>(std::max<int64_t>(nnzM_, 1)));
-        std::vector<int32_t> uni, tmp, pat;
-        std::vector<int32_t> posOf(static_cast<size_t>(n), -1);   // column -> position in the current union
-        int64_t valOff = 0;
-        auto groupEnd = [&](int64_t r) {
-            const int64_t len = mp[r + 1] - mp[r];
-            int64_t e = r + 1;
-            while (e < n && e - r < kSpmmSuperRows && mp[e + 1] - mp[e] == len && std::equal(mc + mp[r], mc + mp[r + 1], mc + mp[e]))
-                ++e;
-            return e;
-        };
-        auto sortedPattern = [&](int64_t r, std::vector<int32_t>& out) {
-            out.assign(mc + mp[r], mc + mp[r + 1]);
-            if (!std::is_sorted(out.begin(), out.end())) std::sort(out.begin(), out.end());
-            out.erase(std::unique(out.begin(), out.end()), out.end());
-        };
-        int64_t r = 0;
-        while (r < n) {
-            int64_t e = groupEnd(r);
-            sortedPattern(r, uni);
-            while (e < n) {
-                const int64_t e2 = groupEnd(e);
-                if (e2 - r > kSpmmSuperRows) break;
-                sortedPattern(e, pat);
-                tmp.clear();
-                std::set_union(uni.begin(), uni.end(), pat.begin(), pat.end(), std::back_inserter(tmp));
-                if (static_cast<double>(tmp.size() - uni.size()) > 0.8 * static_cast<double>(pat.size())) break;
-                uni.swap(tmp);
-                e = e2;
-            }
-            SpmmSuper S{};
-            S.row0 = r;
-            S.pencil = static_cast<int32_t>(std::upper_bound(pOff_.begin(), pOff_.end(), r) - pOff_.begin() - 1);
-            S.rows = static_cast<int32_t>(e - r);
-            S.colOff = static_cast<int64_t>(ucols.size());
-            S.len = static_cast<int32_t>(uni.size());
-            S.valOff = valOff;
-            // every column of rows r..e is in the union, so posOf is fresh for them
-            for (size_t t = 0; t < uni.size(); ++t) posOf[static_cast<size_t>(uni[t])] = static_cast<int32_t>(t);
-            for (int64_t d = r; d < e; ++d)
-                for (int64_t q = mp[d]; q < mp[d + 1]; ++q) {
-                    const int64_t t = posOf[static_cast<size_t>(mc[q])];
-                    dst[static_cast<size_t>(q)] = valOff + t * kSpmmSuperRows + (d - r);
-                }
-            ucols.insert(ucols.end(), uni.begin(), uni.end());
-            valOff += static_cast<int64_t>(uni.size()) * kSpmmSuperRows;
-            sup.push_back(S);
-            r = e;
-        }
+        SuperRows sr = superRows.get();
+        std::vector<SpmmSuper>& sup = sr.sup;
+        std::vector<int32_t>& ucols = sr.ucols;
+        std::vector<int64_t>& dst = sr.dst;
+        const int64_t valOff = sr.valOff;
         nSup_ = static_cast<int64_t>(sup.size());
         supValTotal_ = valOff;
         supDesc_.ensure(sizeof(SpmmSuper) * std::max<size_t>(sup.size(), 1));
@@ -1612,7 +1687,7 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
     // outputs: pencil q's values at theta + q * nev (one pencil: theta[0 ..
     // want)); Z is n x nev column-major, pencil q in its own rows, columns
     // beyond its count zero
-    const int64_t zCols = Pn == 1 ? want[0] : nev;
+    const int64_t zCols = nev;   // every column of the caller's n x nev Z is written
     std::vector<double> th(static_cast<size_t>(Pn == 1 ? std::max(want[0], 1) : Pn * nev), 0.0);
     for (int q = 0; q < Pn; ++q)
         std::copy(P.theta[static_cast<size_t>(q)].begin(), P.theta[static_cast<size_t>(q)].end(),
@@ -1627,7 +1702,10 @@ void Engine::solveValues(const double* kv, const double* mv, bool valuesOnDevice
         std::copy(th.begin(), th.begin() + thN, theta);
     if (recover) {
         const int64_t mc = std::min<int64_t>(mZ, zCols);
-        if (mc > 0) cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * mc * n_, zk, s), "Z");
+        if (mc > 0) {
+            if (outputsOnDevice) cudaCheck(cudaMemcpyAsync(Z, zOut_.as<double>(), sizeof(double) * mc * n_, zk, s), "Z");
+            else copyToHost(Z, zOut_.as<double>(), static_cast<size_t>(mc * n_), s);
+        }
         if (zCols > mc) {
             if (outputsOnDevice)
                 cudaCheck(cudaMemsetAsync(Z + mc * n_, 0, sizeof(double) * (zCols - mc) * n_, s), "Z");

@@ -332,6 +332,11 @@ private:
     double profMs_[kProfCats] = {0};
     int64_t profCount_[kProfCats] = {0};
     cudaEvent_t evSolve0_ = nullptr, evSolve1_ = nullptr;
+    // pinned double buffer of the device -> host result copy (copyToHost)
+    static constexpr size_t kPinChunk = size_t(16) << 20;
+    char* pinRing_ = nullptr;
+    cudaEvent_t pinEv_[2] = {nullptr, nullptr};
+    void copyToHost(double* dst, const double* src, size_t count, cudaStream_t s);
 
     // diagnostics / ledger
     int64_t pA_ = 0, pFinal_ = 0, launches_ = 0;

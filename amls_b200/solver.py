@@ -194,7 +194,9 @@ class AmlsSolver:
         n = K.shape[0]
         nev = max(0, min(int(opt.nev), n))
         theta = np.zeros(max(nev, 1), np.float64)
-        Z = np.zeros((nev, n), np.float64) if opt.recoverVectors and nev > 0 else None
+        # every element of Z is written by the call (columns beyond the
+        # values found are zero); Z.T is the n x nev column-major result
+        Z = np.empty((nev, n), np.float64) if opt.recoverVectors and nev > 0 else None
         p = C.c_int64(0)
         timing = np.zeros(_lib.T_SLOTS, np.float64)
         o = opt.to_c()
@@ -203,7 +205,7 @@ class AmlsSolver:
                                          _lib.ptr(theta), _lib.ptr(Z), C.byref(p),
                                          _lib.ptr(timing)))
         self._last_nev = nev
-        return Solution(theta[:nev].copy(), None if Z is None else Z.T.copy(), int(p.value),
+        return Solution(theta[:nev].copy(), None if Z is None else Z.T, int(p.value),
                         dict(zip(_lib.TIMING_KEYS, timing.tolist())), self.info())
 
     # ---- batch of independent pencils (one launch sequence) ----
