@@ -653,7 +653,7 @@ void Engine::analyzeBatch(int P, const int64_t* pOff, const int64_t* kp, const i
 void Engine::extractGraphDevice(int64_t n, const int64_t* kp, const int32_t* kc, const int64_t* mp,
                                 const int32_t* mc, std::vector<int64_t>& xadj, std::vector<int64_t>& adj) {
     cudaStream_t s = stream_;
-    DevBuf dkp, dkc, dmp, dmc, dcnt, dadj;
+    DevBuf &dkp = grKp_, &dkc = grKc_, &dmp = grMp_, &dmc = grMc_, &dcnt = grCnt_, &dadj = grAdj_;
     const int64_t nk = kp[n], nm = mp[n];
     dkp.ensure(sizeof(int64_t) * (n + 1));
     dmp.ensure(sizeof(int64_t) * (n + 1));
@@ -677,9 +677,8 @@ void Engine::extractGraphDevice(int64_t n, const int64_t* kp, const int32_t* kc,
     LAUNCH(launchGraphFill(n, dkp.as<int64_t>(), dkc.as<int32_t>(), dmp.as<int64_t>(), dmc.as<int32_t>(),
                            dcnt.as<int64_t>(), dadj.as<int64_t>(), s));
     adj.resize(static_cast<size_t>(xadj.back()));
-    cudaCheck(cudaMemcpyAsync(adj.data(), dadj.as<int64_t>(), sizeof(int64_t) * adj.size(), cudaMemcpyDeviceToHost, s),
-              "graph");
-    cudaCheck(cudaStreamSynchronize(s), "graph");
+    static_assert(sizeof(int64_t) == sizeof(double), "the copy moves 8-byte words");
+    copyToHost(reinterpret_cast<double*>(adj.data()), dadj.as<double>(), adj.size(), s);
 }
 
 void Engine::buildStatic() {

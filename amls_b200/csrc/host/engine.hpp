@@ -332,6 +332,8 @@ private:
     double profMs_[kProfCats] = {0};
     int64_t profCount_[kProfCats] = {0};
     cudaEvent_t evSolve0_ = nullptr, evSolve1_ = nullptr;
+    // device buffers of the graph extraction for the partition (kept across analyses)
+    DevBuf grKp_, grKc_, grMp_, grMc_, grCnt_, grAdj_;
     // pinned double buffer of the device -> host result copy (copyToHost)
     static constexpr size_t kPinChunk = size_t(16) << 20;
     char* pinRing_ = nullptr;
