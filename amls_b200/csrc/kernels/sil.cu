@@ -54,20 +54,6 @@ __device__ __forceinline__ uint32_t lcgState(uint32_t seed, uint32_t calls) {
     return A * seed + C;
 }
 
-// Flat unit distribution: unit u of node b (units counted over the nodes
-// in order) goes to global warp (base + u) mod totalWarps.
-template <class F>
-__device__ __forceinline__ void forUnits(const SilDesc* D, int nDesc, int gw, int tw, F&& f) {
-    int base = 0;
-    for (int b = 0; b < nDesc; ++b) {
-        const int units = f(b, -1);            // query
-        if (units <= 0) continue;
-        int start = (gw - base) % tw;
-        if (start < 0) start += tw;
-        for (int u = start; u < units; u += tw) f(b, u);
-        base = (base + units) % tw;
-    }
-}
 }  // namespace
 
 // dst[r + c n] = the front's diagonal block: mode 0 the full symmetric copy of
@@ -144,32 +130,133 @@ cudaError_t launchSilShift(const SilShiftDesc* d, int nDesc, cudaStream_t s) {
 // active != 0 runs steps until state[0] (steps done) reaches `target` or a
 // breakdown (beta < 1e-13) sets state[1].  A node with no step done first
 // builds q_0 from the start vector.
+//
+// At the start of the launch and of every step each CTA reads the nodes'
+// states once into a shared table: which nodes take part, their step j, and
+// exclusive prefix sums of their row units (n) and basis units (j + 1).  A
+// phase's units are numbered over the table and dealt round-robin to the
+// grid's warps, which find their node by binary search in the prefix sums,
+// so a phase costs O(log nodes) per unit instead of a scan of all nodes.
+namespace {
+struct SilTable {
+    int* live;      // node takes part in this step (or, before the loop, is fresh)
+    int* j;         // its step count
+    int* rowPre;    // nDesc + 1: prefix of n over live nodes
+    int* basPre;    // nDesc + 1: prefix of j + 1 over live nodes
+};
+
+// exclusive prefix sum of v[0..n) into pre[0..n] by one CTA (chunked per
+// thread, then a scan of the per-thread totals through shared memory)
+__device__ __forceinline__ void ctaScan(const int* v, int* pre, int n, int* tot) {
+    const int t = threadIdx.x, T = blockDim.x;
+    const int per = (n + T - 1) / T, b0 = min(n, t * per), b1 = min(n, b0 + per);
+    int sum = 0;
+    for (int i = b0; i < b1; ++i) sum += v[i];
+    tot[t] = sum;
+    __syncthreads();
+    if (t == 0) {
+        int run = 0;
+        for (int k = 0; k < T; ++k) {
+            const int x = tot[k];
+            tot[k] = run;
+            run += x;
+        }
+        pre[n] = run;
+    }
+    __syncthreads();
+    int run = tot[t];
+    for (int i = b0; i < b1; ++i) {
+        pre[i] = run;
+        run += v[i];
+    }
+    __syncthreads();
+}
+
+// last node b with pre[b] <= U (pre non-decreasing, pre[0] = 0 <= U < pre[n])
+__device__ __forceinline__ int silFind(const int* pre, int n, int U) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= U) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class F>
+__device__ __forceinline__ void forRows(const SilTable& T, int nDesc, int gw, int tw, F&& f) {
+    const int total = T.rowPre[nDesc];
+    for (int U = gw; U < total; U += tw) {
+        const int b = silFind(T.rowPre, nDesc, U);
+        f(b, U - T.rowPre[b], T.j[b]);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void forBasis(const SilTable& T, int nDesc, int gw, int tw, F&& f) {
+    const int total = T.basPre[nDesc];
+    for (int U = gw; U < total; U += tw) {
+        const int b = silFind(T.basPre, nDesc, U);
+        f(b, U - T.basPre[b], T.j[b]);
+    }
+}
+}  // namespace
+
 __global__ void __launch_bounds__(kSilThreads) silLanczosKernel(const SilDesc* __restrict__ D, int nDesc,
                                                                   int maxSteps) {
     cg::grid_group grid = cg::this_grid();
+    extern __shared__ int silSm[];
     __shared__ double red[32];
+    __shared__ int tot[kSilThreads];
+    __shared__ int anyLive;
+    SilTable T;
+    T.live = silSm;
+    T.j = silSm + nDesc;
+    T.rowPre = silSm + 2 * nDesc;
+    T.basPre = silSm + 3 * nDesc + 1;
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * kSilWarps + (threadIdx.x >> 5);
     const int tw = gridDim.x * kSilWarps;
 
-    // mw = M^ w for the nodes selected by `pick` (warp per row)
-    auto mprod = [&](auto pick) {
-        forUnits(D, nDesc, gw, tw, [&](int b, int u) -> int {
+    // the table from the nodes' states: mode 0 = fresh nodes (no step done),
+    // mode 1 = nodes live in this step; row units in rowPre, basis units in
+    // basPre (T.j doubles as the unit buffer for each scan in turn)
+    auto buildTable = [&](int mode) {
+        for (int b = threadIdx.x; b < nDesc; b += blockDim.x) {
             const SilDesc& d = D[b];
-            if (u < 0) return pick(b) ? d.n : 0;
+            const int s0 = __ldcg(d.state), s1 = __ldcg(d.state + 1);
+            const bool on = mode == 0 ? (d.active && s0 == 0 && d.target > 0)
+                                      : (d.active && s1 == 0 && s0 < d.target);
+            T.live[b] = on ? 1 : 0;
+            T.j[b] = on ? d.n : 0;          // row units, scanned first
+        }
+        __syncthreads();
+        ctaScan(T.j, T.rowPre, nDesc, tot);
+        for (int b = threadIdx.x; b < nDesc; b += blockDim.x)
+            T.j[b] = T.live[b] ? __ldcg(D[b].state) + 1 : 0;   // basis units
+        __syncthreads();
+        ctaScan(T.j, T.basPre, nDesc, tot);
+        for (int b = threadIdx.x; b < nDesc; b += blockDim.x) T.j[b] = __ldcg(D[b].state);
+        if (threadIdx.x == 0) anyLive = T.rowPre[nDesc] > 0;
+        __syncthreads();
+    };
+
+    // mw = M^ w for the table's nodes (warp per row)
+    auto mprod = [&]() {
+        forRows(T, nDesc, gw, tw, [&](int b, int u, int) {
+            const SilDesc& d = D[b];
             double acc = 0.0;
             for (int e = d.mRow[u] + lane; e < d.mRow[u + 1]; e += 32)
                 acc = fma(d.mBase[d.mOff[e]], __ldcg(d.w + d.mCol[e]), acc);
             acc = warpSum<32>(acc);
             if (lane == 0) d.mw[u] = acc;
-            return 0;
         });
     };
 
     // ---- start vector for nodes with no step done ----
-    auto fresh = [&](int b) { return D[b].active && __ldcg(D[b].state) == 0 && D[b].target > 0; };
+    buildTable(0);
     for (int b = 0; b < nDesc; ++b) {
-        if (!fresh(b)) continue;
+        if (!T.live[b]) continue;
         const SilDesc& d = D[b];
         for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < d.n; r += gridDim.x * blockDim.x) {
             const uint32_t x = lcgState(12345u, (uint32_t)r + 1u);
@@ -178,10 +265,10 @@ __global__ void __launch_bounds__(kSilThreads) silLanczosKernel(const SilDesc* _
         }
     }
     grid.sync();
-    mprod(fresh);
+    mprod();
     grid.sync();
     for (int b = blockIdx.x; b < nDesc; b += gridDim.x) {
-        if (!fresh(b)) continue;
+        if (!T.live[b]) continue;
         const SilDesc& d = D[b];
         double s2 = 0.0;
         for (int r = threadIdx.x; r < d.n; r += blockDim.x) s2 += __ldcg(d.w + r) * __ldcg(d.mw + r);
@@ -197,34 +284,24 @@ __global__ void __launch_bounds__(kSilThreads) silLanczosKernel(const SilDesc* _
     grid.sync();
 
     for (int step = 0; step < maxSteps; ++step) {
-        // the same decision in every CTA (states read after the barrier)
-        auto live = [&](int b) {
-            const SilDesc& d = D[b];
-            return d.active && __ldcg(d.state + 1) == 0 && __ldcg(d.state) < d.target;
-        };
-        bool any = false;
-        for (int b = 0; b < nDesc; ++b) any = any || live(b);
-        if (!any) break;
+        // the same table in every CTA (states read after the barrier)
+        buildTable(1);
+        if (!anyLive) break;
         // P1: w = B (M q_j)    (warp per row; B symmetric: row r = column r)
-        forUnits(D, nDesc, gw, tw, [&](int b, int u) -> int {
+        forRows(T, nDesc, gw, tw, [&](int b, int u, int j) {
             const SilDesc& d = D[b];
-            if (u < 0) return live(b) ? d.n : 0;
-            const int j = __ldcg(d.state);
             const double* bc = d.B + (int64_t)u * d.n;
             const double* mq = d.MQ + (int64_t)j * d.n;
             double acc = 0.0;
             for (int c = lane; c < d.n; c += 32) acc = fma(__ldg(bc + c), __ldcg(mq + c), acc);
             acc = warpSum<32>(acc);
             if (lane == 0) d.w[u] = acc;
-            return 0;
         });
         grid.sync();
         for (int pass = 0; pass < 2; ++pass) {
             // P2/P4: coef_l = (M q_l)^T w, l = 0 .. j (warp per l); alpha_j from the first pass
-            forUnits(D, nDesc, gw, tw, [&](int b, int u) -> int {
+            forBasis(T, nDesc, gw, tw, [&](int b, int u, int j) {
                 const SilDesc& d = D[b];
-                const int j = __ldcg(d.state);
-                if (u < 0) return live(b) ? j + 1 : 0;
                 const double* mq = d.MQ + (int64_t)u * d.n;
                 double acc = 0.0;
                 for (int r = lane; r < d.n; r += 32) acc = fma(__ldcg(mq + r), __ldcg(d.w + r), acc);
@@ -233,31 +310,27 @@ __global__ void __launch_bounds__(kSilThreads) silLanczosKernel(const SilDesc* _
                     d.coef[u] = acc;
                     if (pass == 0 && u == j) d.alpha[j] = acc;
                 }
-                return 0;
             });
             grid.sync();
             // P3/P5: w -= Q coef (warp per row, contiguous over l in Q^T)
-            forUnits(D, nDesc, gw, tw, [&](int b, int u) -> int {
+            forRows(T, nDesc, gw, tw, [&](int b, int u, int j) {
                 const SilDesc& d = D[b];
-                if (u < 0) return live(b) ? d.n : 0;
-                const int j = __ldcg(d.state);
                 const double* qt = d.QT + (int64_t)u * d.n;
                 double acc = 0.0;
                 for (int l = lane; l <= j; l += 32) acc = fma(__ldcg(qt + l), __ldcg(d.coef + l), acc);
                 acc = warpSum<32>(acc);
                 if (lane == 0) d.w[u] = __ldcg(d.w + u) - acc;
-                return 0;
             });
             grid.sync();
         }
         // P6: mw = M^ w
-        mprod(live);
+        mprod();
         grid.sync();
         // P7: beta_j = ||w||_M, q_{j+1} = w / beta_j (CTA per node)
         for (int b = blockIdx.x; b < nDesc; b += gridDim.x) {
-            if (!live(b)) continue;
+            if (!T.live[b]) continue;
             const SilDesc& d = D[b];
-            const int j = __ldcg(d.state);
+            const int j = T.j[b];
             double s2 = 0.0;
             for (int r = threadIdx.x; r < d.n; r += blockDim.x) s2 += __ldcg(d.w + r) * __ldcg(d.mw + r);
             s2 = blockSum(s2, red);
@@ -285,21 +358,39 @@ __global__ void __launch_bounds__(kSilThreads) silLanczosKernel(const SilDesc* _
     }
 }
 
-int silLanczosMaxCtas() {
+namespace {
+// nodes per cooperative launch (the shared table holds 4 ints per node)
+constexpr int kSilMaxDesc = 4096;
+
+int silLanczosMaxCtas(size_t smem) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, silLanczosKernel, kSilThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, silLanczosKernel, kSilThreads, smem);
     if (per > 4) per = 4;
     return per * sms;
 }
+}  // namespace
 
 cudaError_t launchSilLanczos(const SilDesc* d, int nDesc, int maxSteps, cudaStream_t s) {
-    if (nDesc <= 0) return cudaSuccess;
-    const int nCta = silLanczosMaxCtas();
-    if (nCta < 1) return cudaErrorCooperativeLaunchTooLarge;
-    void* args[] = {(void*)&d, (void*)&nDesc, (void*)&maxSteps};
-    return cudaLaunchCooperativeKernel((void*)silLanczosKernel, dim3(nCta), dim3(kSilThreads), args, 0, s);
+    // independent nodes: chunks of at most kSilMaxDesc, one launch each
+    for (int b0 = 0; b0 < nDesc; b0 += kSilMaxDesc) {
+        int nb = nDesc - b0 < kSilMaxDesc ? nDesc - b0 : kSilMaxDesc;
+        const size_t smem = sizeof(int) * (4 * static_cast<size_t>(nb) + 2);
+        if (smem > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(silLanczosKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(smem));
+            if (e != cudaSuccess) return e;
+        }
+        const int nCta = silLanczosMaxCtas(smem);
+        if (nCta < 1) return cudaErrorCooperativeLaunchTooLarge;
+        const SilDesc* dc = d + b0;
+        void* args[] = {(void*)&dc, (void*)&nb, (void*)&maxSteps};
+        const cudaError_t e = cudaLaunchCooperativeKernel((void*)silLanczosKernel, dim3(nCta), dim3(kSilThreads), args,
+                                                          smem, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // Count thresholds and Ritz scalings.  thr[b] = 1 / (hi_b - sigma_b): a Ritz
