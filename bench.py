@@ -54,7 +54,7 @@ CONFIGS = {
 
 REFINE = 3          # K^-1 M applications per Rayleigh-Ritz step (Chebyshev degree 2 + 1)
 REFINE_EXTRA = 200  # subspace vectors beyond nev
-REFINE_TOL = 1e-9   # target relative eigenvalue error
+REFINE_TOL = 1e-8   # target relative eigenvalue error: the metric's accuracy bound
 
 
 def workload(name, refine=True, precision="mixed"):
