@@ -21,11 +21,13 @@ host clock around the synchronous call.
 
 Reference arm (--impl reference): the reference algorithm restated in C++
 (oracle/amls_cpu.cpp, checked against the Python restatement by
-tests/test_oracle_cpu.py) on the host cores, each step one full C5 solve on
-the fixture tree of the same partition (no product code loaded); when the
-requested steps would not end within AMLS_REF_BUDGET_S (600 s) fewer are
-timed and the line's `steps` says how many.  The same full run, once, is
-our arm's `cpu_baseline`.
+tests/test_oracle_cpu.py) on the host cores, each step one full C5 solve as
+the reference's AmlsSolver::solve runs it, its nested-dissection partition
+included (the sequential restatement oracle/metis_seq.cpp, which reproduces
+the fixture tree; no product code loaded); when the requested steps would
+not end within AMLS_REF_BUDGET_S (600 s) fewer are timed and the line's
+`steps` says how many.  The same full run, once, is our arm's
+`cpu_baseline`.
 """
 from __future__ import annotations
 
@@ -383,10 +385,9 @@ def run_batch(args, rank, world, dist):
     s.close()
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import cpu
-        from amls_b200.solver import recursive_bisection
         cores = os.cpu_count() or 1
         sample = ps[:16]
-        trees = [recursive_bisection(p.K, p.M, 6, 500)[1] for p in sample]
+        trees = [cpu.sequential_partition(p.K, p.M, 6, 500)[1] for p in sample]
         t0 = time.perf_counter()
         for p, tr in zip(sample, trees):
             cpu.solve(p.K, p.M, tr, 10, threads=cores)
@@ -470,25 +471,38 @@ def dominant_roofline(cat, ms, launches, work, info, pk, src, s, config="C5"):
 
 def c5_tree():
     """The C5 separator tree from its fixture (tests/golden/c5_tree.npz, made
-    by the host partitioner): the CPU runs use it without calling the
-    product's partitioner."""
+    by the host partitioner): the CPU runs check that their own sequential
+    partition reproduces it."""
     g = np.load(os.path.join(ROOT, "tests", "golden", "c5_tree.npz"))
     return {k: g[k].astype(np.int64) for k in ("parent", "left", "right", "idx_ptr", "idx")}
 
 
-def cpu_full_solve(p, tree, threads, nev=500):
-    """One full AMLS solve (eta 2, elimination per pass, vectors) by the C++
-    restatement of the reference algorithm, timed on the host."""
+def cpu_full_solve(p, threads, nev, n_levels, expect_tree=None):
+    """One full AMLS solve as the reference's AmlsSolver::solve runs it, timed
+    on the host: the nested-dissection partition inside the call
+    (solver.cpp:124-134; the sequential restatement oracle/metis_seq.cpp, one
+    thread like the reference's), then elimination per pass, dense local
+    dsygvx, projection, reduced dsygvx and back-transform with vectors
+    (oracle/amls_cpu.cpp).  expect_tree: a fixture the partition must
+    reproduce."""
     from oracle import cpu
     t0 = time.perf_counter()
+    _, tree = cpu.sequential_partition(p.K, p.M, n_levels, 500)
+    t_part = time.perf_counter() - t0
+    if expect_tree is not None:
+        for k, v in expect_tree.items():
+            if not np.array_equal(np.asarray(tree[k], np.int64), v):
+                raise RuntimeError(f"sequential partition differs from the fixture tree ({k})")
     th, _, pp, pa, tm = cpu.solve(p.K, p.M, tree, nev, eta=2.0, vectors=True, threads=threads)
+    tm = dict(partition=t_part, **tm)
     return time.perf_counter() - t0, pp, pa, tm
 
 
 def cpu_baseline_line(t, cores, pp, pa, tm, runs, config="C5"):
     return {"value": t, "unit": "s", "cores": cores, "kind": "port",
             "sample": (f"the full {config} workload ({runs} run{'s' if runs > 1 else ''}, no scaling): the "
-                       f"reference algorithm restated in C++ (oracle/amls_cpu.cpp: elimination re-run "
+                       f"reference algorithm restated in C++ (the sequential nested-dissection partition "
+                       f"of oracle/metis_seq.cpp, then oracle/amls_cpu.cpp: elimination re-run "
                        f"per pass, dense local dsygvx, projection, reduced dsygvx, back-transform, "
                        f"M-normalisation), OpenBLAS single-threaded per call and {cores} host threads "
                        f"over the nodes of a tree level as the reference runs; p = {pp} (pass A "
@@ -503,12 +517,8 @@ def cpu_sample(args):
     cores = os.cpu_count() or 1
     cfg = CONFIGS[args.config]
     p = cases.config_pencil(args.config, seed=0)
-    if args.config == "C5":
-        tree = c5_tree()
-    else:
-        from oracle import cpu
-        tree = cpu.sequential_partition(p.K, p.M, cfg["nLevels"], 500)[1]
-    t, pp, pa, tm = cpu_full_solve(p, tree, cores, cfg["nev"])
+    t, pp, pa, tm = cpu_full_solve(p, cores, cfg["nev"], cfg["nLevels"],
+                                   c5_tree() if args.config == "C5" else None)
     return cpu_baseline_line(t, cores, pp, pa, tm, 1, args.config)
 
 
@@ -523,19 +533,20 @@ def run_reference(args, rank, world):
     cores = os.cpu_count() or 1
     p = cases.config_pencil("C5", seed=0)
     tree = c5_tree()
+    nl = CONFIGS["C5"]["nLevels"]
     budget = float(os.environ.get("AMLS_REF_BUDGET_S", "600"))
     t_start = time.perf_counter()
-    t, pp, pa, tm = cpu_full_solve(p, tree, cores)            # first warm-up step
+    t, pp, pa, tm = cpu_full_solve(p, cores, 500, nl, tree)   # first warm-up step
     warm = 1
     while warm < args.warmup and (time.perf_counter() - t_start) + t * (args.steps + 1) < budget:
-        cpu_full_solve(p, tree, cores)
+        cpu_full_solve(p, cores, 500, nl, tree)
         warm += 1
     times = []
     last = (pp, pa, tm)
     for _ in range(args.steps):
         if times and (time.perf_counter() - t_start) + float(np.mean(times)) > budget:
             break
-        tt, pp, pa, tm = cpu_full_solve(p, tree, cores)
+        tt, pp, pa, tm = cpu_full_solve(p, cores, 500, nl, tree)
         times.append(tt)
         last = (pp, pa, tm)
     v = float(np.mean(times))
