@@ -33,6 +33,7 @@ from __future__ import annotations
 
 import argparse
 import dataclasses
+import functools
 import json
 import os
 import subprocess
@@ -309,6 +310,7 @@ def run_ours(args, rank, world, dist):
     dom_ms, dom_launches = ktimes[dom]
     roof = dominant_roofline(dom, dom_ms / max(args.steps, 1), dom_launches / max(args.steps, 1),
                              work, info, pk, src, s, args.config)
+    phases = phase_roofline(ktimes, max(args.steps, 1), s, t_step, pk)
     line = {
         "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
@@ -322,6 +324,7 @@ def run_ours(args, rank, world, dist):
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(info["launches"]),
         "roofline": roof,
+        "roofline_phases": phases,
         "clocks": clk.summary(),
         "wall_s_per_step": wall / max(args.steps, 1),
         "instrumented_s_per_step": float(np.mean(prof_times)),
@@ -408,8 +411,10 @@ def exact_eigenvalues(config, nev):
     return np.load(path)[key][:nev], name
 
 
+@functools.lru_cache(maxsize=None)
 def fp64_gemm_peak():
-    """cuBLAS DGEMM throughput on this GPU now (8192^3, best of 3), TFLOP/s."""
+    """cuBLAS DGEMM throughput on this GPU now (8192^3, best of 3), TFLOP/s;
+    measured once per process."""
     import torch
     a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
     b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
@@ -463,6 +468,28 @@ def dominant_roofline(cat, ms, launches, work, info, pk, src, s, config="C5"):
     return {"bound": "hbm", "kernel": cat, "achieved": ach, "peak": peak, "unit": "GB/s",
             "frac": ach / peak, "traffic": None, "peak_source": src,
             "launches_per_step": launches, "ms_per_step": ms}
+
+
+def phase_roofline(ktimes, steps, s, t_step, pk):
+    """Per kernel category of one solve: the engine's ledger of algorithmic
+    flops and bytes, the roofline time max(F / FP64 peak, B / HBM peak), the
+    measured time and their ratio; and the whole solve's sum of roofline
+    times over the measured step."""
+    led = s.category_work()
+    p64 = fp64_gemm_peak() * 1e12
+    bw = pk.get("hbm_gbs", 6650.0) * 1e9
+    rows, t_roof = {}, 0.0
+    for k, (ms, n) in ktimes.items():
+        f, b = led.get(k, (0.0, 0.0))
+        t = ms / steps * 1e-3
+        tr = max(f / p64, b / bw)
+        t_roof += tr
+        rows[k] = {"ms": t * 1e3, "gflop": f / 1e9, "gbyte": b / 1e9, "roof_ms": tr * 1e3,
+                   "bound": "fp64" if f / p64 >= b / bw else "hbm",
+                   "frac": tr / t if t > 0 else None, "launches": n / steps}
+    return {"per_category": rows, "roof_ms": t_roof * 1e3, "step_ms": t_step * 1e3,
+            "frac_whole_solve": t_roof / t_step if t_step > 0 else None,
+            "peaks": {"fp64_tflops": p64 / 1e12, "hbm_gbs": bw / 1e9}}
 
 
 # --------------------------------------------------------------------------
