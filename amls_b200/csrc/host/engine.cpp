@@ -894,6 +894,9 @@ void Engine::dropGraphs() {
     elimExec_ = nullptr;
     elimLaunches_ = 0;
     elimEagerRuns_ = 0;
+    for (auto& kv : applyGraphs_) cudaGraphExecDestroy(kv.second.first);
+    applyGraphs_.clear();
+    refineEagerRuns_ = 0;
 }
 
 void Engine::eliminateLaunches(cudaStream_t s) {

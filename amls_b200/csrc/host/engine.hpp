@@ -22,6 +22,7 @@
 //   back-transform z = L^-T S q (subspace_condensation.cpp:263-319),
 //     un-permutation and M-normalisation (solver.cpp:302-311).
 #pragma once
+#include <array>
 #include <chrono>
 #include <cstdint>
 #include <map>
@@ -325,6 +326,12 @@ private:
     cudaGraphExec_t elimExec_ = nullptr;            // captured elimination schedule
     int64_t elimLaunches_ = 0;                      // kernels in it
     int elimEagerRuns_ = 0;                         // eager eliminations since the analysis
+    // the refinement's K^-1 M applications (an M product and the forward and
+    // backward sweeps over the tree levels), captured per (locked rows,
+    // operand and output buffers) from the second refinement of an analysis
+    // on and replayed after: graph and the kernels in it
+    std::map<std::array<uintptr_t, 9>, std::pair<cudaGraphExec_t, int64_t>> applyGraphs_;
+    int refineEagerRuns_ = 0;                       // eager refinements since the analysis
     std::vector<cudaEvent_t> evPool_;
     size_t evUsed_ = 0;
     std::vector<int> evCat_;

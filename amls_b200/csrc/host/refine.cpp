@@ -470,23 +470,29 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
         cudaCheck(cudaMemcpyAsync(b.dev<GemmDesc>(oSweep), act.data(), sizeof(GemmDesc) * act.size(),
                                   cudaMemcpyHostToDevice, s), "lock");
     };
-    auto spmm = [&](const double* Y, double* out, double* out2) {
-        const int m = nq - lock;
+    auto spmmLaunch = [&](const double* Y, double* out, double* out2) {
         LAUNCH(launchSpmmSuperT(supDesc_.as<SpmmSuper>(), nSup_, supCols_.as<int32_t>(), supVal_.as<double>(),
-                                invDev_.as<int64_t>(), Y + lock, m, nq, out + lock, s,
+                                invDev_.as<int64_t>(), Y + lock, nq - lock, nq, out + lock, s,
                                 out2 ? out2 + lock : nullptr));
+    };
+    auto spmmWork = [&]() {
+        const int m = nq - lock;
         catF_[8] += 2.0 * nnzM_ * m;
         catB_[8] += 12.0 * nnzM_ + 16.0 * dn * m;
+    };
+    auto spmm = [&](const double* Y, double* out, double* out2) {
+        spmmLaunch(Y, out, out2);
+        spmmWork();
     };
     // the K^-1 M application on Y (nq x n): X = K^-1 (M Y), with M Y given or
     // formed; keepR keeps R = M Y (= K X, for the Rayleigh-Ritz step), the
     // filter's inner applications form M Y in X directly
-    auto applyT = [&](const double* Y, const double* MY, bool keepR) {
+    auto applyLaunches = [&](const double* Y, const double* MY, bool keepR) {
         if (MY) {
             cudaCheck(cudaMemcpyAsync(X, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
             if (keepR) cudaCheck(cudaMemcpyAsync(R, MY, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s), "copy");
         } else {
-            spmm(Y, X, keepR ? R : nullptr);
+            spmmLaunch(Y, X, keepR ? R : nullptr);
         }
         const GemmDesc* sw = b.dev<GemmDesc>(oSweep);
         // clears the active rows [lock, nq) of split-K outputs (nq x cols blocks)
@@ -508,6 +514,47 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
             clearRows(T.btZero);
             LAUNCH(launchGemmBatched(sw, b.dev<TileRef>(T.btT), T.nbt, s));
         }
+    };
+    // The first refinement of an analysis launches eagerly (a one-shot solve
+    // gains nothing from capturing); later ones capture each application the
+    // first time its locked rows and buffers occur and replay the graph after
+    // (the sweep descriptors it reads are re-uploaded in place, so a replay
+    // sees the current ones).
+    const bool useGraphs = !profiling_ && refineEagerRuns_ > 0;
+    auto applyT = [&](const double* Y, const double* MY, bool keepR) {
+        if (!useGraphs) {
+            applyLaunches(Y, MY, keepR);
+        } else {
+            const std::array<uintptr_t, 9> key{static_cast<uintptr_t>(lock), reinterpret_cast<uintptr_t>(Y),
+                                               reinterpret_cast<uintptr_t>(MY), keepR ? 1u : 0u,
+                                               reinterpret_cast<uintptr_t>(X), reinterpret_cast<uintptr_t>(R),
+                                               reinterpret_cast<uintptr_t>(b.dev<char>(0)),
+                                               static_cast<uintptr_t>(nq), static_cast<uintptr_t>(n)};
+            auto it = applyGraphs_.find(key);
+            if (it == applyGraphs_.end()) {
+                cudaGraph_t g = nullptr;
+                cudaCheck(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "capture refinement");
+                const int64_t l0 = launches_;
+                try {
+                    applyLaunches(Y, MY, keepR);
+                } catch (...) {
+                    cudaStreamEndCapture(s, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                cudaCheck(cudaStreamEndCapture(s, &g), "capture refinement");
+                const int64_t cnt = launches_ - l0;
+                launches_ = l0;
+                cudaGraphExec_t ex = nullptr;
+                const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+                cudaGraphDestroy(g);
+                cudaCheck(e, "instantiate refinement graph");
+                it = applyGraphs_.emplace(key, std::make_pair(ex, cnt)).first;
+            }
+            cudaCheck(cudaGraphLaunch(it->second.first, s), "launch refinement graph");
+            launches_ += it->second.second;
+        }
+        if (!MY) spmmWork();
         catF_[2] += fsolve * (nq - lock) / dq;
     };
     // Chebyshev recurrence buffers (degree = refine - 1)
@@ -635,6 +682,7 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
         }
     }
     theta = prev;
+    if (!useGraphs) ++refineEagerRuns_;
     checkStatus("refinement");
     return it;
 }

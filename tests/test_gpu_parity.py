@@ -273,9 +273,10 @@ def test_invalid_precision(solver):
 
 
 def test_elimination_graph_replay_matches_eager(solver):
-    """The numeric solve replays the elimination as a captured CUDA graph
-    (with per-launch instrumentation off); it gives the eager launches'
-    eigenvalues (up to the order of the extend-add atomics), also on repeat."""
+    """The numeric solve replays the elimination and the refinement's K^-1 M
+    applications as captured CUDA graphs (with per-launch instrumentation
+    off); it gives the eager launches' eigenvalues (up to the order of the
+    extend-add and split-K atomics), also on repeat."""
     p = cases.hex_pencil(8, 8, 8, 1, seed=5)
     o = AmlsOptions(nev=40, nLevels=4, leafSize=200, refine=3)
     solver.analyze(p.K, p.M, o)
