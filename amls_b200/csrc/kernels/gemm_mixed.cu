@@ -21,7 +21,9 @@
 // commits them to the stage's mbarrier, which the loaders wait on before
 // reusing the stage.  The accumulator (128 lanes x 128 FP32 columns of
 // tensor memory) is read back with tcgen05.ld (warp w: lanes 32 (w % 4),
-// columns 64 (w / 4)).  Every mbarrier wait is bounded; on a timeout the
+// columns 64 (w / 4)).  Two CTAs share an SM (64 KB of shared memory and 128
+// tensor-memory columns each), so one CTA's global loads and split overlap
+// the other's.  Every mbarrier wait is bounded; on a timeout the
 // kernel records kDevTimeout in the status word, waits (bounded) for its
 // own MMAs, frees its tensor memory and returns.
 #include <cuda_bf16.h>
@@ -92,21 +94,30 @@ __device__ __forceinline__ bool waitParity(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void splitBf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-    hi = __double2bfloat16(x);
-    lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
-}
-
 // One 8-element K chunk of one operand row into the hi/lo slices: row r (of
 // 128), chunk c (of 4) -> byte offset ((r / 8) * 4 + c) * 128 + (r % 8) * 16.
+// The split goes through FP32: x32 = fp32(x), hi = bf16(x32), lo =
+// bf16(x32 - hi) (the subtraction is exact), so x = hi + lo + r with
+// |r| <= (2^-17 + 2^-24) |x|, the same order as splitting in FP64; per pair
+// of elements it costs two FP64->FP32 conversions, two FP32 subtractions and
+// two packed FP32->BF16x2 conversions.
 __device__ __forceinline__ void storeChunk(uint8_t* hiBase, uint8_t* loBase, int r, int c,
                                            const double (&x)[8]) {
-    __align__(16) __nv_bfloat16 h[8], l[8];
+    uint4 h, l;
+    uint32_t* hw = &h.x;
+    uint32_t* lw = &l.x;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) splitBf16(x[e], h[e], l[e]);
+    for (int e = 0; e < 4; ++e) {
+        const float a = static_cast<float>(x[2 * e]), b = static_cast<float>(x[2 * e + 1]);
+        const __nv_bfloat162 hb = __floats2bfloat162_rn(a, b);
+        const float2 hf = __bfloat1622float2(hb);
+        const __nv_bfloat162 lb = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+        hw[e] = *reinterpret_cast<const uint32_t*>(&hb);
+        lw[e] = *reinterpret_cast<const uint32_t*>(&lb);
+    }
     const int off = ((r >> 3) * 4 + c) * 128 + (r & 7) * 16;
-    *reinterpret_cast<uint4*>(hiBase + off) = *reinterpret_cast<const uint4*>(h);
-    *reinterpret_cast<uint4*>(loBase + off) = *reinterpret_cast<const uint4*>(l);
+    *reinterpret_cast<uint4*>(hiBase + off) = h;
+    *reinterpret_cast<uint4*>(loBase + off) = l;
 }
 
 // slice [k0, k0 + 32) of op(A) rows m0.. and op(B) columns n0.. into a stage
@@ -169,7 +180,7 @@ __device__ __forceinline__ void epilogueStore(const GemmDesc& D, int row, int co
 }
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads, 1) gemmMixedKernel(const GemmDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kThreads, 2) gemmMixedKernel(const GemmDesc* __restrict__ descs,
                                                                const TileRef* __restrict__ tiles,
                                                                int* status) {
     extern __shared__ __align__(128) uint8_t mxSmem[];
