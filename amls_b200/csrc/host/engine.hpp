@@ -330,7 +330,7 @@ private:
     // backward sweeps over the tree levels), captured per (locked rows,
     // operand and output buffers) from the second refinement of an analysis
     // on and replayed after: graph and the kernels in it
-    std::map<std::array<uintptr_t, 9>, std::pair<cudaGraphExec_t, int64_t>> applyGraphs_;
+    std::map<std::array<uintptr_t, 10>, std::pair<cudaGraphExec_t, int64_t>> applyGraphs_;
     int refineEagerRuns_ = 0;                       // eager refinements since the analysis
     std::vector<cudaEvent_t> evPool_;
     size_t evUsed_ = 0;

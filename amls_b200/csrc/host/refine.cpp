@@ -525,11 +525,15 @@ int Engine::refine(double* Q, int nq, int nev, std::vector<double>& theta, bool 
         if (!useGraphs) {
             applyLaunches(Y, MY, keepR);
         } else {
-            const std::array<uintptr_t, 9> key{static_cast<uintptr_t>(lock), reinterpret_cast<uintptr_t>(Y),
-                                               reinterpret_cast<uintptr_t>(MY), keepR ? 1u : 0u,
-                                               reinterpret_cast<uintptr_t>(X), reinterpret_cast<uintptr_t>(R),
-                                               reinterpret_cast<uintptr_t>(b.dev<char>(0)),
-                                               static_cast<uintptr_t>(nq), static_cast<uintptr_t>(n)};
+            // everything the captured launches hold by value: the locked
+            // rows, the operand and output buffers (the split-K clears write
+            // into X and Tm), the launch tables and the sizes
+            const std::array<uintptr_t, 10> key{static_cast<uintptr_t>(lock), reinterpret_cast<uintptr_t>(Y),
+                                                reinterpret_cast<uintptr_t>(MY), keepR ? 1u : 0u,
+                                                reinterpret_cast<uintptr_t>(X), reinterpret_cast<uintptr_t>(R),
+                                                reinterpret_cast<uintptr_t>(Tm),
+                                                reinterpret_cast<uintptr_t>(b.dev<char>(0)),
+                                                static_cast<uintptr_t>(nq), static_cast<uintptr_t>(n)};
             auto it = applyGraphs_.find(key);
             if (it == applyGraphs_.end()) {
                 cudaGraph_t g = nullptr;
