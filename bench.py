@@ -25,7 +25,7 @@ tests/test_oracle_cpu.py) on the host cores, each step one full C5 solve as
 the reference's AmlsSolver::solve runs it, its nested-dissection partition
 included (the sequential restatement oracle/metis_seq.cpp, which reproduces
 the fixture tree; no product code loaded); when the requested steps would
-not end within AMLS_REF_BUDGET_S (600 s) fewer are timed and the line's
+not end within AMLS_REF_BUDGET_S (300 s) fewer are timed and the line's
 `steps` says how many.  The same full run, once, is our arm's
 `cpu_baseline`.
 """
@@ -561,7 +561,7 @@ def run_reference(args, rank, world):
     p = cases.config_pencil("C5", seed=0)
     tree = c5_tree()
     nl = CONFIGS["C5"]["nLevels"]
-    budget = float(os.environ.get("AMLS_REF_BUDGET_S", "600"))
+    budget = float(os.environ.get("AMLS_REF_BUDGET_S", "300"))
     t_start = time.perf_counter()
     t, pp, pa, tm = cpu_full_solve(p, cores, 500, nl, tree)   # first warm-up step
     warm = 1
